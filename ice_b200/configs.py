@@ -1,0 +1,249 @@
+"""The workloads: seeded synthetic cases with the shapes of the reference's
+benchmark configurations, and the crossing-jets case of its validation suite.
+
+No dataset is involved: every field is generated here from a seed.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .case import Case, Family, Numerics, box_bc, box_nodes, empty_state
+
+PI = 3.14159265358979323846
+
+
+def particle_mass(radius, rho_m):
+    return 4.0 / 3.0 * PI * radius ** 3 * rho_m
+
+
+def _gas_layout(case: Case, b: int, rho, u, v, w, T, R=287.05, gam=1.4, k=0.026, mu=1.8e-5):
+    ni, nj, nk = case.dims[b]
+    shp = (nk, nj, ni)
+    prim5 = np.stack([np.broadcast_to(rho, shp), np.broadcast_to(u, shp), np.broadcast_to(v, shp),
+                      np.broadcast_to(w, shp), np.broadcast_to(T, shp)], axis=-1).astype(np.float64)
+    full = lambda x: np.ascontiguousarray(np.broadcast_to(np.float64(x), shp))
+    return {"prim5": np.ascontiguousarray(prim5), "R": full(R), "gam": full(gam), "k": full(k), "mu": full(mu)}
+
+
+def fourier_velocity(rng, shape, spacing, lo, nmodes=32, kmin=1, kmax=8, rms=10.0, ndim=3, length=None):
+    """A divergence-free sum of nmodes seeded Fourier modes at the cell centres, |k| in
+    [kmin, kmax] (units of 2 pi / length), scaled to the given RMS speed. Returns (u, v, w)
+    with shape (nk, nj, ni)."""
+    nk, nj, ni = shape
+    L = length
+    xc = lo[0] + (np.arange(ni) + 0.5) * spacing[0]
+    yc = lo[1] + (np.arange(nj) + 0.5) * spacing[1]
+    zc = lo[2] + (np.arange(nk) + 0.5) * spacing[2]
+    ks, amps, phases = [], [], []
+    while len(ks) < nmodes:
+        kv = rng.integers(-kmax, kmax + 1, size=3)
+        if ndim == 2:
+            kv[2] = 0
+        kn = float(np.linalg.norm(kv))
+        if kn < kmin or kn > kmax:
+            continue
+        a = rng.normal(size=3)
+        if ndim == 2:
+            a[2] = 0.0
+        a = a - kv * (a @ kv) / (kn * kn)          # A . k = 0: divergence-free
+        ks.append(kv); amps.append(a / max(np.linalg.norm(a), 1e-30) / kn); phases.append(rng.uniform(0, 2 * PI))
+    u = np.zeros(shape); v = np.zeros(shape); w = np.zeros(shape)
+    for kv, a, ph in zip(ks, amps, phases):
+        arg = (2 * PI / L) * (kv[0] * xc[None, None, :] + kv[1] * yc[None, :, None] + kv[2] * zc[:, None, None]) + ph
+        cs = np.cos(arg)
+        u += a[0] * cs; v += a[1] * cs; w += a[2] * cs
+    s = rms / math.sqrt(float(np.mean(u * u + v * v + w * w)))
+    return u * s, v * s, w * s
+
+
+def gaussian_blobs(rng, shape, spacing, lo, nblobs, width, length):
+    nk, nj, ni = shape
+    xc = lo[0] + (np.arange(ni) + 0.5) * spacing[0]
+    yc = lo[1] + (np.arange(nj) + 0.5) * spacing[1]
+    zc = lo[2] + (np.arange(nk) + 0.5) * spacing[2]
+    out = np.zeros(shape)
+    which = np.full(shape, -1, dtype=np.int64)
+    best = np.zeros(shape)
+    for m in range(nblobs):
+        c = lo + rng.uniform(0.15, 0.85, size=3) * length
+        g = (np.exp(-((xc[None, None, :] - c[0]) ** 2) / (2 * width ** 2))
+             * np.exp(-((yc[None, :, None] - c[1]) ** 2) / (2 * width ** 2))
+             * np.exp(-((zc[:, None, None] - c[2]) ** 2) / (2 * width ** 2)))
+        out += g
+        which = np.where(g > best, m, which)
+        best = np.maximum(best, g)
+    return np.minimum(out, 1.0), which
+
+
+# ------------------------------------------------------------ config 1
+def riemann_1d(n=2000, steps=1000):
+    """Plain FP64 1-D IG Riemann problem: 2000 cells on [0,1], discontinuity at 0.5,
+    left rho 1 u +1 theta 0.1, right rho 0.5 u -1 theta 0.05, 10 um particles of
+    material density 1000, exchange off, transmissive ends. MUSCL minmod, HLLE, SSP-RK3,
+    CFL 0.5. dt-max is set above the CFL step (1.0) so that the CFL condition sets dt."""
+    dx = 1.0 / n
+    nodes = box_nodes(n, 1, 1, size=(1.0, dx, dx))
+    fam = Family("IG", riemann="HLLE", rho_al=1000.0, cs_al=1000.0)
+    num = Numerics(scheme="RK3", cfl=0.5, dt_max=1.0, limiter="minmod", itermax=steps)
+    rows = box_bc(1, (n, 1, 1), {1: 400, 2: 400, 3: 0, 4: 0, 5: 0, 6: 0})
+    case = Case("riemann_1d", [nodes], [fam], num, rows)
+    st = empty_state((n, 1, 1), 7)
+    xc = (np.arange(n) + 0.5) * dx
+    left = xc < 0.5
+    rho = np.where(left, 1.0, 0.5)
+    u = np.where(left, 1.0, -1.0)
+    theta = np.where(left, 0.1, 0.05)
+    mp = particle_mass(10e-6, 1000.0)
+    I = st[2:3, 2:3, 2:-2]
+    I[..., 0] = rho; I[..., 1] = u; I[..., 2] = 0.0; I[..., 3] = 0.0
+    I[..., 4] = rho * theta; I[..., 5] = 300.0; I[..., 6] = rho / mp
+    case.state = [[st]]
+    return case
+
+
+# --------------------------------------------------- crossing jets (validation)
+def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
+    """The crossing-jets validation case of the reference's suite (its Doisneau cases):
+    100 x 100 cells of 0.01 on [0,1] x [-0.5,0.5], slab 1e-3 thick; face 1 symmetry except
+    two inlets of 10 cells each (402: mass flux 0.7071, 10 m/s at +/-45 deg, 300 K, 1 um;
+    j = 21..30 and 71..80, the MK case's upper inlet at 72..81 as its table has it),
+    faces 2-4 extrapolation; every cell starts at 1e-20; steady (each cell its own dt),
+    RK2, CFL 0.8, MUSCL van Leer, no exchange; constant material density 2000, cp 1500."""
+    # the node coordinates are the decimal values of the case's mesh file, each parsed to
+    # its nearest double, so that the mesh is symmetric about y = 0 to the bit
+    dec = lambda a: np.array([float(f"{v:.8f}") for v in a])
+    x = dec(np.arange(n + 1) / n)
+    y = dec(np.arange(n + 1) / n - 0.5)
+    z = np.array([-0.0005, 0.0005])
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    nodes = np.stack([X, Y, Z], axis=-1)
+    fam = Family(closure, rho_al=2000.0, cs_al=1500.0)
+    num = Numerics(scheme="RK2", time_accurate=False, cfl=0.8, limiter="vanleer", itermax=steps)
+
+    def payload(f, i, j, k):
+        alpha = 7.85400e-01 if j <= n // 2 else -7.85400e-01
+        return (7.07100e-01, 1.0e1, alpha, 0.0, 3.0e2, 1.0e-6, 0.0, 0.0)
+    codes = {1: 300, 2: 400, 3: 400, 4: 400, 5: 0, 6: 0}
+    if upper is None:
+        upper = (72, 81) if closure == "MK" else (71, 80)
+    rows = []
+    for row in box_bc(1, (n, n, 1), codes):
+        b, i, j, k, f, code, pay = row
+        if f == 1 and (21 <= j <= 30 or upper[0] <= j <= upper[1]):
+            rows.append((b, i, j, k, f, 402, payload(f, i, j, k)))
+        else:
+            rows.append(row)
+    case = Case(f"crossing_jets_{closure}", [nodes], [fam], num, rows)
+    st = empty_state((n, n, 1), fam.nc)
+    st[2:-2, 2:-2, 2:-2, :] = 1e-20
+    case.state = [[st]]
+    return case
+
+
+# ------------------------------------------------------------ config 2
+def jets_2d(n=1024, steps=500, seed=2, length=0.1, precision=0):
+    """2-D single block n x n, MK and IG families advanced together (one run, two families),
+    one-way coupled to a frozen gas: velocity = 32 seeded divergence-free Fourier modes
+    (|k| in 1..8, RMS 10 m/s), T = 300 K, p = 101325 Pa (rho = p/(R T)). Two jets enter the
+    left face at +30 and -30 deg (402: 20 um, 300 K, 10 m/s, volume fraction 1e-4); the rest
+    of the left face is symmetry, the other faces extrapolation. Drag Schiller-Naumann, heat
+    Ranz-Marshall; Rusanov, van Leer, SSP-RK2."""
+    rng = np.random.default_rng(seed)
+    dx = length / n
+    nodes = box_nodes(n, n, 1, size=(length, length, dx))
+    rho_m, rp, vf, speed = 1000.0, 20e-6, 1e-4, 10.0
+    fams = [Family("MK", riemann="Rusanov", rho_al=rho_m, cs_al=4180.0, lv_al=2.26e6),
+            Family("IG", riemann="Rusanov", rho_al=rho_m, cs_al=4180.0, lv_al=2.26e6)]
+    num = Numerics(scheme="RK2", cfl=0.5, limiter="vanleer", coupled=True, drag="Schiller-Naumann",
+                   heat="Ranz-Marshall", itermax=steps, precision=precision)
+    j1 = (int(0.30 * n) - n // 40, int(0.30 * n) + n // 40)
+    j2 = (int(0.70 * n) - n // 40, int(0.70 * n) + n // 40)
+    cos30 = math.cos(PI / 6.0)
+    rows = []
+    for row in box_bc(1, (n, n, 1), {1: 300, 2: 400, 3: 400, 4: 400, 5: 0, 6: 0}):
+        b, i, j, k, f, code, pay = row
+        if f == 1 and (j1[0] <= j <= j1[1] or j2[0] <= j <= j2[1]):
+            alpha = PI / 6.0 if j <= n // 2 else -PI / 6.0
+            rows.append((b, i, j, k, f, 402, (vf * rho_m * speed * cos30, speed, alpha, 0.0, 300.0, rp, 0.0, 0.0)))
+        else:
+            rows.append(row)
+    case = Case("jets_2d", [nodes], fams, num, rows)
+    u, v, w = fourier_velocity(rng, (1, n, n), (dx, dx, dx), np.zeros(3), rms=10.0, ndim=2, length=length)
+    T = 300.0
+    rho_g = 101325.0 / (287.05 * T)
+    case.gas = [_gas_layout(case, 0, rho_g, u, v, 0.0 * w, T)]
+    mp = particle_mass(rp, rho_m)
+    states = []
+    for fam in fams:
+        st = empty_state((n, n, 1), fam.nc)
+        I = st[2:-2, 2:-2, 2:-2]
+        I[...] = 0.0
+        I[..., 0] = 1e-20
+        I[..., fam.nc - 2] = 300.0
+        I[..., fam.nc - 1] = 1e-20 / mp
+        if fam.closure == "IG":
+            I[..., 4] = 1e-20
+        states.append(st)
+    case.state = [states]
+    return case
+
+
+# ------------------------------------------------------------ config 3
+def droplet_material(**kw):
+    d = dict(rho_al=1000.0, cs_al=4180.0, lv_al=2.26e6, emiss=0.9, evap="CEM", intf="LK", Mv=18.015,
+             cpv=1996.0, Le=1.0, Yinf=0.0, Tboil=373.15, alphaE=1.0)
+    d.update(kw)
+    return d
+
+
+def _cloud_state(rng, fam, shape, spacing, lo, L, u, v, w, median=30e-6, sigma=0.4, vf=1e-4, nblobs=16,
+                 empty_rho=1e-12):
+    blob, which = gaussian_blobs(rng, shape, spacing, lo, nblobs, width=0.08 * L, length=L)
+    radii = median * np.exp(sigma * rng.normal(size=nblobs))
+    rp = np.where(which >= 0, radii[np.maximum(which, 0)], median)
+    rho = np.maximum(vf * fam.rho_al * blob, empty_rho)
+    mp = 4.0 / 3.0 * PI * rp ** 3 * fam.rho_al
+    nk, nj, ni = shape
+    st = empty_state((ni, nj, nk), fam.nc)
+    I = st[2:-2, 2:-2, 2:-2]
+    I[..., 0] = rho; I[..., 1] = u; I[..., 2] = v; I[..., 3] = w
+    if fam.closure == "IG":
+        I[..., 4] = rho * 1e-2
+    elif fam.closure == "AG":
+        I[..., 4:10] = 0.0
+        I[..., 4] = rho * 1e-2; I[..., 7] = rho * 1e-2; I[..., 9] = rho * 1e-2
+    I[..., fam.nc - 2] = 300.0
+    I[..., fam.nc - 1] = rho / mp
+    return st
+
+
+def gas_recipe(rng, shape, spacing, lo, L, rms=15.0):
+    u, v, w = fourier_velocity(rng, shape, spacing, lo, rms=rms, ndim=3, length=L)
+    blobT, _ = gaussian_blobs(rng, shape, spacing, lo, 8, width=0.15 * L, length=L)
+    T = 300.0 + 1200.0 * blobT / max(float(blobT.max()), 1e-30)
+    rho_g = 101325.0 / (287.05 * T)
+    return rho_g, u, v, w, T
+
+
+def cloud_3d(n=192, steps=200, seed=3, length=0.0192, precision=0):
+    """3-D single block n^3, one AG family of water droplets (lognormal radius, median 30 um,
+    sigma 0.4, volume fraction 1e-4 in 16 seeded Gaussian blobs), frozen gas of 15 m/s RMS
+    Fourier velocity and 300-1500 K smooth temperature blobs. Drag, heat, grey-body radiation,
+    evaporation (CEM gas side, Langmuir-Knudsen interface, MHB98 Stefan blowing). MUSCL van
+    Leer with the Jameson sensor, SSP-RK3. The reference refuses Saurel for AG: Rusanov."""
+    rng = np.random.default_rng(seed)
+    dx = length / n
+    nodes = box_nodes(n, n, n, size=(length, length, length))
+    fam = Family("AG", riemann="Rusanov", **droplet_material())
+    num = Numerics(scheme="RK3", cfl=0.5, limiter="vanleer", shock_detector=True, coupled=True,
+                   drag="Schiller-Naumann", heat="Ranz-Marshall", blowing=True, itermax=steps, precision=precision)
+    rows = box_bc(1, (n, n, n), {f: 400 for f in range(1, 7)})
+    case = Case("cloud_3d", [nodes], [fam], num, rows)
+    shape = (n, n, n)
+    sp = (dx, dx, dx)
+    rho_g, u, v, w, T = gas_recipe(rng, shape, sp, np.zeros(3), length)
+    case.gas = [_gas_layout(case, 0, rho_g, u, v, w, T)]
+    case.state = [[_cloud_state(rng, fam, shape, sp, np.zeros(3), length, u, v, w)]]
+    return case

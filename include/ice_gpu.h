@@ -1,0 +1,230 @@
+/*
+ * ice_gpu.h -- C ABI of the B200 (sm_100a) solve stage of ICE's Eulerian
+ * dispersed-phase time step.
+ *
+ * The Fortran driver keeps its INI registry, multi-block set-up, closure
+ * selection and Tecplot/VTK I/O. After set-up it hands the library the
+ * resolved parameters, the block metrics, the boundary table, the frozen gas
+ * and the initial state; then each call of ice_gpu_step replaces
+ *     call Explicit_Step(simulation%domain(lv))      (src/lib/driver/Wrap_Solve.f90:26)
+ * for one or more time steps, with every array resident in HBM.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success and a non-zero ICE_GPU_E* code on
+ *    failure; ice_gpu_last_error() returns the message. Nothing traps: a
+ *    failing state stops the step and is reported through the status word,
+ *    as the reference's `error stop 1` sites would.
+ *  - Indices in records are 1-based, as in the Fortran tables.
+ *  - Host arrays use the Fortran layouts of the reference, so the driver can
+ *    pass its own arrays with c_loc(); the library copies them and keeps no
+ *    host pointer after a call returns.
+ *  - One host thread per context; a context owns one CUDA stream.
+ */
+#ifndef ICE_GPU_H
+#define ICE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICE_GPU_ABI_VERSION   1
+#define ICE_GPU_MAX_FAMILIES  4
+#define ICE_GPU_NCOND_MAX     12
+#define ICE_GPU_NEP           8
+#define ICE_GPU_REC_INTS      15   /* b i j k f type p bs is js ks fs partner owner cf */
+#define ICE_GPU_REC_REALS     8    /* massflux velocity alpha beta temperature radius gfixed normal_dir */
+
+/* Return codes */
+#define ICE_GPU_OK             0
+#define ICE_GPU_EINVAL         1   /* bad argument or inconsistent input */
+#define ICE_GPU_ECUDA          2   /* CUDA runtime error */
+#define ICE_GPU_ESTATE         3   /* the step stopped on a state the reference stops on */
+#define ICE_GPU_ENOMEM         4
+#define ICE_GPU_ENOTREADY      5   /* a required input has not been given */
+
+/* Status bits of ice_gpu_step_out.status (the reference's error stops) */
+#define ICE_GPU_ST_NAN_STATE   1   /* NaN/Inf after an update   (Lib_Newstate.f90:189-193)  */
+#define ICE_GPU_ST_BAD_RECON   2   /* unphysical first-order face (Mod_Fluxes.f90:238-241,
+                                      Mod_BC_Fluxes.f90:95-98)                               */
+#define ICE_GPU_ST_TIMEOUT     4   /* a bounded device wait gave up                          */
+
+/* Closures (Assign_Setup.f90:104-117) */
+#define ICE_CLOSURE_MK 1           /* rho u v w T n                                   (6) */
+#define ICE_CLOSURE_IG 2           /* rho u v w P T n                                 (7) */
+#define ICE_CLOSURE_AG 3           /* rho u v w P11 P12 P13 P22 P23 P33 T n          (12) */
+
+/* Riemann solvers (Lib_Riemann.f90:30-57) */
+#define ICE_RIEMANN_SAUREL  1
+#define ICE_RIEMANN_RUSANOV 2
+#define ICE_RIEMANN_HLLE    3
+
+/* Limiters, in the order of assign_limiter (Lib_Limiters.f90:35-86); 0 is first order */
+#define ICE_LIM_IORD       0
+#define ICE_LIM_MINMOD     1
+#define ICE_LIM_VANALBADA  2
+#define ICE_LIM_VANLEER    3
+#define ICE_LIM_OSPRE      4
+#define ICE_LIM_UMIST      5
+#define ICE_LIM_OSHER      6
+#define ICE_LIM_SWEBY      7
+#define ICE_LIM_MC         8
+#define ICE_LIM_KOREN      9
+#define ICE_LIM_SUPERBEE  10
+
+/* Precision forms */
+#define ICE_PREC_FP64      0       /* plain form: everything FP64                       */
+#define ICE_PREC_FP32FLUX  1       /* reconstruction, Riemann fluxes and sources in FP32,
+                                      RK accumulation, dt reduction and norms in FP64    */
+
+/* One particle family: its closure, its Riemann solver, its frozen slots and
+ * the constant-property material it is made of (condensed_phase_t,
+ * src/lib/config/Config_Types_m.f90; ep packed as Setup_Materials.f90:152-160). */
+typedef struct ice_gpu_family {
+    int32_t closure;                    /* ICE_CLOSURE_*                                  */
+    int32_t riemann;                    /* ICE_RIEMANN_*                                  */
+    int32_t nfrozen;                    /* slots setup_freeze does not integrate          */
+    int32_t frozen[ICE_GPU_NCOND_MAX];  /* their 1-based numbers                          */
+    double  rho_al;                     /* material density [kg/m3]                       */
+    double  cs_al;                      /* material specific heat [J/(kg K)]              */
+    double  lv_al;                      /* latent heat [J/kg]                             */
+    double  emiss;                      /* surface emissivity [-]                         */
+    int32_t evap;                       /* 0 none, 1 d2, 2 CEM, 3 CEM-B, 4 ASM, 5 TC      */
+    int32_t intf;                       /* 0 VLE, 1 Langmuir-Knudsen                      */
+    int32_t liq;                        /* 0 ITC (P2T not supported: ICE_GPU_EINVAL)      */
+    int32_t boil;                       /* 0 clamp (ZGR not supported: ICE_GPU_EINVAL)    */
+    double  ep[ICE_GPU_NEP];            /* Mv Lv cpv Le Yinf LvMv/Ru 1/Tboil alphaE      */
+} ice_gpu_family;
+
+/* The resolved numerics of a run (obj_time_scheme, obj_space_scheme, obj_irs,
+ * obj_sim_param, obj_io of the reference). */
+typedef struct ice_gpu_params {
+    int32_t nfam;                       /* ngroups                                        */
+    int32_t ndir;                       /* 1, 2 or 3 (Mod_Metrics check_mesh_type)        */
+    int32_t nrk;                        /* 1 euler, 2 RK2, 3 RK3                          */
+    int32_t time_accurate;              /* 1: one global dt; 0: each cell its own dt      */
+    double  cfl;
+    double  dt_max;
+    double  tau_factor;
+    int32_t cfl_ramp_iter;
+    int32_t limiter;                    /* ICE_LIM_*; 0 = first-order reconstruction      */
+    int32_t shock_detector;             /* 1: Jameson sensor on density                   */
+    int32_t irs;                        /* implicit residual smoothing (steady runs only) */
+    double  irs_beta;
+    int32_t coupled;                    /* one-way coupling to a frozen gas: sources on   */
+    int32_t drag;                       /* 1..13, Lib_Drag.f90:19-79                      */
+    int32_t heat;                       /* 1..8,  Lib_Heat.f90:18-64                      */
+    int32_t blow;                       /* 0 none, 1 MHB98 f2                             */
+    int32_t precision;                  /* ICE_PREC_*                                     */
+    int32_t itermax;                    /* iterations of this call of the solver          */
+    int32_t sol_diter;
+    int32_t shell_diter;
+    int32_t res_diter;
+    int32_t pad0;
+    double  time_threshold;
+    double  res_threshold;
+    double  sol_dtime;
+    ice_gpu_family fam[ICE_GPU_MAX_FAMILIES];
+} ice_gpu_params;
+
+/* What one call of ice_gpu_step leaves for the driver (Explicit_Step's outputs). */
+typedef struct ice_gpu_step_out {
+    double  dtglobal;                   /* the last step's global dt                      */
+    double  time;                       /* simulated time after the last step             */
+    int32_t iter;                       /* grid%iter after the last step                  */
+    int32_t todo;                       /* 1 continue, 2 output, 3 end (Mod_Explicit.f90:225-239) */
+    int32_t status;                     /* ICE_GPU_ST_* bits                              */
+    int32_t have_norm;                  /* residual[] holds the last step's norm          */
+    int64_t nfloored;                   /* negative densities floored so far              */
+    double  residual[5];                /* residual norm (rho, rho u, rho v, rho w, T)    */
+} ice_gpu_step_out;
+
+typedef struct ice_gpu_ctx ice_gpu_ctx;
+
+/* Set-up (after setup_freeze, Wrap_Setup.f90:121). dims: 3 ints per block.
+ * replaces: allocate_data / Allocate_Block (driver/Mod_Allocate_Data.f90:8-133)
+ * for the solve stage's arrays. */
+int ice_gpu_create(const ice_gpu_params* params, int32_t nblocks, const int32_t* dims,
+                   ice_gpu_ctx** ctx);
+
+/* Metrics of block b (1-based), Fortran layouts of Allocate_Block:
+ *   face_d : per face 4 doubles (N(3), A), dir(1)%f(0:ni,1:nj,1:nk),
+ *            dir(2)%f(1:ni,0:nj,1:nk), dir(3)%f(1:ni,1:nj,0:nk)
+ *   vol    : (1:ni,1:nj,1:nk)
+ *   dl     : 3 doubles per cell on (0:ni+1,0:nj+1,0:nk+1)
+ *   M      : 9 doubles per cell (column-major c(3,3)) on (0:ni+1,0:nj+1,0:nk+1)
+ * replaces: setup_metrics' results (numerics/space/Mod_Metrics.f90:19-60). */
+int ice_gpu_set_block(ice_gpu_ctx* ctx, int32_t b, const double* face1, const double* face2,
+                      const double* face3, const double* vol, const double* dl, const double* M);
+
+/* The whole boundary table in table order (grid%bc), ICE_GPU_REC_INTS ints and
+ * ICE_GPU_REC_REALS reals per record, partner/owner/cf as Pair_Connections left
+ * them. The library builds the per-family record lists, the boundary cells with
+ * their records in face order and the connection owners from it.
+ * replaces: build_local_bc_index (parallel/Mod_GhostExchange.f90:103-172). */
+int ice_gpu_set_records(ice_gpu_ctx* ctx, int32_t nrec, const int32_t* rec, const double* inlet);
+
+/* Frozen gas of block b: prim5 (5,ni,nj,nk) = rho u v w T, then R, gamma, k, mu (ni,nj,nk).
+ * replaces: setup_gas (driver/Mod_Phase.f90:11-63). */
+int ice_gpu_set_gas(ice_gpu_ctx* ctx, int32_t b, const double* prim5, const double* R,
+                    const double* gam, const double* k, const double* mu);
+
+/* State of family p (1-based) in block b: prim (ncond, 1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc),
+ * gc = 2; inj the injected-ghost flags on the same cells (NULL: all false).
+ * replaces: setup_cond's result (driver/Mod_Phase.f90:66-124). */
+int ice_gpu_upload_state(ice_gpu_ctx* ctx, int32_t b, int32_t p, const double* prim,
+                         const uint8_t* inj);
+
+/* The state back in the same layout (interior cells exact; ghost cells hold the
+ * last fill). Called before Write_Solution (Wrap_Postprocess.f90:120-196). */
+int ice_gpu_download_state(ice_gpu_ctx* ctx, int32_t b, int32_t p, double* prim);
+
+/* Simulated time and iteration count (a restart, or a second call of the solver). */
+int ice_gpu_set_time(ice_gpu_ctx* ctx, double time, int32_t iter, int32_t iter_from_call);
+
+/* nsteps time steps. replaces: call Explicit_Step(grid) (driver/Wrap_Solve.f90:26),
+ * numerics/time/explicit/Mod_Explicit.f90:11-245. Returns ICE_GPU_ESTATE when a
+ * step ended on a state the reference stops on (out->status says which). */
+int ice_gpu_step(ice_gpu_ctx* ctx, int32_t nsteps, ice_gpu_step_out* out);
+
+/* The residual norm of the last step: total[5], and fam[5*nfam] per family (may be NULL).
+ * replaces: residual_norm (diagnostic/Mod_Diagnostic.f90:22-83). */
+int ice_gpu_residual_norm(ice_gpu_ctx* ctx, double* total, double* fam);
+
+/* A runtime re-read of input.ini (Wrap_Postprocess.f90:255 -> Read_Ini.f90:61): the
+ * numerics may change between steps; nfam, closures and ndir may not. */
+int ice_gpu_update_params(ice_gpu_ctx* ctx, const ice_gpu_params* params);
+
+/* The message of the last failing call on ctx (or of ice_gpu_create when ctx is NULL). */
+int ice_gpu_last_error(const ice_gpu_ctx* ctx, char* buf, int32_t buflen);
+
+int ice_gpu_destroy(ice_gpu_ctx* ctx);
+
+/* Host-only: partner, owner and face number of every connection record (101/201)
+ * of a boundary table in table order, written into fields 13..15 of rec.
+ * replaces: Pair_Connections (io/IO_BC.f90:360-510). ngroups families, the
+ * records of boundary cell n and family p at position (n-1)*ngroups + p. */
+int ice_gpu_pair_connections(int32_t nblocks, const int32_t* dims, int32_t ngroups,
+                             int32_t nrec, int32_t* rec, char* err, int32_t errlen);
+
+/* Debug / parity: the index maps the library built from the boundary table.
+ * For family p: nbcell boundary cells, first[nbcell+1] (1-based into recs),
+ * recs[] (1-based record numbers in face order), nown owners own[] (1-based).
+ * Pass NULL arrays to query the counts. replaces nothing: it exposes
+ * grid%bcells(p) and grid%conn(p)%own for comparison with the reference's. */
+int ice_gpu_index_maps(const ice_gpu_ctx* ctx, int32_t p, int32_t* nbcell, int32_t* first,
+                       int32_t* nrecs, int32_t* recs, int32_t* nown, int32_t* own);
+
+/* Measurement: device time [ms] of the kernels of the last ice_gpu_step, by kernel
+ * class (0 dt, 1 ghost, 2 beta, 3 bound, 4 stage, 5 irs, 6 norm), and the
+ * number of kernels launched. Filled only when the context was made with
+ * profiling on (ice_gpu_set_profiling). */
+int ice_gpu_set_profiling(ice_gpu_ctx* ctx, int32_t on);
+int ice_gpu_kernel_times(const ice_gpu_ctx* ctx, double* ms, int32_t nclass, int64_t* nlaunch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICE_GPU_H */
