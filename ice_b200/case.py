@@ -304,9 +304,11 @@ def interior(a):
     return a[2:-2, 2:-2, 2:-2]
 
 
-def box_bc(b, dims, codes, payload=None):
-    """One block's boundary table, faces 1..6 as the ATLAS order of make_case.py: i faces per (j,k),
-    then j faces, then k faces. codes: {face: code}; payload(face, i, j, k) -> tuple."""
+def box_bc(b, dims, codes, payload=None, face_major=False):
+    """One block's boundary table. Default: the order of the reference's bench generator
+    (test/bench/make_case.py: i faces per (j,k), then j faces, then k faces); face_major: face 1,
+    then 2, ... 6, each face's cells with the first index fastest (the ATLAS tables of the
+    reference's validation cases). codes: {face: code}; payload(face, i, j, k) -> tuple."""
     ni, nj, nk = dims
     rows = []
 
@@ -314,6 +316,18 @@ def box_bc(b, dims, codes, payload=None):
         code = codes[f]
         pay = payload(f, i, j, k) if (payload and 401 <= code <= 403) else ()
         rows.append((b, i, j, k, f, code, pay))
+    if face_major:
+        for f in range(1, 7):
+            d = (f - 1) // 2
+            n = [ni, nj, nk]
+            fixed = 1 if f % 2 == 1 else n[d]
+            t1, t2 = [a for a in range(3) if a != d]
+            for c2 in range(1, n[t2] + 1):
+                for c1 in range(1, n[t1] + 1):
+                    ijk = [0, 0, 0]
+                    ijk[d], ijk[t1], ijk[t2] = fixed, c1, c2
+                    rec(ijk[0], ijk[1], ijk[2], f)
+        return rows
     for k in range(1, nk + 1):
         for j in range(1, nj + 1):
             rec(1, j, k, 1)

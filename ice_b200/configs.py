@@ -129,7 +129,7 @@ def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
     if upper is None:
         upper = (72, 81) if closure == "MK" else (71, 80)
     rows = []
-    for row in box_bc(1, (n, n, 1), codes):
+    for row in box_bc(1, (n, n, 1), codes, face_major=True):
         b, i, j, k, f, code, pay = row
         if f == 1 and (21 <= j <= 30 or upper[0] <= j <= upper[1]):
             rows.append((b, i, j, k, f, 402, payload(f, i, j, k)))
@@ -247,3 +247,151 @@ def cloud_3d(n=192, steps=200, seed=3, length=0.0192, precision=0):
     case.gas = [_gas_layout(case, 0, rho_g, u, v, w, T)]
     case.state = [[_cloud_state(rng, fam, shape, sp, np.zeros(3), length, u, v, w)]]
     return case
+
+
+# ------------------------------------------------------------ config 4 / 5
+def solid_material(**kw):
+    d = dict(rho_al=2700.0, cs_al=900.0, lv_al=1.08e7, emiss=0.8, evap="none")
+    d.update(kw)
+    return d
+
+
+FAMILY_RADIUS = {"MK": 10e-6, "IG": 30e-6, "AG": 60e-6}
+
+
+def tree_blocks(nblocks, seed, lo=16, hi=160):
+    """A tree of blocks joined face to face: block 0 first, each next block attached to a free face
+    of an earlier one, its two axes along the face those of the face, the third drawn uniformly in
+    lo..hi. Returns (dims, origins in cells, connections [(parent, face, child, child_face)])."""
+    rng = np.random.default_rng(seed)
+    dims = [tuple(int(x) for x in rng.integers(lo, hi + 1, size=3))]
+    orig = [np.zeros(3, dtype=np.int64)]
+    used = [set()]
+    conns = []
+    while len(dims) < nblocks:
+        p = int(rng.integers(0, len(dims)))
+        free = [f for f in range(1, 7) if f not in used[p]]
+        if not free:
+            continue
+        f = int(rng.choice(free))
+        d = (f - 1) // 2
+        nd = list(dims[p])
+        nd[d] = int(rng.integers(lo, hi + 1))
+        fc = f + 1 if f % 2 == 1 else f - 1          # the child's face against the parent
+        o = orig[p].copy()
+        if f % 2 == 0:
+            o[d] += dims[p][d]
+        else:
+            o[d] -= nd[d]
+        dims.append(tuple(nd)); orig.append(o); used.append({fc})
+        used[p].add(f)
+        conns.append((p, f, len(dims) - 1, fc))
+    return dims, orig, conns
+
+
+def multiblock_tree(nblocks=48, seed=9, lo=16, hi=160, h=1e-4, families=("MK", "IG", "AG"), steps=100,
+                    precision=0, evaporation_everywhere=False, scheme="RK3", gas_seed=None):
+    """3-D multi-block case: nblocks blocks of U[lo, hi] cells per axis joined by matched face
+    connections (101) in a seeded tree; the other faces extrapolation (400). Families MK (inert solid
+    particles, 10 um), IG (water droplets, 30 um), AG (water droplets, 60 um); the gas recipe and the
+    exchange terms of the 192^3 case (drag, heat, radiation, evaporation with LK and blowing). The
+    per-family default Riemann solver (Saurel MK, Rusanov IG/AG), MUSCL van Leer with the Jameson
+    sensor, SSP-RK3."""
+    dims, orig, conns = tree_blocks(nblocks, seed, lo, hi)
+    nodes = [box_nodes(*dm, lo=tuple(o * h), size=tuple(np.array(dm) * h)) for dm, o in zip(dims, orig)]
+    fams = []
+    for cl in families:
+        mat = solid_material() if cl == "MK" else droplet_material()
+        fams.append(Family(cl, **mat))
+    num = Numerics(scheme=scheme, cfl=0.5, limiter="vanleer", shock_detector=True, coupled=True,
+                   drag="Schiller-Naumann", heat="Ranz-Marshall", blowing=True, itermax=steps, precision=precision)
+    link = {}
+    for (p, f, c, fc) in conns:
+        link[(p, f)] = (c, fc)
+        link[(c, fc)] = (p, f)
+    rows = []
+    for b, (ni, nj, nk) in enumerate(dims):
+        codes = {f: (101 if (b, f) in link else 400) for f in range(1, 7)}
+        for row in box_bc(b + 1, (ni, nj, nk), codes):
+            bb, i, j, k, f, code, pay = row
+            if code == 101:
+                ob, of = link[(b, f)]
+                d = (f - 1) // 2
+                src = [i, j, k]
+                src[d] = 1 if f % 2 == 0 else dims[ob][d]     # the first cell of the block across
+                rows.append((bb, i, j, k, f, 101, (ob + 1, src[0], src[1], src[2], of)))
+            else:
+                rows.append(row)
+    case = Case(f"multiblock_{nblocks}", nodes, fams, num, rows)
+    rng = np.random.default_rng(seed if gas_seed is None else gas_seed)
+    ext_lo = np.min([o for o in orig], axis=0) * h
+    ext_hi = np.max([o + np.array(dm) for o, dm in zip(orig, dims)], axis=0) * h
+    L = float(np.max(ext_hi - ext_lo))
+    # the gas recipe evaluated at every block's own cell centres, in one frame
+    modes = _draw_modes(rng, 32, 1, 8)
+    tblobs = [(ext_lo + rng.uniform(0.15, 0.85, size=3) * (ext_hi - ext_lo)) for _ in range(8)]
+    dblobs = [(ext_lo + rng.uniform(0.15, 0.85, size=3) * (ext_hi - ext_lo)) for _ in range(16)]
+    radii = {cl: FAMILY_RADIUS[cl] * np.exp(0.4 * rng.normal(size=16)) for cl in families}
+    case.gas, case.state = [], []
+    for b, (dm, o) in enumerate(zip(dims, orig)):
+        xc = [(o[a] + np.arange(dm[a]) + 0.5) * h for a in range(3)]
+        u, v, w = _eval_modes(modes, xc, L, rms=15.0)
+        T = 300.0 + 1200.0 * np.minimum(_eval_blobs(tblobs, xc, 0.15 * L), 1.0)
+        rho_g = 101325.0 / (287.05 * T)
+        case.gas.append(_gas_layout(case, b, rho_g, u, v, w, T))
+        blob = np.minimum(_eval_blobs(dblobs, xc, 0.08 * L), 1.0)
+        per_fam = []
+        for fam in fams:
+            rp = radii[fam.closure][np.argmax(np.stack([_eval_blobs([c], xc, 0.08 * L) for c in dblobs]), axis=0)]
+            floor = 1e-4 * fam.rho_al * 1e-3 if evaporation_everywhere else 1e-12
+            rho = np.maximum(1e-4 * fam.rho_al * blob, floor)
+            mp = 4.0 / 3.0 * PI * rp ** 3 * fam.rho_al
+            st = empty_state(dm, fam.nc)
+            I = st[2:-2, 2:-2, 2:-2]
+            I[..., 0] = rho; I[..., 1] = u; I[..., 2] = v; I[..., 3] = w
+            if fam.closure == "IG":
+                I[..., 4] = rho * 1e-2
+            elif fam.closure == "AG":
+                I[..., 4:10] = 0.0
+                I[..., 4] = rho * 1e-2; I[..., 7] = rho * 1e-2; I[..., 9] = rho * 1e-2
+            I[..., fam.nc - 2] = 300.0
+            I[..., fam.nc - 1] = rho / mp
+            per_fam.append(st)
+        case.state.append(per_fam)
+    case.conns = conns
+    return case
+
+
+def _draw_modes(rng, nmodes, kmin, kmax):
+    modes = []
+    while len(modes) < nmodes:
+        kv = rng.integers(-kmax, kmax + 1, size=3)
+        kn = float(np.linalg.norm(kv))
+        if kn < kmin or kn > kmax:
+            continue
+        a = rng.normal(size=3)
+        a = a - kv * (a @ kv) / (kn * kn)
+        modes.append((kv, a / max(np.linalg.norm(a), 1e-30) / kn, rng.uniform(0, 2 * PI)))
+    return modes
+
+
+def _eval_modes(modes, xc, L, rms):
+    x, y, z = xc
+    shape = (len(z), len(y), len(x))
+    u = np.zeros(shape); v = np.zeros(shape); w = np.zeros(shape)
+    for kv, a, ph in modes:
+        cs = np.cos((2 * PI / L) * (kv[0] * x[None, None, :] + kv[1] * y[None, :, None] + kv[2] * z[:, None, None]) + ph)
+        u += a[0] * cs; v += a[1] * cs; w += a[2] * cs
+    # the RMS of the mode sum over a periodic box of side L, independent of the block
+    s = rms / math.sqrt(sum(0.5 * float(a @ a) for _, a, _ in modes))
+    return u * s, v * s, w * s
+
+
+def _eval_blobs(centres, xc, width):
+    x, y, z = xc
+    out = 0.0
+    for c in centres:
+        out = out + (np.exp(-((x[None, None, :] - c[0]) ** 2) / (2 * width ** 2))
+                     * np.exp(-((y[None, :, None] - c[1]) ** 2) / (2 * width ** 2))
+                     * np.exp(-((z[:, None, None] - c[2]) ** 2) / (2 * width ** 2)))
+    return out

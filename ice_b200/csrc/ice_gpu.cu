@@ -1,0 +1,819 @@
+// ice_gpu.cu -- the B200 (sm_100a) solve stage of ICE's Eulerian dispersed-phase time step,
+// behind the C ABI of include/ice_gpu.h.
+//
+// One call of ice_gpu_step replaces `call Explicit_Step(grid)` (src/lib/driver/Wrap_Solve.f90:26;
+// numerics/time/explicit/Mod_Explicit.f90:11-245). Every array is resident in HBM; a step is a
+// CUDA graph of:
+//   k_begin        iteration counters, dt reset                      (Mod_Explicit.f90:40-44)
+//   k_dt           per-cell CFL dt + global min (FP64, warp shuffles) (Mod_dt.f90:11-112,256-275)
+//   k_time         dtglobal, time += dt                               (Mod_Explicit.f90:67-73)
+//   per family, per RK stage:
+//     k_ghost1/2   both ghost layers from the record list, block
+//                  connections as on-device copies in one HBM pool    (Lib_Ghost.f90:29-387)
+//     k_beta       Jameson sensor (when on)                           (Mod_Fluxes.f90:366-389)
+//     k_conn       connection-face fluxes by their owner records      (Mod_BC_Fluxes.f90:151-170)
+//     k_bound      boundary cells, records summed in face order        (Mod_BC_Fluxes.f90:105-144)
+//     k_stage      interior face fluxes of a tile in shared memory, gathered per cell in the
+//                  odd-then-even order (Mod_Fluxes.f90:421-521), fused with the source
+//                  (Mod_Sources.f90:465-622), the residual (Lib_Residual.f90:147-156) and the RK
+//                  update with cons<->prim and the state checks (Lib_Newstate.f90:198-219)
+//     (k_irs, k_update when implicit residual smoothing is on: Lib_IRS.f90:34-86)
+//
+// The state is stored structure-of-arrays, one contiguous array per variable over every block
+// of a family (ghost layers included), in three buffers that rotate over the RK stages: the
+// stage reads U_{k-1} (stencil) and U_0 (pointwise) and writes U_k, so no state copy
+// (state_copy, Lib_Newstate.f90:65-106) and no zeroing of the residual (Lib_Residual.f90:13-41)
+// remain: the residual lives in registers.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cstdarg>
+#include <vector>
+#include <string>
+#include <algorithm>
+#include <memory>
+#include "ice_kernels.cuh"
+#include "../../include/ice_gpu.h"
+
+using namespace ice;
+
+namespace {
+
+constexpr int kMaxF = ICE_GPU_MAX_FAMILIES;
+
+// ------------------------------------------------------------------ host side
+struct HRec {
+  int b, i, j, k, f, type, p, bs, is, js, ks, fs, partner, owner, cf;
+  double massflux, velocity, alpha, beta, temperature, radius, gfixed, normal_dir;
+};
+
+template <typename T> struct DevBuf {
+  T* p = nullptr; size_t n = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t count) {
+    if (p) { cudaFree(p); p = nullptr; }
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc((void**)&p, count * sizeof(T));
+  }
+};
+
+struct FamHost {
+  int closure, riemann, nc;
+  DevBuf<double> S[3];
+  DevBuf<unsigned char> inj;
+  DevBuf<double> dt, tau, beta;
+  DevBuf<int> bmap;
+  DevBuf<double> Rb, connF, resid, resid2, resid3;
+  DevBuf<DRec> recs;
+  DevBuf<int> bfirst, blist, own;
+  int nrec = 0, nbc = 0, nown = 0, ncf = 0;
+  std::vector<int> h_first, h_list, h_own;   // 0-based record numbers of the whole table
+};
+
+
+}  // namespace
+
+struct ice_gpu_ctx {
+  ice_gpu_params P;
+  int nb = 0;
+  std::vector<int> dims;
+  std::vector<DBlock> hblk;
+  long long NG = 0, NI = 0, NR = 0, NF[3] = {0, 0, 0};
+  DevBuf<DBlock> blk;
+  DevBuf<double> face[3], vol, dl, M, gas;
+  bool have_gas = false;
+  std::vector<bool> have_block;
+  bool have_records = false;
+  FamHost fam[kMaxF];
+  std::vector<HRec> recs;
+  DevBuf<Tile> tiles;
+  int ntile = 0, TX = 0, TY = 0, TZ = 0;
+  DevBuf<NormChunk> chunks;
+  DevBuf<double> npart;
+  int nchunk = 0;
+  std::vector<int> chunk_block;
+  DevBuf<Status> st;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  int phase = 0;          // buffer holding the current state
+  int prev_phase = -1;    // buffer holding the state before the last step
+  bool profiling = false;
+  double kms[KC_N] = {0};
+  long long nlaunch = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+};
+
+static std::string g_create_err;
+
+static int fail(ice_gpu_ctx* c, int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap; va_start(ap, fmt); vsnprintf(buf, sizeof buf, fmt, ap); va_end(ap);
+  if (c) c->err = buf; else g_create_err = buf;
+  return code;
+}
+
+#define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) \
+  return fail(c, ICE_GPU_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); } while (0)
+
+static int nbase_of(int cl) { return cl == ICE_CLOSURE_MK ? 6 : cl == ICE_CLOSURE_IG ? 7 : 12; }
+
+static void free_graphs(ice_gpu_ctx* c) {
+  for (auto& g : c->graph) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
+  FamHost& H = c->fam[p];
+  const ice_gpu_family& pf = c->P.fam[p];
+  FamDev F;
+  memset(&F, 0, sizeof F);
+  F.closure = H.closure; F.riemann = H.riemann; F.nc = H.nc;
+  F.limiter = c->P.limiter; F.sd = c->P.shock_detector; F.coupled = c->P.coupled;
+  F.drag = c->P.drag; F.heat = c->P.heat; F.blow = c->P.blow;
+  F.frozen_mask = 0;
+  for (int q = 0; q < pf.nfrozen; ++q) F.frozen_mask |= 1u << (pf.frozen[q] - 1);
+  F.mat.rho = pf.rho_al; F.mat.cp = pf.cs_al; F.mat.lv = pf.lv_al; F.mat.emiss = pf.emiss;
+  F.mat.evap = pf.evap; F.mat.intf = pf.intf;
+  for (int q = 0; q < ICE_GPU_NEP; ++q) F.mat.ep[q] = pf.ep[q];
+  // buffer roles (see the rotation in step_graph)
+  int a = phase, b = (phase + 1) % 3, cc = (phase + 2) % 3;
+  int up = srk == 1 ? a : srk == 2 ? b : cc;
+  int out = srk == 1 ? b : srk == 2 ? cc : b;
+  F.U0 = H.S[a].p; F.Up = H.S[up].p; F.Ug = H.S[up].p; F.Uo = H.S[out].p;
+  F.inj = H.inj.p;
+  F.beta = c->P.shock_detector ? H.beta.p : nullptr;
+  F.betaw = H.beta.p;
+  F.dt = c->P.time_accurate ? nullptr : H.dt.p;
+  F.dtg = &c->st.p->dtglobal;
+  F.tau = H.tau.p;
+  F.bmap = H.bmap.p;
+  F.Rb = H.Rb.p; F.Rbw = H.Rb.p;
+  F.connF = H.connF.p;
+  F.resid = H.resid.p;
+  static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
+  F.rk = RKC[c->P.nrk - 1][srk - 1];
+  F.write_tau = srk == c->P.nrk;
+  return F;
+}
+
+static Geo make_geo(ice_gpu_ctx* c) {
+  Geo G;
+  G.blk = c->blk.p; G.nb = c->nb;
+  G.NG = c->NG; G.NI = c->NI; G.NR = c->NR;
+  for (int d = 0; d < 3; ++d) { G.NF[d] = c->NF[d]; G.face[d] = c->face[d].p; }
+  G.vol = c->vol.p; G.dl = c->dl.p; G.M = c->M.p; G.gas = c->gas.p;
+  return G;
+}
+
+// ---------------------------------------------------------------- kernel dispatch
+#define GRID(n, t) ((unsigned)(((n) + (t) - 1) / (t)))
+
+static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_t s,
+                          void (*tick)(void*, int, cudaStream_t)) {
+  FamHost& H = c->fam[p];
+  LaunchArgs a;
+  a.G = make_geo(c);
+  a.F = make_famdev(c, p, srk, phase);
+  a.recs = H.recs.p; a.nrec = H.nrec;
+  a.own = H.own.p; a.nown = H.nown;
+  a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc;
+  a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.TZ = c->TZ;
+  a.ndir = c->P.ndir; a.sd = c->P.shock_detector; a.irs = c->P.irs; a.precision = c->P.precision;
+  a.irs_beta = c->P.irs_beta;
+  a.resid = H.resid.p; a.resid2 = H.resid2.p; a.resid3 = H.resid3.p;
+  a.st = c->st.p;
+  a.s = s;
+  a.tick = tick; a.tick_ctx = c;
+  if (H.closure == ICE_CLOSURE_MK) launch_family_mk(a);
+  else if (H.closure == ICE_CLOSURE_IG) launch_family_ig(a);
+  else launch_family_ag(a);
+}
+
+static void launch_dt(ice_gpu_ctx* c, int p, int phase, cudaStream_t s) {
+  Geo G = make_geo(c);
+  FamDev F = make_famdev(c, p, 1, phase);
+  double* dto = c->P.time_accurate ? nullptr : c->fam[p].dt.p;
+  unsigned g = GRID(c->NI, 256);
+  switch (c->fam[p].closure) {
+    case ICE_CLOSURE_MK: k_dt<MK><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
+    case ICE_CLOSURE_IG: k_dt<IG><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
+    default: k_dt<AG><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
+  }
+}
+
+static int next_phase(const ice_gpu_ctx* c, int phase) {
+  return c->P.nrk == 2 ? (phase + 2) % 3 : (phase + 1) % 3;
+}
+
+// One Explicit_Step on stream s starting from buffer `phase`.
+static void enqueue_step(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*tick)(void*, int, cudaStream_t)) {
+  k_begin<<<1, 1, 0, s>>>(c->st.p);
+  for (int p = 0; p < c->P.nfam; ++p) launch_dt(c, p, phase, s);
+  k_time<<<1, 1, 0, s>>>(c->st.p, c->P.time_accurate);
+  if (tick) tick(c, KC_DT, s);
+  for (int p = 0; p < c->P.nfam; ++p)
+    for (int srk = 1; srk <= c->P.nrk; ++srk) launch_family(c, p, srk, phase, s, tick);
+}
+
+static void prof_tick(void* vc, int cls, cudaStream_t s) {
+  ice_gpu_ctx* c = (ice_gpu_ctx*)vc;
+  cudaEventRecord(c->ev1, s);
+  cudaEventSynchronize(c->ev1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->kms[cls] += ms;
+  cudaEventRecord(c->ev0, s);
+}
+
+static long long launches_per_step(const ice_gpu_ctx* c) {
+  long long n = 2 + c->P.nfam;
+  for (int p = 0; p < c->P.nfam; ++p) {
+    const FamHost& H = c->fam[p];
+    long long per = (H.nrec > 0 ? 2 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0);
+    per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
+    n += per * c->P.nrk;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------- set-up helpers
+static void tile_shape(int ndir, int& TX, int& TY, int& TZ) {
+  if (ndir == 1) { TX = 256; TY = 1; TZ = 1; }
+  else if (ndir == 2) { TX = 32; TY = 8; TZ = 1; }
+  else { TX = 32; TY = 4; TZ = 2; }
+}
+
+static int build_tiles(ice_gpu_ctx* c) {
+  tile_shape(c->P.ndir, c->TX, c->TY, c->TZ);
+  std::vector<Tile> t;
+  for (int b = 0; b < c->nb; ++b) {
+    int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
+    for (int k = 0; k < nk; k += c->TZ)
+      for (int j = 0; j < nj; j += c->TY)
+        for (int i = 0; i < ni; i += c->TX) t.push_back(Tile{b, i, j, k});
+  }
+  c->ntile = (int)t.size();
+  CK(c->tiles.alloc(t.size()));
+  CK(cudaMemcpy(c->tiles.p, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  // norm chunks: 2048 cells of one block each
+  std::vector<NormChunk> ch;
+  c->chunk_block.clear();
+  for (int b = 0; b < c->nb; ++b) {
+    long long n = (long long)c->dims[3 * b] * c->dims[3 * b + 1] * c->dims[3 * b + 2];
+    for (long long q = 0; q < n; q += 2048) {
+      ch.push_back(NormChunk{b, c->hblk[b].ioff + q, c->hblk[b].ioff + std::min(n, q + 2048)});
+      c->chunk_block.push_back(b);
+    }
+  }
+  c->nchunk = (int)ch.size();
+  CK(c->chunks.alloc(ch.size()));
+  CK(cudaMemcpy(c->chunks.p, ch.data(), ch.size() * sizeof(NormChunk), cudaMemcpyHostToDevice));
+  CK(c->npart.alloc((size_t)c->nchunk * 5));
+  return 0;
+}
+
+extern "C" {
+
+int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims, ice_gpu_ctx** out) {
+  ice_gpu_ctx* c = nullptr;
+  if (!P || !dims || !out || nblocks < 1) return fail(nullptr, ICE_GPU_EINVAL, "create: null argument or no block");
+  if (P->nfam < 1 || P->nfam > kMaxF) return fail(nullptr, ICE_GPU_EINVAL, "create: nfam %d out of 1..%d", P->nfam, kMaxF);
+  if (P->nrk < 1 || P->nrk > 3) return fail(nullptr, ICE_GPU_EINVAL, "create: nrk %d", P->nrk);
+  if (P->ndir < 1 || P->ndir > 3) return fail(nullptr, ICE_GPU_EINVAL, "create: ndir %d", P->ndir);
+  for (int p = 0; p < P->nfam; ++p) {
+    const ice_gpu_family& f = P->fam[p];
+    if (f.closure < 1 || f.closure > 3) return fail(nullptr, ICE_GPU_EINVAL, "family %d: closure %d", p + 1, f.closure);
+    if (f.riemann == ICE_RIEMANN_SAUREL && f.closure != ICE_CLOSURE_MK)
+      return fail(nullptr, ICE_GPU_EINVAL, "family %d: riemann-solver = Saurel is specific to the MK closure; use Rusanov or HLLE", p + 1);
+    if (f.liq != 0 || f.boil != 0)
+      return fail(nullptr, ICE_GPU_EINVAL, "family %d: liquid-conduction P2T and boiling ZGR are not supported", p + 1);
+  }
+  if (P->irs && P->time_accurate)
+    return fail(nullptr, ICE_GPU_EINVAL, "irs = true needs time-accurate = false (Assign_Setup.f90:79-83)");
+  std::unique_ptr<ice_gpu_ctx> u(new ice_gpu_ctx);
+  c = u.get();
+  c->P = *P;
+  c->nb = nblocks;
+  c->dims.assign(dims, dims + 3 * nblocks);
+  c->have_block.assign(nblocks, false);
+  long long G = 0, I = 0, R = 0, F0 = 0, F1 = 0, F2 = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    int ni = dims[3 * b], nj = dims[3 * b + 1], nk = dims[3 * b + 2];
+    if (ni < 1 || nj < 1 || nk < 1) return fail(nullptr, ICE_GPU_EINVAL, "block %d: dims %d %d %d", b + 1, ni, nj, nk);
+    DBlock B;
+    B.ni = ni; B.nj = nj; B.nk = nk; B.pad = 0;
+    B.goff = G; B.ioff = I; B.roff = R; B.foff[0] = F0; B.foff[1] = F1; B.foff[2] = F2;
+    G += (long long)(ni + 4) * (nj + 4) * (nk + 4);
+    I += (long long)ni * nj * nk;
+    R += (long long)(ni + 2) * (nj + 2) * (nk + 2);
+    F0 += (long long)(ni + 1) * nj * nk; F1 += (long long)ni * (nj + 1) * nk; F2 += (long long)ni * nj * (nk + 1);
+    c->hblk.push_back(B);
+  }
+  c->NG = G; c->NI = I; c->NR = R; c->NF[0] = F0; c->NF[1] = F1; c->NF[2] = F2;
+  cudaError_t e;
+#define CKC(call) do { e = (call); if (e != cudaSuccess) return fail(nullptr, ICE_GPU_ECUDA, "%s: %s", #call, cudaGetErrorString(e)); } while (0)
+  CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CKC(c->blk.alloc(nblocks));
+  CKC(cudaMemcpy(c->blk.p, c->hblk.data(), nblocks * sizeof(DBlock), cudaMemcpyHostToDevice));
+  for (int d = 0; d < 3; ++d) CKC(c->face[d].alloc((size_t)4 * c->NF[d]));
+  CKC(c->vol.alloc(I));
+  CKC(c->dl.alloc((size_t)3 * R));
+  CKC(c->M.alloc((size_t)9 * I));
+  if (P->coupled) CKC(c->gas.alloc((size_t)9 * I));
+  for (int p = 0; p < P->nfam; ++p) {
+    FamHost& H = c->fam[p];
+    H.closure = P->fam[p].closure; H.riemann = P->fam[p].riemann; H.nc = nbase_of(H.closure);
+    for (int s = 0; s < 3; ++s) {
+      CKC(H.S[s].alloc((size_t)H.nc * G));
+      // poison: a ghost cell no record fills stays NaN, as Allocate_Block leaves it
+      CKC(cudaMemset(H.S[s].p, 0xFF, sizeof(double) * H.nc * G));
+    }
+    CKC(H.inj.alloc(G)); CKC(cudaMemset(H.inj.p, 0, G));
+    CKC(H.dt.alloc(I));
+    CKC(H.tau.alloc(I));
+    std::vector<double> inf(I, INFINITY);
+    CKC(cudaMemcpy(H.tau.p, inf.data(), I * sizeof(double), cudaMemcpyHostToDevice));
+    CKC(H.beta.alloc(I));
+    std::vector<double> one(I, 1.0);
+    CKC(cudaMemcpy(H.beta.p, one.data(), I * sizeof(double), cudaMemcpyHostToDevice));
+    CKC(H.bmap.alloc(I)); CKC(cudaMemset(H.bmap.p, 0xFF, I * sizeof(int)));
+    if (P->irs) { CKC(H.resid.alloc((size_t)H.nc * I)); CKC(H.resid2.alloc((size_t)H.nc * I)); CKC(H.resid3.alloc((size_t)H.nc * I)); }
+  }
+  CKC(c->st.alloc(1));
+  Status s0; memset(&s0, 0, sizeof s0);
+  CKC(cudaMemcpy(c->st.p, &s0, sizeof s0, cudaMemcpyHostToDevice));
+  CKC(cudaEventCreate(&c->ev0)); CKC(cudaEventCreate(&c->ev1));
+#undef CKC
+  if (build_tiles(c)) { g_create_err = c->err; return ICE_GPU_ECUDA; }
+  *out = u.release();
+  return 0;
+}
+
+int ice_gpu_destroy(ice_gpu_ctx* c) {
+  if (!c) return 0;
+  cudaStreamSynchronize(c->stream);
+  free_graphs(c);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int ice_gpu_last_error(const ice_gpu_ctx* c, char* buf, int32_t n) {
+  if (!buf || n <= 0) return ICE_GPU_EINVAL;
+  const std::string& s = c ? c->err : g_create_err;
+  strncpy(buf, s.c_str(), n - 1); buf[n - 1] = 0;
+  return 0;
+}
+
+int ice_gpu_set_block(ice_gpu_ctx* c, int32_t b1, const double* f1, const double* f2, const double* f3,
+                      const double* vol, const double* dl, const double* M) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (b1 < 1 || b1 > c->nb) return fail(c, ICE_GPU_EINVAL, "set_block: block %d out of range", b1);
+  if (!f1 || !f2 || !f3 || !vol || !dl || !M) return fail(c, ICE_GPU_EINVAL, "set_block: null array");
+  const DBlock& B = c->hblk[b1 - 1];
+  int ni = B.ni, nj = B.nj, nk = B.nk;
+  const double* fs[3] = {f1, f2, f3};
+  long long nf[3] = {(long long)(ni + 1) * nj * nk, (long long)ni * (nj + 1) * nk, (long long)ni * nj * (nk + 1)};
+  std::vector<double> tmp;
+  for (int d = 0; d < 3; ++d) {
+    tmp.resize(nf[d]);
+    for (int comp = 0; comp < 4; ++comp) {
+      for (long long q = 0; q < nf[d]; ++q) tmp[q] = fs[d][4 * q + comp];
+      CK(cudaMemcpy(c->face[d].p + (long long)comp * c->NF[d] + B.foff[d], tmp.data(), nf[d] * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  }
+  long long ncell = (long long)ni * nj * nk, nring = (long long)(ni + 2) * (nj + 2) * (nk + 2);
+  CK(cudaMemcpy(c->vol.p + B.ioff, vol, ncell * sizeof(double), cudaMemcpyHostToDevice));
+  tmp.resize(nring);
+  for (int comp = 0; comp < 3; ++comp) {
+    for (long long q = 0; q < nring; ++q) tmp[q] = dl[3 * q + comp];
+    CK(cudaMemcpy(c->dl.p + (long long)comp * c->NR + B.roff, tmp.data(), nring * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  // M on the interior cells only (compute_dt reads nothing else)
+  tmp.resize(ncell);
+  for (int comp = 0; comp < 9; ++comp) {
+    for (int k = 0; k < nk; ++k) for (int j = 0; j < nj; ++j) for (int i = 0; i < ni; ++i) {
+      long long r = ((long long)(k + 1) * (nj + 2) + (j + 1)) * (ni + 2) + (i + 1);
+      tmp[((long long)k * nj + j) * ni + i] = M[9 * r + comp];
+    }
+    CK(cudaMemcpy(c->M.p + (long long)comp * c->NI + B.ioff, tmp.data(), ncell * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  c->have_block[b1 - 1] = true;
+  return 0;
+}
+
+int ice_gpu_set_gas(ice_gpu_ctx* c, int32_t b1, const double* prim5, const double* R, const double* gam,
+                    const double* k, const double* mu) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (!c->P.coupled) return fail(c, ICE_GPU_EINVAL, "set_gas: the run is not coupled");
+  if (b1 < 1 || b1 > c->nb) return fail(c, ICE_GPU_EINVAL, "set_gas: block %d out of range", b1);
+  const DBlock& B = c->hblk[b1 - 1];
+  long long n = (long long)B.ni * B.nj * B.nk;
+  std::vector<double> tmp(n);
+  for (int comp = 0; comp < 5; ++comp) {
+    for (long long q = 0; q < n; ++q) tmp[q] = prim5[5 * q + comp];
+    CK(cudaMemcpy(c->gas.p + (long long)comp * c->NI + B.ioff, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const double* rest[4] = {R, gam, k, mu};
+  for (int comp = 0; comp < 4; ++comp)
+    CK(cudaMemcpy(c->gas.p + (long long)(5 + comp) * c->NI + B.ioff, rest[comp], n * sizeof(double), cudaMemcpyHostToDevice));
+  c->have_gas = true;
+  return 0;
+}
+
+int ice_gpu_upload_state(ice_gpu_ctx* c, int32_t b1, int32_t p1, const double* prim, const uint8_t* inj) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam) return fail(c, ICE_GPU_EINVAL, "upload_state: bad block/family");
+  if (!prim) return fail(c, ICE_GPU_EINVAL, "upload_state: null prim");
+  const DBlock& B = c->hblk[b1 - 1];
+  FamHost& H = c->fam[p1 - 1];
+  long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
+  std::vector<double> tmp(ng);
+  CK(cudaStreamSynchronize(c->stream));
+  for (int v = 0; v < H.nc; ++v) {
+    for (long long q = 0; q < ng; ++q) tmp[q] = prim[(long long)H.nc * q + v];
+    CK(cudaMemcpy(H.S[c->phase].p + (long long)v * c->NG + B.goff, tmp.data(), ng * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (inj) CK(cudaMemcpy(H.inj.p + B.goff, inj, ng, cudaMemcpyHostToDevice));
+  c->prev_phase = -1;
+  return 0;
+}
+
+int ice_gpu_download_state(ice_gpu_ctx* c, int32_t b1, int32_t p1, double* prim) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam) return fail(c, ICE_GPU_EINVAL, "download_state: bad block/family");
+  const DBlock& B = c->hblk[b1 - 1];
+  FamHost& H = c->fam[p1 - 1];
+  long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
+  std::vector<double> tmp(ng);
+  CK(cudaStreamSynchronize(c->stream));
+  for (int v = 0; v < H.nc; ++v) {
+    CK(cudaMemcpy(tmp.data(), H.S[c->phase].p + (long long)v * c->NG + B.goff, ng * sizeof(double), cudaMemcpyDeviceToHost));
+    for (long long q = 0; q < ng; ++q) prim[(long long)H.nc * q + v] = tmp[q];
+  }
+  return 0;
+}
+
+int ice_gpu_set_time(ice_gpu_ctx* c, double time, int32_t iter, int32_t iter_from_call) {
+  if (!c) return ICE_GPU_EINVAL;
+  Status s;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(&s, c->st.p, sizeof s, cudaMemcpyDeviceToHost));
+  s.time = time; s.iter = iter; s.iter_from_call = iter_from_call;
+  CK(cudaMemcpy(c->st.p, &s, sizeof s, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int ice_gpu_update_params(ice_gpu_ctx* c, const ice_gpu_params* P) {
+  if (!c || !P) return ICE_GPU_EINVAL;
+  if (P->nfam != c->P.nfam || P->ndir != c->P.ndir) return fail(c, ICE_GPU_EINVAL, "update_params: nfam and ndir may not change");
+  for (int p = 0; p < P->nfam; ++p) {
+    if (P->fam[p].closure != c->P.fam[p].closure) return fail(c, ICE_GPU_EINVAL, "update_params: closures may not change");
+    if (P->fam[p].riemann == ICE_RIEMANN_SAUREL && P->fam[p].closure != ICE_CLOSURE_MK)
+      return fail(c, ICE_GPU_EINVAL, "update_params: Saurel is specific to MK");
+  }
+  if (P->irs && P->time_accurate) return fail(c, ICE_GPU_EINVAL, "update_params: irs needs a steady run");
+  if (P->irs && !c->P.irs) {
+    for (int p = 0; p < c->P.nfam; ++p) {
+      FamHost& H = c->fam[p];
+      CK(H.resid.alloc((size_t)H.nc * c->NI)); CK(H.resid2.alloc((size_t)H.nc * c->NI)); CK(H.resid3.alloc((size_t)H.nc * c->NI));
+    }
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->P = *P;
+  for (int p = 0; p < c->P.nfam; ++p) c->fam[p].riemann = P->fam[p].riemann;
+  free_graphs(c);
+  return 0;
+}
+
+// build_local_bc_index + collect_boundary_cells + collect_owner_records
+// (parallel/Mod_GhostExchange.f90:103-360) for a device that owns every block.
+int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const double* rr) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (nrec < 0 || (nrec > 0 && (!ri || !rr))) return fail(c, ICE_GPU_EINVAL, "set_records: bad arguments");
+  c->recs.resize(nrec);
+  for (int n = 0; n < nrec; ++n) {
+    const int32_t* q = ri + (long long)n * ICE_GPU_REC_INTS;
+    const double* x = rr + (long long)n * ICE_GPU_REC_REALS;
+    HRec& r = c->recs[n];
+    r.b = q[0]; r.i = q[1]; r.j = q[2]; r.k = q[3]; r.f = q[4]; r.type = q[5]; r.p = q[6];
+    r.bs = q[7]; r.is = q[8]; r.js = q[9]; r.ks = q[10]; r.fs = q[11]; r.partner = q[12]; r.owner = q[13]; r.cf = q[14];
+    r.massflux = x[0]; r.velocity = x[1]; r.alpha = x[2]; r.beta = x[3]; r.temperature = x[4]; r.radius = x[5];
+    r.gfixed = x[6]; r.normal_dir = x[7];
+    if (r.b < 1 || r.b > c->nb || r.p < 1 || r.p > c->P.nfam || r.f < 1 || r.f > 6)
+      return fail(c, ICE_GPU_EINVAL, "record %d: bad block, family or face", n + 1);
+    const int* d = &c->dims[3 * (r.b - 1)];
+    if (r.i < 1 || r.i > d[0] || r.j < 1 || r.j > d[1] || r.k < 1 || r.k > d[2])
+      return fail(c, ICE_GPU_EINVAL, "record %d: cell %d %d %d outside block %d", n + 1, r.i, r.j, r.k, r.b);
+    {
+      const int ijk[3] = {r.i, r.j, r.k};
+      int dd = (r.f - 1) / 2;
+      if (ijk[dd] != (r.f % 2 == 1 ? 1 : d[dd]))
+        return fail(c, ICE_GPU_EINVAL, "record %d: cell %d %d %d is off its face %d", n + 1, r.i, r.j, r.k, r.f);
+    }
+    int t = r.type;
+    bool known = t == 0 || t == 101 || t == 201 || t == 200 || t == 300 || t == 301 || t == 400 || (t >= 401 && t <= 403);
+    if (!known) return fail(c, ICE_GPU_EINVAL, "record %d: boundary code %d is not supported on the device", n + 1, t);
+    if (t == 101 || t == 201) {
+      if (r.bs < 1 || r.bs > c->nb) return fail(c, ICE_GPU_EINVAL, "record %d: source block %d", n + 1, r.bs);
+      if (r.fs < 1 || r.fs > 6) return fail(c, ICE_GPU_EINVAL, "record %d: source face %d", n + 1, r.fs);
+      const int* ds = &c->dims[3 * (r.bs - 1)];
+      int g0 = (r.fs == 1) - (r.fs == 2), g1 = (r.fs == 3) - (r.fs == 4), g2 = (r.fs == 5) - (r.fs == 6);
+      int s1[3] = {r.is, r.js, r.ks}, s2[3] = {r.is + g0, r.js + g1, r.ks + g2};
+      for (int a = 0; a < 3; ++a)
+        if (s1[a] < 1 || s1[a] > ds[a] || s2[a] < 1 || s2[a] > ds[a])
+          return fail(c, ICE_GPU_EINVAL, "record %d: the two source cells of its ghosts are not inside block %d", n + 1, r.bs);
+      if (r.partner < 1 || r.partner > nrec || r.cf < 1) return fail(c, ICE_GPU_EINVAL, "record %d: connection not paired", n + 1);
+    }
+    if ((t >= 401 && t <= 403) && t != 402 && !c->P.coupled)
+      return fail(c, ICE_GPU_EINVAL, "record %d: inlet %d takes its speed from the gas, and the run has no gas", n + 1, t);
+  }
+  for (int p = 0; p < c->P.nfam; ++p) {
+    FamHost& H = c->fam[p];
+    // the family's records in table order
+    std::vector<int> grp;
+    for (int n = 0; n < nrec; ++n) if (c->recs[n].p == p + 1) grp.push_back(n);
+    std::vector<int> pos(nrec, -1);
+    for (size_t q = 0; q < grp.size(); ++q) pos[grp[q]] = (int)q;
+    std::vector<DRec> dr(grp.size());
+    int ncf = 0;
+    for (size_t q = 0; q < grp.size(); ++q) {
+      const HRec& r = c->recs[grp[q]];
+      DRec& d = dr[q];
+      d.b = r.b - 1; d.i = r.i - 1; d.j = r.j - 1; d.k = r.k - 1; d.f = r.f; d.type = r.type;
+      d.bs = r.bs - 1; d.is = r.is - 1; d.js = r.js - 1; d.ks = r.ks - 1; d.fs = r.fs;
+      d.owner = r.owner; d.cf = r.cf - 1;
+      if (r.type == 101 || r.type == 201) {
+        const HRec& q2 = c->recs[r.partner - 1];
+        d.pb = q2.b - 1; d.pi = q2.i - 1; d.pj = q2.j - 1; d.pk = q2.k - 1;
+        ncf = std::max(ncf, r.cf);
+      } else { d.pb = d.pi = d.pj = d.pk = 0; }
+      d.normal_dir = r.normal_dir != 0.0;
+      d.massflux = r.massflux; d.velocity = r.velocity; d.alpha = r.alpha; d.beta = r.beta;
+      d.temperature = r.temperature; d.radius = r.radius; d.gfixed = r.gfixed;
+    }
+    H.nrec = (int)grp.size();
+    CK(H.recs.alloc(dr.size()));
+    if (!dr.empty()) CK(cudaMemcpy(H.recs.p, dr.data(), dr.size() * sizeof(DRec), cudaMemcpyHostToDevice));
+    // boundary cells: block by block in cell order, the records of a cell by face (stable)
+    H.h_first.clear(); H.h_list.clear();
+    std::vector<int> bmap(c->NI, -1);
+    for (int b = 0; b < c->nb; ++b) {
+      const DBlock& B = c->hblk[b];
+      long long ncell = (long long)B.ni * B.nj * B.nk;
+      std::vector<int> head(ncell, -1), tail(ncell, -1), next(nrec, -1);
+      for (int n : grp) {
+        const HRec& r = c->recs[n];
+        if (r.b != b + 1 || r.type == 0) continue;
+        long long q = ((long long)(r.k - 1) * B.nj + (r.j - 1)) * B.ni + (r.i - 1);
+        if (head[q] < 0) head[q] = n; else next[tail[q]] = n;
+        tail[q] = n;
+      }
+      for (long long q = 0; q < ncell; ++q) {
+        if (head[q] < 0) continue;
+        bmap[B.ioff + q] = (int)H.h_first.size();
+        int s0 = (int)H.h_list.size();
+        H.h_first.push_back(s0);
+        for (int n = head[q]; n >= 0; n = next[n]) H.h_list.push_back(n);
+        for (size_t m = s0 + 1; m < H.h_list.size(); ++m) {
+          int n = H.h_list[m]; long long l = (long long)m - 1;
+          while (l >= s0 && c->recs[H.h_list[l]].f > c->recs[n].f) { H.h_list[l + 1] = H.h_list[l]; --l; }
+          H.h_list[l + 1] = n;
+        }
+      }
+    }
+    H.nbc = (int)H.h_first.size();
+    H.h_first.push_back((int)H.h_list.size());
+    std::vector<int> dlist(H.h_list.size());
+    for (size_t q = 0; q < H.h_list.size(); ++q) dlist[q] = pos[H.h_list[q]];
+    CK(H.bfirst.alloc(H.h_first.size()));
+    CK(cudaMemcpy(H.bfirst.p, H.h_first.data(), H.h_first.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(H.blist.alloc(std::max<size_t>(dlist.size(), 1)));
+    if (!dlist.empty()) CK(cudaMemcpy(H.blist.p, dlist.data(), dlist.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(H.bmap.p, bmap.data(), c->NI * sizeof(int), cudaMemcpyHostToDevice));
+    CK(H.Rb.alloc((size_t)std::max(H.nbc, 1) * H.nc));
+    // connection owners, table order
+    H.h_own.clear();
+    for (int n : grp) {
+      const HRec& r = c->recs[n];
+      if ((r.type == 101 || r.type == 201) && r.owner) H.h_own.push_back(n);
+    }
+    H.nown = (int)H.h_own.size();
+    H.ncf = ncf;
+    std::vector<int> down(H.h_own.size());
+    for (size_t q = 0; q < H.h_own.size(); ++q) down[q] = pos[H.h_own[q]];
+    CK(H.own.alloc(std::max<size_t>(down.size(), 1)));
+    if (!down.empty()) CK(cudaMemcpy(H.own.p, down.data(), down.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(H.connF.alloc((size_t)std::max(ncf, 1) * H.nc));
+  }
+  c->have_records = true;
+  free_graphs(c);
+  return 0;
+}
+
+int ice_gpu_index_maps(const ice_gpu_ctx* c, int32_t p1, int32_t* nbcell, int32_t* first, int32_t* nrecs,
+                       int32_t* recs, int32_t* nown, int32_t* own) {
+  if (!c || p1 < 1 || p1 > c->P.nfam || !nbcell || !nrecs || !nown) return ICE_GPU_EINVAL;
+  const FamHost& H = c->fam[p1 - 1];
+  *nbcell = H.nbc; *nrecs = (int)H.h_list.size(); *nown = H.nown;
+  if (first) for (size_t q = 0; q < H.h_first.size(); ++q) first[q] = H.h_first[q] + 1;
+  if (recs) for (size_t q = 0; q < H.h_list.size(); ++q) recs[q] = H.h_list[q] + 1;
+  if (own) for (size_t q = 0; q < H.h_own.size(); ++q) own[q] = H.h_own[q] + 1;
+  return 0;
+}
+
+static int check_ready(ice_gpu_ctx* c) {
+  for (int b = 0; b < c->nb; ++b) if (!c->have_block[b]) return fail(c, ICE_GPU_ENOTREADY, "block %d has no metrics", b + 1);
+  if (!c->have_records) return fail(c, ICE_GPU_ENOTREADY, "no boundary table");
+  if (c->P.coupled && !c->have_gas) return fail(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas");
+  return 0;
+}
+
+int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (int rc = check_ready(c)) return rc;
+  if (nsteps < 0) return fail(c, ICE_GPU_EINVAL, "step: nsteps %d", nsteps);
+  cudaStream_t s = c->stream;
+  if (c->profiling) {
+    for (double& x : c->kms) x = 0.0;
+    c->nlaunch = 0;
+  }
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  CK(cudaEventCreate(&t0)); CK(cudaEventCreate(&t1));
+  CK(cudaEventRecord(t0, s));
+  for (int n = 0; n < nsteps; ++n) {
+    int ph = c->phase;
+    if (c->profiling) {
+      CK(cudaEventRecord(c->ev0, s));
+      enqueue_step(c, ph, s, prof_tick);
+      c->nlaunch += launches_per_step(c);
+    } else {
+      if (!c->graph[ph]) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(c, ph, s, nullptr);
+        CK(cudaStreamEndCapture(s, &g));
+        CK(cudaGraphInstantiate(&c->graph[ph], g, 0));
+        cudaGraphDestroy(g);
+      }
+      CK(cudaGraphLaunch(c->graph[ph], s));
+    }
+    c->prev_phase = ph;
+    c->phase = next_phase(c, ph);
+  }
+  CK(cudaEventRecord(t1, s));
+  CK(cudaStreamSynchronize(s));
+  float dms = 0.f;
+  CK(cudaEventElapsedTime(&dms, t0, t1));
+  cudaEventDestroy(t0); cudaEventDestroy(t1);
+  CK(cudaGetLastError());
+  Status h;
+  CK(cudaMemcpy(&h, c->st.p, sizeof h, cudaMemcpyDeviceToHost));
+  int rc = 0;
+  if (out) {
+    out->dtglobal = h.dtglobal; out->time = h.time; out->iter = h.iter; out->status = (int)h.flags;
+    out->nfloored = (int64_t)h.nfloored; out->have_norm = 0;
+    bool endsim = h.iter_from_call >= c->P.itermax || h.time >= c->P.time_threshold;
+    bool iosim = c->P.sol_diter > 0 && h.iter % c->P.sol_diter == 0;
+    out->todo = endsim ? 3 : iosim ? 2 : 1;
+    for (int m = 0; m < 5; ++m) out->residual[m] = 0.0;
+    out->device_ms = dms;
+  }
+  if (h.flags & (ICE_GPU_ST_NAN_STATE | ICE_GPU_ST_BAD_RECON)) {
+    rc = fail(c, ICE_GPU_ESTATE, "%s", (h.flags & ICE_GPU_ST_NAN_STATE) ?
+              "invalid state after the update (NaN or infinity)" : "unphysical state at first order on a face");
+  }
+  return rc;
+}
+
+int ice_gpu_residual_norm(ice_gpu_ctx* c, double* total, double* fam) {
+  if (!c || !total) return ICE_GPU_EINVAL;
+  if (c->prev_phase < 0) return fail(c, ICE_GPU_ENOTREADY, "residual_norm: no step taken since the state was set");
+  Geo G = make_geo(c);
+  int nf = c->P.nfam;
+  std::vector<double> part((size_t)c->nb * nf * 5, 0.0);
+  std::vector<double> h((size_t)c->nchunk * 5);
+  for (int p = 0; p < nf; ++p) {
+    FamHost& H = c->fam[p];
+    k_norm<<<c->nchunk, 256, 0, c->stream>>>(G, H.S[c->phase].p, H.S[c->prev_phase].p, nbase_of(H.closure) - 2,
+                                             c->chunks.p, c->npart.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h.data(), c->npart.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < c->nchunk; ++q) {
+      double* a = &part[((size_t)c->chunk_block[q] * nf + p) * 5];
+      for (int m = 0; m < 5; ++m) a[m] = a[m] + h[(size_t)q * 5 + m];
+    }
+  }
+  double tot[5] = {0, 0, 0, 0, 0};
+  for (int b = 0; b < c->nb; ++b) for (int p = 0; p < nf; ++p) for (int m = 0; m < 5; ++m) tot[m] = tot[m] + part[((size_t)b * nf + p) * 5 + m];
+  for (int m = 0; m < 5; ++m) total[m] = sqrt(tot[m]);
+  if (fam) {
+    for (int p = 0; p < nf; ++p) {
+      double f[5] = {0, 0, 0, 0, 0};
+      for (int b = 0; b < c->nb; ++b) for (int m = 0; m < 5; ++m) f[m] = f[m] + part[((size_t)b * nf + p) * 5 + m];
+      for (int m = 0; m < 5; ++m) fam[p * 5 + m] = sqrt(f[m]);
+    }
+  }
+  return 0;
+}
+
+int ice_gpu_set_profiling(ice_gpu_ctx* c, int32_t on) {
+  if (!c) return ICE_GPU_EINVAL;
+  c->profiling = on != 0;
+  return 0;
+}
+
+int ice_gpu_kernel_times(const ice_gpu_ctx* c, double* ms, int32_t nclass, int64_t* nlaunch) {
+  if (!c) return ICE_GPU_EINVAL;
+  for (int q = 0; q < nclass && q < KC_N; ++q) ms[q] = c->kms[q];
+  if (nlaunch) *nlaunch = c->profiling ? c->nlaunch : 0;
+  return 0;
+}
+
+// Pair_Connections (io/IO_BC.f90:360-510)
+int ice_gpu_pair_connections(int32_t nb, const int32_t* dims, int32_t ngroups, int32_t nrec, int32_t* rec,
+                             char* err, int32_t errlen) {
+  auto R = [&](int n, int f) -> int32_t& { return rec[(long long)n * ICE_GPU_REC_INTS + f]; };
+  enum { Fb, Fi, Fj, Fk, Ff, Ftype, Fp, Fbs, Fis, Fjs, Fks, Ffs, Fpartner, Fowner, Fcf };
+  auto tang = [](int f, int i, int j, int k, int* t) {
+    if (f <= 2) { t[0] = j; t[1] = k; } else if (f <= 4) { t[0] = i; t[1] = k; } else { t[0] = i; t[1] = j; }
+  };
+  auto msg = [&](const char* fmt, int a, int b2) {
+    if (err && errlen > 0) snprintf(err, errlen, fmt, a, b2);
+    return ICE_GPU_EINVAL;
+  };
+  if (nb < 1 || ngroups < 1 || nrec < 0 || !dims || (nrec > 0 && !rec)) return msg("bad arguments (%d %d)", nb, ngroups);
+  for (int n = 0; n < nrec; ++n)
+    if (R(n, Ftype) == 101 || R(n, Ftype) == 201) { R(n, Fpartner) = 0; R(n, Fowner) = 0; R(n, Fcf) = 0; }
+  for (int p = 1; p <= ngroups; ++p) {
+    std::vector<std::vector<int>> map((size_t)nb * 6);
+    std::vector<int> mdim((size_t)nb * 12, 0);
+    for (int n = p - 1; n < nrec; n += ngroups) {
+      int ty = R(n, Ftype);
+      if (ty != 101 && ty != 201) continue;
+      int b = R(n, Fb), f = R(n, Ff), t[2], nt[2];
+      if (b < 1 || b > nb || f < 1 || f > 6) return msg("record %d: bad block or face %d", n + 1, f);
+      size_t key = (size_t)(b - 1) * 6 + (f - 1);
+      if (map[key].empty()) {
+        tang(f, dims[3 * (b - 1)], dims[3 * (b - 1) + 1], dims[3 * (b - 1) + 2], nt);
+        map[key].assign((size_t)nt[0] * nt[1], 0);
+        mdim[2 * key] = nt[0]; mdim[2 * key + 1] = nt[1];
+      }
+      tang(f, R(n, Fi), R(n, Fj), R(n, Fk), t);
+      if (t[0] < 1 || t[1] < 1 || t[0] > mdim[2 * key] || t[1] > mdim[2 * key + 1]) return msg("record %d: cell off its face %d", n + 1, f);
+      map[key][(size_t)(t[1] - 1) * mdim[2 * key] + (t[0] - 1)] = n + 1;
+    }
+    for (int n = p - 1; n < nrec; n += ngroups) {
+      int ty = R(n, Ftype);
+      if (ty != 101 && ty != 201) continue;
+      int b = R(n, Fbs), f = R(n, Ffs), q = 0, t[2];
+      if (b >= 1 && b <= nb && f >= 1 && f <= 6) {
+        size_t key = (size_t)(b - 1) * 6 + (f - 1);
+        if (!map[key].empty()) {
+          tang(f, R(n, Fis), R(n, Fjs), R(n, Fks), t);
+          if (t[0] >= 1 && t[1] >= 1 && t[0] <= mdim[2 * key] && t[1] <= mdim[2 * key + 1])
+            q = map[key][(size_t)(t[1] - 1) * mdim[2 * key] + (t[0] - 1)];
+        }
+      }
+      if (q) {
+        int qq = q - 1;
+        if (R(qq, Fi) != R(n, Fis) || R(qq, Fj) != R(n, Fjs) || R(qq, Fk) != R(n, Fks)) q = 0;
+      }
+      if (!q) return msg("record %d points at no connection record of its family (face %d)", n + 1, f);
+      if (q == n + 1) return msg("record %d points at its own cell and face %d", n + 1, f);
+      int qq = q - 1;
+      if (R(qq, Ftype) != ty || R(qq, Fbs) != R(n, Fb) || R(qq, Ffs) != R(n, Ff) || R(qq, Fis) != R(n, Fi) ||
+          R(qq, Fjs) != R(n, Fj) || R(qq, Fks) != R(n, Fk))
+        return msg("records %d and %d do not point at each other", n + 1, q);
+      int across = dims[3 * (b - 1) + (f + 1) / 2 - 1];
+      if (across < 2) return msg("record %d: the block across has %d cell across its face", n + 1, across);
+      R(n, Fpartner) = q;
+      int fn = R(n, Ff), fq = R(qq, Ff);
+      if (fn % 2 == 0 && fq % 2 == 1) R(n, Fowner) = 1;
+      else if (fn % 2 == 1 && fq % 2 == 0) R(n, Fowner) = 0;
+      else {
+        int k1[5] = {R(n, Fb), R(n, Ff), R(n, Fk), R(n, Fj), R(n, Fi)};
+        int k2[5] = {R(qq, Fb), R(qq, Ff), R(qq, Fk), R(qq, Fj), R(qq, Fi)};
+        int less = 0;
+        for (int m = 0; m < 5; ++m) if (k1[m] != k2[m]) { less = k1[m] < k2[m]; break; }
+        R(n, Fowner) = less;
+      }
+    }
+    int nf = 0;
+    for (int n = p - 1; n < nrec; n += ngroups) {
+      int ty = R(n, Ftype);
+      if ((ty != 101 && ty != 201) || !R(n, Fowner)) continue;
+      ++nf;
+      R(n, Fcf) = nf;
+      R(R(n, Fpartner) - 1, Fcf) = nf;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,647 @@
+// ice_kernels.cuh -- the kernels of the solve stage that depend on the closure (and the Riemann
+// solver): per-cell dt, the ghost fill of both layers, connection and boundary fluxes, the fused
+// stage kernel and the separate update of the IRS path. Included by the per-closure units
+// (ice_fam_*.cu) and by ice_gpu.cu, each instantiating what it launches.
+#pragma once
+#include "ice_layout.cuh"
+
+namespace ice {
+namespace {
+
+// ------------------------------------------------------------------ stencil functor
+struct GStencil {            // q(s, v): cell s = 0..3 of the stencil, variable v
+  const double* P; long long NG, g0, st;
+  __device__ __forceinline__ double operator()(int s, int v) const { return __ldg(P + (long long)v * NG + g0 + s * st); }
+};
+
+template <typename R> struct CStencil {        // converted to R (FP32-flux form)
+  const double* P; long long NG, g0, st;
+  __device__ __forceinline__ R operator()(int s, int v) const { return (R)__ldg(P + (long long)v * NG + g0 + s * st); }
+};
+
+// One interior face along d between 0-based cells c (lower, coords ci,cj,ck) and c+1.
+// face_flux + compute_flux_ (Mod_Fluxes.f90:599-685). Returns true on an unphysical
+// first-order face.
+template <int CL, int RS, typename R>
+__device__ __forceinline__ bool face_flux(const Geo& G, const FamDev& F, const DBlock& B, int d, int i, int j, int k,
+                                         R* flux) {
+  constexpr int nc = NC<CL>::v;
+  int c = d == 0 ? i : d == 1 ? j : k;
+  int n = d == 0 ? B.ni : d == 1 ? B.nj : B.nk;
+  int o0 = d == 0, o1 = d == 1, o2 = d == 2;
+  R bf = (R)1;
+  if (F.beta) bf = (R)mn(F.beta[iidx(B, i, j, k)], F.beta[iidx(B, i + o0, j + o1, k + o2)]);
+  R len[4];
+#pragma unroll
+  for (int s = -1; s <= 2; ++s) len[s + 1] = (R)G.dl[(long long)d * G.NR + ridx(B, i + s * o0, j + s * o1, k + s * o2)];
+  if (c == 0 && F.inj[gidx(B, i - o0, j - o1, k - o2)]) len[0] = (R)0;
+  if (c == n - 2 && F.inj[gidx(B, i + 2 * o0, j + 2 * o1, k + 2 * o2)]) len[3] = (R)0;
+  R dl0 = (R)0.5*(len[0] + len[1]), dl1 = (R)0.5*(len[1] + len[2]), dl2 = (R)0.5*(len[2] + len[3]);
+  R dll = (R)0.5*len[1], dlr = (R)0.5*len[2];
+  long long st = gstride(B, d);
+  CStencil<R> q{F.Up, G.NG, gidx(B, i, j, k) - st, st};
+  R pl[nc], pr[nc], fl[nc];
+  bool bad = reconstruct<CL, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
+  long long fi = fidx(B, d, i, j, k, c + 1);
+  long long NF = G.NF[d];
+  R nrm[3] = {(R)G.face[d][fi], (R)G.face[d][NF + fi], (R)G.face[d][2 * NF + fi]};
+  R area = (R)G.face[d][3 * NF + fi];
+  riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
+  return bad;
+}
+
+// record_flux (Mod_BC_Fluxes.f90:180-272): the flux through a record's face into its cell.
+template <int CL, int RS>
+__device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double* flux, const double* beta_face) {
+  constexpr int nc = NC<CL>::v;
+  const DBlock& B = G.blk[r.b];
+  int f = r.f, i = r.i, j = r.j, k = r.k;
+  int g0 = (f == 1) - (f == 2), g1 = (f == 3) - (f == 4), g2 = (f == 5) - (f == 6);  // guide(f,:)
+  int ig = i - g0, jg = j - g1, kg = k - g2;
+  int ig2 = i - 2 * g0, jg2 = j - 2 * g1, kg2 = k - 2 * g2;
+  int ip = i + g0, jp = j + g1, kp = k + g2;
+  int dir = (f + 1) / 2 - 1;
+  double bv = beta_face ? *beta_face : (F.beta ? F.beta[iidx(B, i, j, k)] : 1.0);
+  double dl_g1 = G.dl[(long long)dir * G.NR + ridx(B, ig, jg, kg)];
+  double dl_m = G.dl[(long long)dir * G.NR + ridx(B, i, j, k)];
+  double dl_4 = G.dl[(long long)dir * G.NR + ridx(B, ip, jp, kp)];
+  double dl0, dl1, dl2, dll, dlr;
+  double pl[nc], pr[nc], fl[nc];
+  bool bad;
+  const double* P = F.Up;
+  long long NF = G.NF[dir];
+  if (f % 2 == 1) {
+    long long fi = fidx(B, dir, i, j, k, (dir == 0 ? i : dir == 1 ? j : k));   // the face below the cell
+    double nrm[3] = {G.face[dir][fi], G.face[dir][NF + fi], G.face[dir][2 * NF + fi]};
+    double area = G.face[dir][3 * NF + fi];
+    dl0 = dl_g1; dl1 = 0.5*(dl_g1 + dl_m); dl2 = 0.5*(dl_m + dl_4);
+    dll = 0.5*dl_g1; dlr = 0.5*dl_m;
+    if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = 0.5*dl_m; dll = 0.0; }
+    if (F.inj[gidx(B, ip, jp, kp)]) dl2 = 0.5*dl_m;
+    long long a[4] = {gidx(B, ig2, jg2, kg2), gidx(B, ig, jg, kg), gidx(B, i, j, k), gidx(B, ip, jp, kp)};
+    auto q = [&](int s, int v) { return P[(long long)v * G.NG + a[s]]; };
+    bad = reconstruct<CL, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
+    riemann<CL, RS, double>(pl, pr, nrm, fl, F.mat.cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
+  } else {
+    long long fi = fidx(B, dir, i, j, k, (dir == 0 ? i : dir == 1 ? j : k) + 1);  // the face above the cell
+    double nrm[3] = {G.face[dir][fi], G.face[dir][NF + fi], G.face[dir][2 * NF + fi]};
+    double area = G.face[dir][3 * NF + fi];
+    dl0 = 0.5*(dl_4 + dl_m); dl1 = 0.5*(dl_m + dl_g1); dl2 = dl_g1;
+    dll = 0.5*dl_m; dlr = 0.5*dl_g1;
+    if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = 0.5*dl_m; dlr = 0.0; }
+    if (F.inj[gidx(B, ip, jp, kp)]) dl0 = 0.5*dl_m;
+    long long a[4] = {gidx(B, ip, jp, kp), gidx(B, i, j, k), gidx(B, ig, jg, kg), gidx(B, ig2, jg2, kg2)};
+    auto q = [&](int s, int v) { return P[(long long)v * G.NG + a[s]]; };
+    bad = reconstruct<CL, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
+    riemann<CL, RS, double>(pl, pr, nrm, fl, F.mat.cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) flux[v] = -(fl[v] * area);
+  }
+  return bad;
+}
+
+// ------------------------------------------------------------------ step control
+// Locates the block of interior cell q (flat over every block) by binary search on ioff.
+__device__ __forceinline__ int find_block(const DBlock* blk, int nb, long long q) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (blk[mid].ioff <= q) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void decode(const DBlock& B, long long q, int& i, int& j, int& k) {
+  long long l = q - B.ioff;
+  i = (int)(l % B.ni); l /= B.ni;
+  j = (int)(l % B.nj);
+  k = (int)(l / B.nj);
+}
+
+// compute_dt / compute_dt_ (Mod_dt.f90:11-112, 256-275), every block of one family.
+template <int CL>
+__global__ void __launch_bounds__(256) k_dt(Geo G, FamDev F, Status* st, double cfl, int ramp, double dt_max,
+                                            double tau_factor, int ndir, double* dt_out) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double dt = INFINITY;
+  if (q < G.NI) {
+    const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+    int i, j, k; decode(B, q, i, j, k);
+    constexpr int nc = NC<CL>::v;
+    double p[nc];
+    long long g = gidx(B, i, j, k);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
+    double rate = 0.0;
+    dt = (double)1e+5f;
+    for (int d = 0; d < ndir; ++d) {
+      double t0 = G.M[(long long)d * G.NI + q], t1 = G.M[(long long)(3 + d) * G.NI + q], t2 = G.M[(long long)(6 + d) * G.NI + q];
+      double gn = norm2_3(t0, t1, t2);
+      double vs[3] = {t0 / gn, t1 / gn, t2 / gn};
+      rate = rate + (fabs(p[1]*vs[0] + p[2]*vs[1] + p[3]*vs[2]) + wavespeed<CL>(p, vs)) * gn;
+    }
+    if (rate > 0.0) dt = mn(dt, 1.0/rate);
+    dt = dt * cfl;
+    int it = st->iter;
+    if (it <= ramp) dt = dt * (double)it / (double)ramp;
+    dt = mn(dt, dt_max);
+    if (F.coupled && tau_factor > 0.0) {
+      double tau = F.tau[q];
+      if (p[0] > kRhoEmpty && !not_finite(tau) && tau > 0.0) dt = mn(dt, tau_factor*tau);
+    }
+    if (dt_out) dt_out[q] = dt;
+  }
+  // warp and block min; a positive double orders as its bits
+  unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
+  for (int o = 16; o > 0; o >>= 1) bits = min(bits, __shfl_xor_sync(0xffffffffu, bits, o));
+  __shared__ unsigned long long wmin[8];
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = bits;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = wmin[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = min(m, wmin[w]);
+    atomicMin(&st->dtbits, m);
+  }
+}
+
+// ------------------------------------------------------------------ ghosts
+__device__ __forceinline__ int ghost_rule(const DRec& r, double veln) {
+  int rule = 0;  // copy
+  if (r.type == 200) rule = 1;
+  else if (r.type == 300 || r.type == 301) {
+    if (veln*(double)(1 - 2*(r.f % 2)) <= 0.0 || r.f == 3) rule = 1;
+  } else if (r.type >= 401 && r.type <= 403) {
+    if (!(veln*(double)(1 - 2*(r.f % 2)) > 0.0)) {
+      rule = 2;
+      if (r.massflux == 0.0) rule = 1;
+    }
+  }
+  return rule;
+}
+
+__device__ __forceinline__ void rec_normal(const Geo& G, const DBlock& B, const DRec& r, double* n, double* area) {
+  int d = (r.f - 1) / 2;
+  int F = (d == 0 ? r.i : d == 1 ? r.j : r.k) + 1 - (r.f % 2);   // im - mod(fm,2), 1-based
+  long long fi = fidx(B, d, r.i, r.j, r.k, F);
+  long long NF = G.NF[d];
+  n[0] = G.face[d][fi]; n[1] = G.face[d][NF + fi]; n[2] = G.face[d][2 * NF + fi];
+  if (area) *area = G.face[d][3 * NF + fi];
+}
+
+// ghost_record (Lib_Ghost.f90:76-267), every record type but 102
+template <int CL>
+__global__ void k_ghost1(Geo G, FamDev F, const DRec* recs, int nrec) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nrec) return;
+  constexpr int nc = NC<CL>::v;
+  const DRec r = recs[n];
+  const DBlock& B = G.blk[r.b];
+  int g0 = (r.f == 1) - (r.f == 2), g1 = (r.f == 3) - (r.f == 4), g2 = (r.f == 5) - (r.f == 6);
+  long long gg = gidx(B, r.i - g0, r.j - g1, r.k - g2);
+  long long gm = gidx(B, r.i, r.j, r.k);
+  double* P = F.Ug;
+  const long long NG = G.NG;
+  switch (r.type) {
+    case 101: case 201: {
+      const DBlock& S = G.blk[r.bs];
+      long long gs = gidx(S, r.is, r.js, r.ks);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg] = P[v * NG + gs];
+      break;
+    }
+    case 200: case 300: case 301: {
+      double nrm[3]; rec_normal(G, B, r, nrm, nullptr);
+      double m[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) m[v] = P[v * NG + gm];
+      double gv[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) gv[v] = m[v];
+      double vel[3] = {m[1], m[2], m[3]};
+      double veln = vel[0]*nrm[0] + vel[1]*nrm[1] + vel[2]*nrm[2];
+      if (ghost_rule(r, veln) == 1) {
+        for (int a = 0; a < 3; ++a) vel[a] = vel[a] - 2.0*veln*nrm[a];
+        if constexpr (CL == AG) mirror_tensor(m + 4, nrm, gv + 4);
+      }
+      gv[1] = vel[0]; gv[2] = vel[1]; gv[3] = vel[2];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg] = gv[v];
+      break;
+    }
+    case 0: case 400: {
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg] = P[v * NG + gm];
+      break;
+    }
+    case 401: case 402: case 403: {
+      double nrm[3]; rec_normal(G, B, r, nrm, nullptr);
+      double m[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) m[v] = P[v * NG + gm];
+      double vel[3] = {m[1], m[2], m[3]};
+      double veln = vel[0]*nrm[0] + vel[1]*nrm[1] + vel[2]*nrm[2];
+      int rule = ghost_rule(r, veln);
+      F.inj[gg] = (rule == 2);
+      double gv[nc];
+      if (rule == 0) {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) gv[v] = m[v];
+      } else if (rule == 1) {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) gv[v] = m[v];
+        for (int a = 0; a < 3; ++a) vel[a] = vel[a] - 2.0*veln*nrm[a];
+        gv[1] = vel[0]; gv[2] = vel[1]; gv[3] = vel[2];
+        if constexpr (CL == AG) mirror_tensor(m + 4, nrm, gv + 4);
+      } else {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) gv[v] = 0.0;
+        double sgn = (double)(2*(r.f % 2) - 1);
+        double inward[3] = {sgn*nrm[0], sgn*nrm[1], sgn*nrm[2]};
+        long long q = iidx(B, r.i, r.j, r.k);
+        const double* gas = G.gas;
+        double v3[3], speed;
+        auto injv = [&](double sp) {
+          if (r.normal_dir) { v3[0] = sp*inward[0]; v3[1] = sp*inward[1]; v3[2] = sp*inward[2]; }
+          else { v3[0] = sp*cos(r.beta)*cos(r.alpha); v3[1] = sp*cos(r.beta)*sin(r.alpha); v3[2] = sp*sin(r.beta); }
+        };
+        if (r.type == 401) {
+          double gu = gas[1 * G.NI + q], gvv = gas[2 * G.NI + q], gw = gas[3 * G.NI + q];
+          double vn = gu*inward[0] + gvv*inward[1] + gw*inward[2];
+          injv(r.velocity*vn);
+          gv[1] = v3[0]; gv[2] = v3[1]; gv[3] = v3[2];
+          gv[0] = r.massflux*gas[q]/r.velocity;
+          vn = fabs(gv[1]*nrm[0] + gv[2]*nrm[1] + gv[3]*nrm[2]);
+          if (r.gfixed > 0.0 && vn > 0.0) gv[0] = gv[0] + r.massflux*r.gfixed/vn;
+          gv[nc - 2] = r.temperature*gas[4 * G.NI + q];
+        } else if (r.type == 402) {
+          injv(r.velocity);
+          gv[1] = v3[0]; gv[2] = v3[1]; gv[3] = v3[2];
+          double vn = gv[1]*nrm[0] + gv[2]*nrm[1] + gv[3]*nrm[2];
+          gv[0] = r.massflux/fabs(vn);
+          gv[nc - 2] = r.temperature;
+        } else {
+          speed = norm2_3(gas[1 * G.NI + q], gas[2 * G.NI + q], gas[3 * G.NI + q]);
+          injv(r.velocity*speed);
+          gv[1] = v3[0]; gv[2] = v3[1]; gv[3] = v3[2];
+          double vn = gv[1]*nrm[0] + gv[2]*nrm[1] + gv[3]*nrm[2];
+          gv[0] = r.massflux/fabs(vn);
+          gv[nc - 2] = r.temperature;
+        }
+        gv[nc - 1] = gv[0]/F.mat.rho/(4.0/3.0*kPi*pow(r.radius, 3.0));
+        if constexpr (CL == IG) gv[4] = 1e-6;
+        if constexpr (CL == AG) { gv[4] = 1e-6; gv[7] = 1e-6; gv[9] = 1e-6; }
+      }
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg] = gv[v];
+      break;
+    }
+    default: break;
+  }
+}
+
+// second_ghost_record (Lib_Ghost.f90:312-387)
+template <int CL>
+__global__ void k_ghost2(Geo G, FamDev F, const DRec* recs, int nrec) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nrec) return;
+  constexpr int nc = NC<CL>::v;
+  const DRec r = recs[n];
+  if (r.type == 0) return;
+  const DBlock& B = G.blk[r.b];
+  int g0 = (r.f == 1) - (r.f == 2), g1 = (r.f == 3) - (r.f == 4), g2 = (r.f == 5) - (r.f == 6);
+  long long gg1 = gidx(B, r.i - g0, r.j - g1, r.k - g2);
+  long long gg2 = gidx(B, r.i - 2 * g0, r.j - 2 * g1, r.k - 2 * g2);
+  long long gm = gidx(B, r.i, r.j, r.k);
+  long long gp = gidx(B, r.i + g0, r.j + g1, r.k + g2);
+  double* P = F.Ug;
+  const long long NG = G.NG;
+  switch (r.type) {
+    case 101: case 201: {
+      const DBlock& S = G.blk[r.bs];
+      int s0 = (r.fs == 1) - (r.fs == 2), s1 = (r.fs == 3) - (r.fs == 4), s2 = (r.fs == 5) - (r.fs == 6);
+      long long gs = gidx(S, r.is + s0, r.js + s1, r.ks + s2);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg2] = P[v * NG + gs];
+      break;
+    }
+    case 200: case 300: case 301: case 401: case 402: case 403: {
+      double nrm[3]; rec_normal(G, B, r, nrm, nullptr);
+      double m1 = P[1 * NG + gm], m2 = P[2 * NG + gm], m3 = P[3 * NG + gm];
+      double veln = m1*nrm[0] + m2*nrm[1] + m3*nrm[2];
+      int rule = ghost_rule(r, veln);
+      double gv[nc];
+      if (rule == 2) {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) gv[v] = P[v * NG + gg1];
+      } else {
+        double mp[nc];
+#pragma unroll
+        for (int v = 0; v < nc; ++v) { mp[v] = P[v * NG + gp]; gv[v] = mp[v]; }
+        if (rule == 1) {
+          double d = mp[1]*nrm[0] + mp[2]*nrm[1] + mp[3]*nrm[2];
+          for (int a = 0; a < 3; ++a) gv[1 + a] = mp[1 + a] - 2.0*d*nrm[a];
+          if constexpr (CL == AG) mirror_tensor(mp + 4, nrm, gv + 4);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg2] = gv[v];
+      break;
+    }
+    default: {
+#pragma unroll
+      for (int v = 0; v < nc; ++v) P[v * NG + gg2] = 3.0*P[v * NG + gg1] - 3.0*P[v * NG + gm] + P[v * NG + gp];
+      break;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ boundary fluxes
+template <int CL, int RS>
+__global__ void k_conn(Geo G, FamDev F, const DRec* recs, const int* own, int nown, Status* st) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nown) return;
+  constexpr int nc = NC<CL>::v;
+  const DRec& r = recs[own[n]];
+  double bo = 1.0, bq = 1.0;
+  if (F.beta) {
+    bo = F.beta[iidx(G.blk[r.b], r.i, r.j, r.k)];
+    bq = F.beta[iidx(G.blk[r.pb], r.pi, r.pj, r.pk)];
+  }
+  double bf = mn(bo, bq);
+  double fl[nc];
+  if (record_flux<CL, RS>(G, F, r, fl, &bf)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) F.connF[(long long)r.cf * nc + v] = fl[v];
+}
+
+template <int CL, int RS>
+__global__ void k_bound(Geo G, FamDev F, const DRec* recs, const int* first, const int* list, int nbc, Status* st) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nbc) return;
+  constexpr int nc = NC<CL>::v;
+  double acc[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) acc[v] = 0.0;
+  for (int rr = first[c]; rr < first[c + 1]; ++rr) {
+    const DRec& r = recs[list[rr]];
+    double fl[nc];
+    if (r.type == 200 && CL == MK) continue;
+    if (r.type == 101 || r.type == 201) {
+#pragma unroll
+      for (int v = 0; v < nc; ++v) { double x = F.connF[(long long)r.cf * nc + v]; fl[v] = r.owner ? x : -x; }
+    } else {
+      if (record_flux<CL, RS>(G, F, r, fl, nullptr)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
+    }
+#pragma unroll
+    for (int v = 0; v < nc; ++v) acc[v] = acc[v] + fl[v];
+  }
+#pragma unroll
+  for (int v = 0; v < nc; ++v) F.Rbw[(long long)c * nc + v] = acc[v];
+}
+
+// ------------------------------------------------------------------ the stage
+
+// One CTA = one tile of TX x TY x TZ cells of one block (256 threads). For each direction the
+// faces of the tile are computed once into shared memory, then every cell takes its two faces in
+// the reference's odd-then-even order; then source, residual and the RK update.
+template <int CL, int RS, bool WRITE_R, typename R>
+__global__ void __launch_bounds__(256)
+k_stage(Geo G, FamDev F, const Tile* tiles, int ndir, int TX, int TY, int TZ, Status* st) {
+  constexpr int nc = NC<CL>::v;
+  const int NT = TX * TY * TZ;
+  extern __shared__ double smem[];   // [nc][slots of the direction]
+  const Tile t = tiles[blockIdx.x];
+  const DBlock& B = G.blk[t.b];
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = (tid / TX) % TY, tz = tid / (TX * TY);
+  const int i = t.i0 + tx, j = t.j0 + ty, k = t.k0 + tz;
+  const bool inside = i < B.ni && j < B.nj && k < B.nk;
+  const int dims[3] = {B.ni, B.nj, B.nk};
+  const int org[3] = {t.i0, t.j0, t.k0};
+  bool bad = false;
+
+  double r[nc];
+  int bc = -1;
+  if (inside) bc = F.bmap[iidx(B, i, j, k)];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) r[v] = (bc >= 0 && inside) ? F.Rb[(long long)bc * nc + v] : 0.0;
+
+  for (int d = 0; d < ndir; ++d) {
+    if (dims[d] < 2) continue;
+    // face slots: the lower cell runs over org[d]-1 .. org[d]+T[d]-1 along d
+    const int sx = d == 0 ? TX + 1 : TX, sy = d == 1 ? TY + 1 : TY, sz = d == 2 ? TZ + 1 : TZ;
+    const int ns = sx * sy * sz;
+    for (int s = tid; s < ns; s += NT) {
+      int a = s % sx, b = (s / sx) % sy, c = s / (sx * sy);
+      int fi = t.i0 + a - (d == 0), fj = t.j0 + b - (d == 1), fk = t.k0 + c - (d == 2);
+      int cl = d == 0 ? fi : d == 1 ? fj : fk;
+      bool ok = cl >= 0 && cl <= dims[d] - 2 && fi < B.ni && fj < B.nj && fk < B.nk && fi >= 0 && fj >= 0 && fk >= 0;
+      if (ok) {
+        R fl[nc];
+        bad |= face_flux<CL, RS, R>(G, F, B, d, fi, fj, fk, fl);
+#pragma unroll
+        for (int v = 0; v < nc; ++v) smem[v * ns + s] = (double)fl[v];
+      }
+    }
+    __syncthreads();
+    if (inside) {
+      const int c = d == 0 ? i : d == 1 ? j : k;
+      const int n = dims[d];
+      const int tc = d == 0 ? tx : d == 1 ? ty : tz;
+      // slot of the face below the cell (lower cell c-1) and above it (lower cell c)
+      int slo = tx + ty * sx + tz * sx * sy;
+      int sup = slo + (d == 0 ? 1 : d == 1 ? sx : sx * sy);
+      (void)tc;
+      const int ci = c + 1;
+      if (ci % 2 == 1) {
+        if (ci < n) {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] - smem[v * ns + sup];
+        }
+        if (ci > 1) {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + smem[v * ns + slo];
+        }
+      } else {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) r[v] = r[v] + smem[v * ns + slo];
+        if (ci < n) {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] - smem[v * ns + sup];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  (void)org;
+  if (bad) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
+  if (!inside) return;
+
+  const long long q = iidx(B, i, j, k);
+  const long long g = gidx(B, i, j, k);
+  double p[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
+  double s[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) s[v] = 0.0;
+  if (F.coupled) {
+    double gas[5] = {G.gas[q], G.gas[G.NI + q], G.gas[2 * G.NI + q], G.gas[3 * G.NI + q], G.gas[4 * G.NI + q]};
+    if constexpr (sizeof(R) == 8) {
+      double tau = cell_source<CL, double>(p, gas, G.gas[5 * G.NI + q], G.gas[6 * G.NI + q], G.gas[7 * G.NI + q],
+                                           G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, s);
+      if (F.write_tau) F.tau[q] = tau;
+    } else {
+      R pf[nc], gf[5], sf[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) pf[v] = (R)p[v];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) gf[v] = (R)gas[v];
+      R tau = cell_source<CL, R>(pf, gf, (R)G.gas[5 * G.NI + q], (R)G.gas[6 * G.NI + q], (R)G.gas[7 * G.NI + q],
+                                 (R)G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, sf);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) s[v] = (double)sf[v];
+      if (F.write_tau) F.tau[q] = (double)tau;
+    }
+#pragma unroll
+    for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) s[v] = 0.0;
+  }
+  const double dt = F.dt ? F.dt[q] : *F.dtg;
+  const double vol = G.vol[q];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) r[v] = (r[v]/vol + s[v]) * dt;
+#pragma unroll
+  for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) r[v] = 0.0;
+  if constexpr (WRITE_R) {
+#pragma unroll
+    for (int v = 0; v < nc; ++v) F.resid[(long long)v * G.NI + q] = r[v];
+    return;
+  } else {
+    double po[nc], co[nc], cn[nc];
+#pragma unroll
+    for (int v = 0; v < nc; ++v) po[v] = F.U0[(long long)v * G.NG + g];
+    prim2cons<CL, double>(po, co, F.mat.cp);
+    prim2cons<CL, double>(p, cn, F.mat.cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + r[v]) * F.rk; cn[v] = co[v] + rr; }
+    if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
+    cons2prim<CL>(cn, p, F.mat.cp);
+    if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];
+  }
+}
+
+// ------------------------------------------------------------------ IRS and the separate update
+template <int CL>
+__global__ void k_update(Geo G, FamDev F, Status* st) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.NI) return;
+  constexpr int nc = NC<CL>::v;
+  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  int i, j, k; decode(B, q, i, j, k);
+  long long g = gidx(B, i, j, k);
+  double p[nc], po[nc], co[nc], cn[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) { p[v] = F.Up[(long long)v * G.NG + g]; po[v] = F.U0[(long long)v * G.NG + g]; }
+  prim2cons<CL, double>(po, co, F.mat.cp);
+  prim2cons<CL, double>(p, cn, F.mat.cp);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + F.resid[(long long)v * G.NI + q]) * F.rk; cn[v] = co[v] + rr; }
+  if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
+  cons2prim<CL>(cn, p, F.mat.cp);
+  if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];
+}
+
+
+__global__ void k_begin(Status* st) {
+  st->iter += 1;
+  st->iter_from_call += 1;
+  double d = (double)1e+5f;
+  st->dtbits = (unsigned long long)__double_as_longlong(d);
+}
+
+__global__ void k_time(Status* st, int time_accurate) {
+  double d = __longlong_as_double((long long)st->dtbits);
+  st->dtglobal = d;
+  if (time_accurate) st->time = st->time + d;
+}
+
+
+// ------------------------------------------------------------------ sensor
+__global__ void k_beta(Geo G, FamDev F) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.NI) return;
+  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  int i, j, k; decode(B, q, i, j, k);
+  const double* P = F.Up;   // variable 0: density
+  F.betaw[q] = sd_rho(P[gidx(B, i, j, k)], P[gidx(B, i - 1, j, k)], P[gidx(B, i + 1, j, k)],
+                      P[gidx(B, i, j - 1, k)], P[gidx(B, i, j + 1, k)],
+                      P[gidx(B, i, j, k - 1)], P[gidx(B, i, j, k + 1)]);
+}
+
+
+// One Jacobi sweep of direction d (Lib_IRS.f90:278-293): out = (R + b (star_{-1} + star_{+1}))/(1+2b),
+// with the ghost values of star fixed to the first and last cell of R (zero gradient).
+__global__ void k_irs(Geo G, int nc, const double* R0, const double* star, double* out, int d, double beta) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.NI) return;
+  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  int i, j, k; decode(B, q, i, j, k);
+  int c = d == 0 ? i : d == 1 ? j : k;
+  int n = d == 0 ? B.ni : d == 1 ? B.nj : B.nk;
+  long long st = d == 0 ? 1 : d == 1 ? B.ni : (long long)B.ni * B.nj;
+  long long qm = c > 0 ? q - st : q;         // ghost 0 = cell 1 of the original residual
+  long long qp = c < n - 1 ? q + st : q;
+  for (int v = 0; v < nc; ++v) {
+    const double* S = (c > 0 ? star : R0) + (long long)v * G.NI;
+    const double* Sp = (c < n - 1 ? star : R0) + (long long)v * G.NI;
+    out[(long long)v * G.NI + q] = (R0[(long long)v * G.NI + q] + beta*(S[qm] + Sp[qp])) / (1.0 + 2.0*beta);
+  }
+}
+
+
+// ------------------------------------------------------------------ residual norm
+// residual_sq (Mod_Diagnostic.f90:106-130): per CTA, sums of (new - old)^2 of rho, u, v, w, T
+// over a contiguous range of one block's cells, reduced in a fixed order.
+
+__global__ void k_norm(Geo G, const double* Un, const double* Uo, int iT, const NormChunk* ch, double* part) {
+  const NormChunk c = ch[blockIdx.x];
+  const DBlock& B = G.blk[c.b];
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (long long q = c.q0 + threadIdx.x; q < c.q1; q += blockDim.x) {
+    int i, j, k; decode(B, q, i, j, k);
+    long long g = gidx(B, i, j, k);
+    int vs[5] = {0, 1, 2, 3, iT};
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      double d = fabs(Un[(long long)vs[m] * G.NG + g] - Uo[(long long)vs[m] * G.NG + g]);
+      acc[m] = acc[m] + d*d;
+    }
+  }
+  __shared__ double red[5][256];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) red[m][threadIdx.x] = acc[m];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) red[m][threadIdx.x] = red[m][threadIdx.x] + red[m][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int m = 0; m < 5; ++m) part[(long long)blockIdx.x * 5 + m] = red[m][0];
+  }
+}
+
+
+}  // namespace
+}  // namespace ice

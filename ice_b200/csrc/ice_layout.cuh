@@ -1,0 +1,119 @@
+// ice_layout.cuh -- the device layout of the solve stage: blocks, geometry, records, status,
+// the per-family view the kernels read, and the launch interface of the per-closure units.
+#pragma once
+#include <cuda_runtime.h>
+#include "ice_physics.cuh"
+
+namespace ice {
+
+
+// ------------------------------------------------------------------ device layout
+struct DBlock {
+  int ni, nj, nk, pad;
+  long long goff;     // ghost-cell pools (1-gc:n+gc)^3
+  long long ioff;     // interior pools
+  long long roff;     // ring pools (0:n+1)^3
+  long long foff[3];  // face pools of each direction
+};
+
+struct Geo {                 // geometry shared by the families
+  const DBlock* blk;
+  int nb;
+  long long NG, NI, NR, NF[3];
+  const double* face[3];     // 4 SoA components (nx, ny, nz, A) of NF[d] each
+  const double* vol;         // NI
+  const double* dl;          // 3 SoA components of NR
+  const double* M;           // 9 SoA components of NI (column-major c(3,3))
+  const double* gas;         // 9 SoA components of NI: rho u v w T R gam k mu
+};
+
+struct DRec {                // one boundary record, 0-based cells
+  int b, i, j, k, f, type;
+  int bs, is, js, ks, fs;
+  int owner, cf;             // cf 0-based (-1 when none)
+  int pb, pi, pj, pk;        // the partner's cell (connections)
+  int normal_dir;
+  double massflux, velocity, alpha, beta, temperature, radius, gfixed;
+};
+
+struct Status {
+  unsigned int flags;
+  unsigned int pad;
+  unsigned long long nfloored;
+  unsigned long long dtbits;  // running min of dt as the bits of a positive double
+  double dtglobal;
+  double time;
+  int iter;
+  int iter_from_call;
+};
+
+__device__ __forceinline__ long long gidx(const DBlock& B, int i, int j, int k) {
+  return B.goff + ((long long)(k + 2) * (B.nj + 4) + (j + 2)) * (B.ni + 4) + (i + 2);
+}
+__device__ __forceinline__ long long iidx(const DBlock& B, int i, int j, int k) {
+  return B.ioff + ((long long)k * B.nj + j) * B.ni + i;
+}
+__device__ __forceinline__ long long ridx(const DBlock& B, int i, int j, int k) {
+  return B.roff + ((long long)(k + 1) * (B.nj + 2) + (j + 1)) * (B.ni + 2) + (i + 1);
+}
+// face d with Fortran index F (the 1-based index of the cell below it along d), other indices 0-based
+__device__ __forceinline__ long long fidx(const DBlock& B, int d, int i, int j, int k, int F) {
+  if (d == 0) return B.foff[0] + ((long long)k * B.nj + j) * (B.ni + 1) + F;
+  if (d == 1) return B.foff[1] + ((long long)k * (B.nj + 1) + F) * B.ni + i;
+  return B.foff[2] + ((long long)F * B.nj + j) * B.ni + i;
+}
+__device__ __forceinline__ long long gstride(const DBlock& B, int d) {
+  return d == 0 ? 1LL : d == 1 ? (long long)(B.ni + 4) : (long long)(B.ni + 4) * (B.nj + 4);
+}
+
+struct FamDev {              // what the kernels of one family read
+  int closure, riemann, nc, limiter, sd, coupled, drag, heat, blow;
+  unsigned int frozen_mask;  // bit v: slot v+1 frozen
+  Mat mat;
+  const double* U0;          // pointwise U_0
+  const double* Up;          // stencil U_{k-1}
+  double* Uo;                // U_k
+  double* Ug;                // buffer whose ghosts the ghost kernels fill (== Up)
+  unsigned char* inj;
+  const double* beta;        // NI, or null (1)
+  double* betaw;
+  const double* dt;          // NI (steady) or null
+  const double* dtg;         // &status->dtglobal (time-accurate)
+  double* tau;               // NI
+  const int* bmap;           // NI: boundary-cell index or -1
+  const double* Rb;          // [nbcell][nc]
+  double* Rbw;
+  double* connF;             // [ncf][nc]
+  double* resid;             // IRS: [v][NI]
+  double rk;
+  int write_tau;
+};
+
+struct Tile { int b, i0, j0, k0; };
+struct NormChunk { int b; long long q0, q1; };
+
+// Everything one family's stage needs, for the launcher of its closure's translation unit.
+struct LaunchArgs {
+  Geo G;
+  FamDev F;
+  const DRec* recs; int nrec;
+  const int* own; int nown;
+  const int* bfirst; const int* blist; int nbc;
+  const Tile* tiles; int ntile; int TX, TY, TZ;
+  int ndir, sd, irs, precision;
+  double irs_beta;
+  double* resid; double* resid2; double* resid3;
+  Status* st;
+  cudaStream_t s;
+  void (*tick)(void*, int, cudaStream_t);
+  void* tick_ctx;
+};
+
+enum { KC_DT = 0, KC_GHOST, KC_BETA, KC_BOUND, KC_STAGE, KC_IRS, KC_NORM, KC_N };
+
+void launch_family_mk(const LaunchArgs& a);
+void launch_family_ig(const LaunchArgs& a);
+void launch_family_ag(const LaunchArgs& a);
+size_t stage_smem_bytes(int nc, int TX, int TY, int TZ);
+
+}  // namespace ice

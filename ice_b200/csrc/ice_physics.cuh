@@ -1,0 +1,717 @@
+// ice_physics.cuh -- device arithmetic of ICE's dispersed-phase step: closures,
+// limiters, MUSCL reconstruction, Riemann solvers, shock sensor, drag, heat,
+// evaporation and the cell source.
+//
+// Every function keeps the reference's operation order (a Fortran chain of * / + -
+// evaluates left to right) and the library is compiled with --fmad=false, so the
+// plain form (R = double) rounds exactly as the unfused Fortran source does.
+// Constants the reference writes as default-real (single precision) literals are
+// promoted from float as gfortran promotes them (1e-25 in the closures, 1e-20 in
+// drag and tau, 1e+5 in compute_dt).
+//
+// R is the arithmetic type of reconstruction, Riemann fluxes and sources: double in
+// the plain form, float in the FP32-flux form (the RK accumulation, dt and norms stay
+// double in both, in ice_gpu.cu).
+//
+// References (file:line in the ICE sources):
+//   closures      physics/Lib_Model_MK.f90:11-184, Lib_Model_IG.f90:11-202, Lib_Model_AG.f90:11-296
+//   limiters      numerics/space/Lib_Limiters.f90:314-493
+//   reconstruct   numerics/space/Lib_Reconstruction.f90:17-99
+//   Riemann       numerics/fluxes/riemann/Lib_Riemann.f90:61-241
+//   sensor        numerics/space/Lib_Shock_Detector.f90:17-42
+//   drag / heat   physics/Lib_Drag.f90:83-324, physics/Lib_Heat.f90:68-160
+//   evaporation   physics/Lib_Evaporation.f90:129-261, 287-545, 738-745
+//   source        physics/Mod_Sources.f90:230-274, 465-622
+#pragma once
+#include <cstdint>
+#include <cmath>
+#include "../../include/ice_gpu.h"
+
+namespace ice {
+
+constexpr int MK = ICE_CLOSURE_MK, IG = ICE_CLOSURE_IG, AG = ICE_CLOSURE_AG;
+
+template <int CL> struct NC;
+template <> struct NC<MK> { static constexpr int v = 6; };
+template <> struct NC<IG> { static constexpr int v = 7; };
+template <> struct NC<AG> { static constexpr int v = 12; };
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kSigmaSB = 5.670374419e-8;
+constexpr double kRhoEmpty = 1e-6;
+constexpr double kThetaCap = 1.0;
+constexpr double kRu = 8314.46;
+constexpr double kPatm = 101325.0;
+constexpr double kXsCap = 1e-12;
+
+// Material constants of one family on the constant-property path, in device-friendly form.
+struct Mat {
+  double rho, cp, lv, emiss;
+  int evap, intf;
+  double ep[ICE_GPU_NEP];
+};
+enum { EP_MV = 0, EP_LV, EP_CPV, EP_LE, EP_YINF, EP_LVMVRU, EP_INVTB, EP_ALPHAE };
+
+template <typename R> __device__ __forceinline__ R epsv() { return (R)(double)1e-25f; }
+
+__device__ __forceinline__ bool not_finite(double x) {
+  return ((__double_as_longlong(x) >> 52) & 0x7FF) == 0x7FF;
+}
+__device__ __forceinline__ bool not_finite(float x) { return !isfinite(x); }
+
+template <typename R> __device__ __forceinline__ R mn(R a, R b) { return b < a ? b : a; }
+template <typename R> __device__ __forceinline__ R mx(R a, R b) { return b > a ? b : a; }
+
+// gfortran NORM2 of three values (scaled sum of squares), Mod_dt.f90:269, Mod_Sources.f90:35
+template <typename R> __device__ __forceinline__ R norm2_3(R a, R b, R c) {
+  R v[3] = {a, b, c};
+  R scale = (R)0, s = (R)1;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    if (v[m] != (R)0) {
+      R ax = fabs(v[m]);
+      if (scale < ax) { R q = scale / ax; s = (R)1 + s * q * q; scale = ax; }
+      else            { R q = ax / scale; s = s + q * q; }
+    }
+  }
+  return sqrt(s) * scale;
+}
+
+// ------------------------------------------------------------------ closures
+template <int CL, typename R> __device__ __forceinline__ void prim2cons(const R* p, R* c, R cp) {
+  R n2 = p[1]*p[1] + p[2]*p[2] + p[3]*p[3];
+  c[0] = p[0];
+  c[1] = p[0]*p[1]; c[2] = p[0]*p[2]; c[3] = p[0]*p[3];
+  if constexpr (CL == MK) {
+    c[4] = p[0]*cp*p[4] + (R)0.5*p[0]*n2;
+    c[5] = p[5];
+  } else if constexpr (CL == IG) {
+    c[4] = p[0]*n2 + (R)3*p[4];
+    c[5] = p[0]*cp*p[5] + (R)0.5*c[4];
+    c[6] = p[6];
+  } else {
+    c[4] = p[0]*p[1]*p[1] + p[4];
+    c[5] = p[0]*p[1]*p[2] + p[5];
+    c[6] = p[0]*p[1]*p[3] + p[6];
+    c[7] = p[0]*p[2]*p[2] + p[7];
+    c[8] = p[0]*p[2]*p[3] + p[8];
+    c[9] = p[0]*p[3]*p[3] + p[9];
+    c[10] = p[0]*cp*p[10] + (R)0.5*(c[4] + c[7] + c[9]);
+    c[11] = p[11];
+  }
+}
+
+// cons -> prim with the reference's floors (Lib_Model_*: cons_2_prim_*)
+template <int CL> __device__ __forceinline__ void cons2prim(const double* c, double* p, double cp) {
+  const double eps = epsv<double>();
+  p[0] = c[0];
+  p[1] = c[1] / (p[0] + eps); p[2] = c[2] / (p[0] + eps); p[3] = c[3] / (p[0] + eps);
+  double n2 = p[1]*p[1] + p[2]*p[2] + p[3]*p[3];
+  if constexpr (CL == MK) {
+    p[4] = (c[4] - 0.5*p[0]*n2) / (cp*p[0] + eps);
+    p[5] = c[5];
+    if (p[0] < eps) {
+#pragma unroll
+      for (int v = 0; v < 6; ++v) p[v] = eps;
+    }
+    if (p[4] < eps) p[4] = eps;
+    if (p[5] < eps) p[5] = eps;
+  } else if constexpr (CL == IG) {
+    p[4] = 1.0/3.0 * (c[4] - p[0]*n2);
+    if (p[0] <= kRhoEmpty && p[4] > p[0]*kThetaCap) p[4] = p[0]*kThetaCap;
+    p[5] = (c[5] - 0.5*c[4]) / (cp*p[0] + eps);
+    p[6] = c[6];
+    if (p[0] < eps) {
+#pragma unroll
+      for (int v = 0; v < 7; ++v) p[v] = eps;
+    }
+    if (p[4] < eps) p[4] = eps;
+    if (p[5] < eps) p[5] = eps;
+    if (p[6] < eps) p[6] = eps;
+  } else {
+    p[4] = c[4] - p[0]*p[1]*p[1];
+    p[5] = c[5] - p[0]*p[1]*p[2];
+    p[6] = c[6] - p[0]*p[1]*p[3];
+    p[7] = c[7] - p[0]*p[2]*p[2];
+    p[8] = c[8] - p[0]*p[2]*p[3];
+    p[9] = c[9] - p[0]*p[3]*p[3];
+    p[10] = (c[10] - 0.5*(c[4] + c[7] + c[9])) / (cp*p[0] + eps);
+    p[11] = c[11];
+    if (p[0] <= kRhoEmpty && p[4] + p[7] + p[9] > 3.0*p[0]*kThetaCap) {
+      double f = 3.0*p[0]*kThetaCap / (p[4] + p[7] + p[9]);
+#pragma unroll
+      for (int v = 4; v < 10; ++v) p[v] = p[v] * f;
+    }
+    if (p[0] < eps) {
+#pragma unroll
+      for (int v = 0; v < 12; ++v) p[v] = eps;
+      p[5] = 0.0; p[6] = 0.0; p[8] = 0.0;
+    }
+    if (p[4] < eps) p[4] = eps;
+    if (fabs(p[5]) < eps) p[5] = 0.0;
+    if (fabs(p[6]) < eps) p[6] = 0.0;
+    if (p[7] < eps) p[7] = eps;
+    if (fabs(p[8]) < eps) p[8] = 0.0;
+    if (p[9] < eps) p[9] = eps;
+    if (p[10] < eps) p[10] = eps;
+    if (p[11] < eps) p[11] = eps;
+  }
+}
+
+template <int CL, typename R> __device__ __forceinline__ bool check_prim(const R* p) {
+  constexpr int nc = NC<CL>::v;
+  bool bad = false;
+#pragma unroll
+  for (int v = 0; v < nc; ++v) bad |= not_finite(p[v]);
+  if (bad || p[0] < (R)0) return false;
+  if constexpr (CL == IG) { if (p[4] < (R)0) return false; }
+  if constexpr (CL == AG) { if (p[4] < (R)0 || p[7] < (R)0 || p[9] < (R)0) return false; }
+  return true;
+}
+
+template <int CL, typename R> __device__ __forceinline__ R wavespeed(const R* p, const R* n) {
+  if constexpr (CL == MK) {
+    return (R)0;
+  } else if constexpr (CL == IG) {
+    R pr = (p[4] + p[4] + p[4]) / (R)3;
+    return sqrt((R)3*pr / (p[0] + epsv<R>()));
+  } else {
+    R pnn = n[0]*(p[4]*n[0] + p[5]*n[1] + p[6]*n[2]) +
+            n[1]*(p[5]*n[0] + p[7]*n[1] + p[8]*n[2]) +
+            n[2]*(p[6]*n[0] + p[8]*n[1] + p[9]*n[2]);
+    return sqrt((R)3*fmax(pnn, (R)0) / (p[0] + epsv<R>()));
+  }
+}
+
+template <int CL, typename R> __device__ __forceinline__ void flux_make(const R* p, const R* n, R* f, R cp) {
+  R n2 = p[1]*p[1] + p[2]*p[2] + p[3]*p[3];
+  R un = p[1]*n[0] + p[2]*n[1] + p[3]*n[2];
+  f[0] = p[0]*un;
+  if constexpr (CL == MK) {
+    f[1] = f[0]*p[1]; f[2] = f[0]*p[2]; f[3] = f[0]*p[3];
+    f[4] = f[0]*((R)0.5*n2 + cp*p[4]);
+    f[5] = p[5]*un;
+  } else if constexpr (CL == IG) {
+    f[1] = f[0]*p[1] + p[4]*n[0];
+    f[2] = f[0]*p[2] + p[4]*n[1];
+    f[3] = f[0]*p[3] + p[4]*n[2];
+    f[4] = f[0]*n2 + (R)5*p[4]*un;
+    f[5] = f[0]*((R)0.5*n2 + cp*p[5]) + (R)2.5*p[4]*un;
+    f[6] = p[6]*un;
+  } else {
+    R p1n = p[4]*n[0] + p[5]*n[1] + p[6]*n[2];
+    R p2n = p[5]*n[0] + p[7]*n[1] + p[8]*n[2];
+    R p3n = p[6]*n[0] + p[8]*n[1] + p[9]*n[2];
+    f[1] = f[0]*p[1] + p1n;
+    f[2] = f[0]*p[2] + p2n;
+    f[3] = f[0]*p[3] + p3n;
+    f[4] = f[0]*p[1]*p[1] + un*p[4] + p[1]*p1n + p[1]*p1n;
+    f[5] = f[0]*p[1]*p[2] + un*p[5] + p[1]*p2n + p[2]*p1n;
+    f[6] = f[0]*p[1]*p[3] + un*p[6] + p[1]*p3n + p[3]*p1n;
+    f[7] = f[0]*p[2]*p[2] + un*p[7] + p[2]*p2n + p[2]*p2n;
+    f[8] = f[0]*p[2]*p[3] + un*p[8] + p[2]*p3n + p[3]*p2n;
+    f[9] = f[0]*p[3]*p[3] + un*p[9] + p[3]*p3n + p[3]*p3n;
+    f[10] = f[0]*((R)0.5*n2 + (R)0.5*(p[4] + p[7] + p[9])/(p[0] + epsv<R>()) + cp*p[10])
+          + p[1]*p1n + p[2]*p2n + p[3]*p3n;
+    f[11] = p[11]*un;
+  }
+}
+
+// H P H, H = I - 2 n n^T (Lib_Model_AG.f90:181-200)
+__device__ __forceinline__ void mirror_tensor(const double* p, const double* n, double* pm) {
+  double t0 = p[0]*n[0] + p[1]*n[1] + p[2]*n[2];
+  double t1 = p[1]*n[0] + p[3]*n[1] + p[4]*n[2];
+  double t2 = p[2]*n[0] + p[4]*n[1] + p[5]*n[2];
+  double s = n[0]*t0 + n[1]*t1 + n[2]*t2;
+  pm[0] = p[0] - 4.0*n[0]*t0 + 4.0*s*n[0]*n[0];
+  pm[1] = p[1] - 2.0*(n[0]*t1 + t0*n[1]) + 4.0*s*n[0]*n[1];
+  pm[2] = p[2] - 2.0*(n[0]*t2 + t0*n[2]) + 4.0*s*n[0]*n[2];
+  pm[3] = p[3] - 4.0*n[1]*t1 + 4.0*s*n[1]*n[1];
+  pm[4] = p[4] - 2.0*(n[1]*t2 + t1*n[2]) + 4.0*s*n[1]*n[2];
+  pm[5] = p[5] - 4.0*n[2]*t2 + 4.0*s*n[2]*n[2];
+}
+
+// ------------------------------------------------------------------ limiters
+template <typename R> __device__ __forceinline__ R limiter(int lim, R x, R y, R cx, R cy) {
+  if (lim == ICE_LIM_IORD) return (R)0;
+  R ru = y / (x + (R)1e-30), phi;
+  switch (lim) {
+    case ICE_LIM_MINMOD: phi = mx((R)0, mn((R)1, ru)); return phi * x;
+    case ICE_LIM_VANALBADA: phi = (ru*ru + ru) / (ru*ru + (R)1); break;
+    case ICE_LIM_VANLEER: phi = (ru + fabs(ru)) / ((R)1 + fabs(ru)); break;
+    case ICE_LIM_OSPRE: phi = ((R)1.5*(ru*ru + ru)) / (ru*ru + ru + (R)1); break;
+    case ICE_LIM_UMIST: phi = mx((R)0, mn(mn(mn((R)2*ru, (R)0.25 + (R)0.75*ru), (R)0.75 + (R)0.25*ru), (R)2)); break;
+    case ICE_LIM_OSHER: phi = mx((R)0, mn(ru, (R)1.5)); break;
+    case ICE_LIM_SWEBY: phi = mx(mx((R)0, mn((R)1.5*ru, (R)1)), mn(ru, (R)1.5)); break;
+    case ICE_LIM_MC: phi = mx((R)0, mn(mn((R)2*ru, (R)0.5*((R)1 + ru)), (R)2)); break;
+    case ICE_LIM_KOREN: phi = mx((R)0, mn((R)2*ru, mn(((R)1 + (R)2*ru)/(R)3, (R)2))); break;
+    case ICE_LIM_SUPERBEE: phi = mx(mx((R)0, mn((R)2*ru, (R)1)), mn(ru, (R)2)); break;
+    default: return (R)0;
+  }
+  if (ru > (R)0) phi = mn(mn(phi, cx), cy*ru);
+  return phi * x;
+}
+
+// The four cells of a stencil: a source of values q(s, v), s = 0..3 (prev, local, next, next2).
+// state_reconstruction + slope_bounds; returns true when the first-order fallback is itself
+// unphysical (report_stencil).
+template <int CL, typename R, typename Q>
+__device__ __forceinline__ bool reconstruct(int lim, const Q& q, R dl0, R dl1, R dl2, R dll, R dlr,
+                                            R* pl, R* pr, R beta) {
+  constexpr int nc = NC<CL>::v;
+  R cxl, cyl, cxr, cyr, limval = beta;
+  if (dll > (R)0) { cxl = dl1/dll; cyl = dl0/dll; } else { cxl = (R)2; cyl = (R)2; }
+  if (dlr > (R)0) { cxr = dl2/dlr; cyr = dl1/dlr; } else { cxr = (R)2; cyr = (R)2; }
+  const R re = (R)kRhoEmpty;
+  R r0 = q(0, 0), r1 = q(1, 0), r2 = q(2, 0), r3 = q(3, 0);
+  bool first_l = r0 <= re || r1 <= re || r2 <= re;
+  bool first_r = r1 <= re || r2 <= re || r3 <= re;
+  if (first_l) {
+#pragma unroll
+    for (int v = 0; v < nc; ++v) pl[v] = q(1, v);
+  }
+  if (first_r) {
+#pragma unroll
+    for (int v = 0; v < nc; ++v) pr[v] = q(2, v);
+  }
+  bool st_l = first_l, st_r = first_r;
+  // the weight halves each pass: from any weight <= 1 it is below 1e-18 within 61 passes; the
+  // cap only guards a non-finite weight, for which the reference would not end
+  for (int pass = 0; (!st_l || !st_r) && pass < 256; ++pass) {
+    if (pass == 255) limval = (R)0;
+#pragma unroll
+    for (int v = 0; v < nc; ++v) {
+      R a1 = q(1, v), a2 = q(2, v);
+      R slope1 = (a2 - a1) / dl1;
+      if (!first_l) {
+        R slope0 = (a1 - q(0, v)) / dl0;
+        R sl = limiter(lim, slope1, slope0, cxl, cyl) * limval;
+        pl[v] = a1 + sl*dll;
+      }
+      if (!first_r) {
+        R slope2 = (q(3, v) - a2) / dl2;
+        R sr = limiter(lim, slope2, slope1, cxr, cyr) * limval;
+        pr[v] = a2 - sr*dlr;
+      }
+    }
+    if (!first_l) st_l = check_prim<CL>(pl);
+    if (!first_r) st_r = check_prim<CL>(pr);
+    limval = (R)0.5*limval;
+    if (limval < (R)1e-18 && !(st_l && st_r)) {
+#pragma unroll
+      for (int v = 0; v < nc; ++v) { pl[v] = q(1, v); pr[v] = q(2, v); }
+      if (!(check_prim<CL>(pl) && check_prim<CL>(pr))) return true;
+      break;
+    }
+  }
+  return false;
+}
+
+// ------------------------------------------------------------------ Riemann
+template <typename R> __device__ __forceinline__ void saurel(const R* p1, const R* p4, const R* n, R* f, R cp) {
+  R vn1 = p1[1]*n[0] + p1[2]*n[1] + p1[3]*n[2];
+  R vn4 = p4[1]*n[0] + p4[2]*n[1] + p4[3]*n[2];
+  R vn = (R)0.5*(vn1 + vn4);
+  if (vn > (R)0 || vn < (R)0) {
+    const R* p = vn > (R)0 ? p1 : p4;
+    R vs = vn > (R)0 ? vn1 : vn4;
+    R ut = (p[1] - vs*n[0]), vt = (p[2] - vs*n[1]), wt = (p[3] - vs*n[2]);
+    R uu = vs*n[0] + ut, vv = vs*n[1] + vt, ww = vs*n[2] + wt;
+    f[0] = p[0]*vn;
+    f[1] = uu*f[0]; f[2] = vv*f[0]; f[3] = ww*f[0];
+    f[4] = f[0]*((R)0.5*(uu*uu + vv*vv + ww*ww) + cp*p[4]);
+    f[5] = p[5]*vn;
+  } else {
+#pragma unroll
+    for (int v = 0; v < 6; ++v) f[v] = (R)0;
+  }
+}
+
+template <int CL, typename R> __device__ __forceinline__ void rusanov(const R* p1, const R* p4, const R* n, R* f, R cp) {
+  constexpr int nc = NC<CL>::v;
+  R c1[nc], c4[nc], f1[nc], f4[nc];
+  R vn1 = p1[1]*n[0] + p1[2]*n[1] + p1[3]*n[2];
+  R vn4 = p4[1]*n[0] + p4[2]*n[1] + p4[3]*n[2];
+  R s1 = wavespeed<CL>(p1, n), s4 = wavespeed<CL>(p4, n);
+  prim2cons<CL>(p1, c1, cp); prim2cons<CL>(p4, c4, cp);
+  flux_make<CL>(p1, n, f1, cp); flux_make<CL>(p4, n, f4, cp);
+  R A = fabs(vn1 - s1);
+  A = mx(A, (R)fabs(vn4 - s4)); A = mx(A, (R)fabs(vn1 + s1)); A = mx(A, (R)fabs(vn4 + s4));
+#pragma unroll
+  for (int v = 0; v < nc; ++v) f[v] = (R)0.5 * (f1[v] + f4[v] - A*(c4[v] - c1[v]));
+}
+
+template <int CL, typename R> __device__ __forceinline__ void hlle(const R* p1, const R* p4, const R* n, R* f, R cp) {
+  constexpr int nc = NC<CL>::v;
+  R vn1 = p1[1]*n[0] + p1[2]*n[1] + p1[3]*n[2];
+  R vn4 = p4[1]*n[0] + p4[2]*n[1] + p4[3]*n[2];
+  R s1 = wavespeed<CL>(p1, n), s4 = wavespeed<CL>(p4, n);
+  R r1 = sqrt(p1[0]), r4 = sqrt(p4[0]);
+  R uR = (r1*p1[1] + r4*p4[1]) / (r1 + r4);
+  R vR = (r1*p1[2] + r4*p4[2]) / (r1 + r4);
+  R wR = (r1*p1[3] + r4*p4[3]) / (r1 + r4);
+  R vnR = uR*n[0] + vR*n[1] + wR*n[2];
+  R sR = (r1*s1 + r4*s4) / (r1 + r4);
+  R S1 = mn(mn((R)0, vn1 - s1), vnR - sR);
+  R S4 = mx(mx((R)0, vn4 + s4), vnR + sR);
+  R a0 = -S1, a1 = S1*S4, a2 = S4;
+  int loc = 0; R m = a0;
+  if (a1 < m) { loc = 1; m = a1; }
+  if (a2 < m) { loc = 2; m = a2; }
+  if (loc == 0) {
+    flux_make<CL>(p1, n, f, cp);
+  } else if (loc == 2) {
+    flux_make<CL>(p4, n, f, cp);
+  } else {
+    R f1[nc], f4[nc], c1[nc], c4[nc];
+    flux_make<CL>(p1, n, f1, cp); flux_make<CL>(p4, n, f4, cp);
+    prim2cons<CL>(p1, c1, cp); prim2cons<CL>(p4, c4, cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) f[v] = (S4*f1[v] - S1*f4[v] + S1*S4*(c4[v] - c1[v])) / (S4 - S1);
+  }
+}
+
+template <int CL, int RS, typename R> __device__ __forceinline__ void riemann(const R* p1, const R* p4, const R* n, R* f, R cp) {
+  if constexpr (RS == ICE_RIEMANN_SAUREL) saurel<R>(p1, p4, n, f, cp);
+  else if constexpr (RS == ICE_RIEMANN_HLLE) hlle<CL>(p1, p4, n, f, cp);
+  else rusanov<CL>(p1, p4, n, f, cp);
+}
+
+// ------------------------------------------------------------------ sensor
+__device__ __forceinline__ double sd_rho(double r, double r1, double r2, double r3, double r4, double r5, double r6) {
+  double kp1 = fabs((r2 - 2.0*r + r1) / (r2 + 2.0*r + r1 + 1e-30));
+  double kp2 = fabs((r4 - 2.0*r + r3) / (r4 + 2.0*r + r3 + 1e-30));
+  double kp3 = fabs((r6 - 2.0*r + r5) / (r6 + 2.0*r + r5 + 1e-30));
+  double sw = mx(mx(kp1, kp2), kp3);
+  if (sw < 1.0/20.0) {
+    double phi = mx(sw*20.0, 0.0);
+    return 1.0 - tanh(10.0*phi*phi*phi);
+  }
+  return 0.0;
+}
+
+// ------------------------------------------------------------------ drag
+template <typename R> __device__ __forceinline__ R toll_d() { return (R)(double)1e-20f; }
+
+template <typename R> __device__ __forceinline__ R drag_wen_yu(R Re) {
+  if (Re <= (R)1000) return (R)24/(Re + toll_d<R>()) * ((R)1 + (R)0.15*pow(Re, (R)0.687));
+  return (R)0.43;
+}
+template <typename R> __device__ R henderson1(R Re, R Ma, R G, R Tr) {
+  const R t = toll_d<R>();
+  R sg = pow((R)0.5*G, (R)0.5);
+  R X = Re + Ma*sg*((R)4.33 + ((R)3.65 - (R)1.53*Tr)/((R)1 + (R)0.353*Tr)*exp(-(R)0.247*Re/(Ma*sg + t))) + t;
+  R rs = pow(Re, (R)0.5);
+  return (R)24*pow(X, (R)-1)
+       + exp(-(R)0.5*Ma/(rs + t))*(((R)4.5 + (R)0.38*((R)0.03*Re + (R)0.48*rs)) / ((R)1 + (R)0.03*Re + (R)0.48*rs)
+                                   + (R)0.1*(Ma*Ma) + (R)0.2*pow(Ma, (R)8))
+       + (R)0.6*Ma*sg*((R)1 - exp(-Ma/(Re + t)));
+}
+template <typename R> __device__ R henderson2(R Re, R Ma, R G, R Tr) {
+  const R t = toll_d<R>();
+  R q = pow(Ma/(Re + t), (R)0.5);
+  return ((R)0.9 + (R)0.34/((Ma*Ma) + t) + (R)1.86*q*((R)2 + (R)2/(Ma*Ma*(R)0.5*G + t)
+          + ((R)1.058/(Ma*pow((R)0.5*G, (R)0.5) + t))*pow(Tr, (R)0.5)) - (R)1/(pow(Ma, (R)4)*(G*G)*(R)0.25 + t))
+         / ((R)1 + (R)1.86*q);
+}
+template <typename R> __device__ R drag(R Re, R Ma, R G, R Tr, int sel) {
+  const R t = toll_d<R>();
+  switch (sel) {
+    case 1: return (R)0.45;
+    case 2: return (R)24/(Re + t);
+    case 3: return (R)24/(Re + t) * ((R)1 + (R)3*Re/(R)16);
+    case 4: return (R)24/(Re + t) * ((R)1 + (R)0.15*pow(Re, (R)0.687));
+    case 5: return drag_wen_yu(Re);
+    case 6: if (Re < (R)1000) return (R)24/(Re + t) * ((R)1 + pow(Re, (R)(2.0/3.0))/(R)6); return (R)0.4392;
+    case 7: return (R)24/(Re + t) * ((R)1 + (R)0.15*pow(Re, (R)0.687) + (R)0.0175*Re/((R)1 + (R)4.25*(R)1e4*pow(Re, (R)-1.16)));
+    case 8: {
+      R a1, a2, a3;
+      if (Re <= (R)0.1) { a1 = 0; a2 = 24; a3 = 0; }
+      else if (Re <= (R)1.0) { a1 = (R)3.69; a2 = (R)22.73; a3 = (R)0.0903; }
+      else if (Re <= (R)10) { a1 = (R)1.222; a2 = (R)29.1667; a3 = (R)-3.8889; }
+      else if (Re <= (R)100) { a1 = (R)0.6167; a2 = (R)46.5; a3 = (R)-116.67; }
+      else if (Re <= (R)1000) { a1 = (R)0.3644; a2 = (R)98.33; a3 = (R)-2778; }
+      else if (Re <= (R)5000) { a1 = (R)0.357; a2 = (R)148.62; a3 = (R)-4.75e+4; }
+      else if (Re <= (R)10000) { a1 = (R)0.46; a2 = (R)-490.546; a3 = (R)57.87e+4; }
+      else { a1 = (R)0.5191; a2 = (R)-1662.5; a3 = (R)5.4167e+6; }
+      return a1 + a2/(Re + t) + a3/(Re*Re + t);
+    }
+    case 9: {
+      R Cd0 = drag_wen_yu(Re);
+      return Cd0 * ((R)1 + exp(-(R)0.427/(pow(Ma, (R)4.63) + t) - (R)3/(pow(Re, (R)0.88) + t))) /
+             ((R)1 + Ma/(Re + t)*((R)3.82 + (R)1.28*exp(-(R)1.25*Re/(Ma + t))));
+    }
+    case 10:
+      if (Ma <= (R)1) return henderson1(Re, Ma, G, Tr);
+      if (Ma >= (R)1.75) return henderson2(Re, Ma, G, Tr);
+      {
+        R Cd1 = henderson1(Re, (R)1, G, Tr), Cd2 = henderson2(Re, (R)1.75, G, Tr);
+        return Cd1 + (R)(4.0/3.0)*(Ma - (R)1)*(Cd2 - Cd1);
+      }
+    case 11: {
+      R g = (R)1.25*((R)1 + tanh((R)0.77*log10(Re + t) - (R)1.92));
+      g = pow((R)10, g);
+      R h = (R)2.3 + (R)1.7*pow(Tr, (R)0.5) - (R)2.3*tanh((R)1.17*log10(Ma + t));
+      R Cd0 = drag_wen_yu(Re);
+      return (R)2 + (Cd0 - (R)2)*exp(-(R)3.07*pow(G, (R)0.5)*Ma*g/(Re + t)) + h/(Ma*pow(G, (R)0.5) + t)*exp(-Re/((R)2*Ma + t));
+    }
+    case 12: {
+      R g = ((R)1 + Re*((R)12.278 + (R)0.548*Re)) / ((R)1 + (R)11.278*Re);
+      R h = (R)5.6/((R)1 + Ma) + (R)1.7*pow(Tr, (R)0.5);
+      R Cd0 = drag_wen_yu(Re);
+      return (R)2 + (Cd0 - (R)2)*exp(-(R)3.07*pow(G, (R)0.5)*Ma*g/(Re + t)) + h/(Ma*pow(G, (R)0.5) + t)*exp(-Re/((R)2*Ma + t));
+    }
+    case 13: return (R)0;
+  }
+  return (R)0;
+}
+
+// ------------------------------------------------------------------ heat
+template <typename R> __device__ R heat(R Re, R Pr, R Ma, int sel) {
+  const R t = (R)1e-20;
+  switch (sel) {
+    case 1: return (R)2;
+    case 2: return (R)2.5*pow(Re, (R)0.15) + (R)0.04*Re;
+    case 3: return (R)2 + (R)0.37*pow(Re, (R)0.6)*pow(Pr, (R)(1.0/3.0));
+    case 4: return (R)2 + (R)0.459*pow(Re, (R)0.55)*pow(Pr, (R)(1.0/3.0));
+    case 5: return pow(pow((R)2 + (R)0.654*pow(Re, (R)0.5)*pow(Pr, (R)0.5), (R)-1) + (R)3.42*Ma/(Re*Pr + t), (R)-1);
+    case 6: return (R)2 + (R)0.6*pow(Re, (R)0.5)*pow(Pr, (R)(1.0/3.0));
+    case 7: {
+      R Nu = (R)2 + (R)0.459*pow(Re, (R)0.55)*pow(Pr, (R)0.33);
+      return Nu / ((R)1 + (R)3.42*Ma/(Re*Pr + t)*Nu);
+    }
+    case 8: return (R)0;
+  }
+  return (R)0;
+}
+
+// ------------------------------------------------------------------ evaporation
+template <typename R> __device__ __forceinline__ R blowing(R gamma, R Rg, R mug, R kg, R rhop, R dp, R mp, R mdot) {
+  if (mdot >= (R)0 || mp <= (R)0 || mug <= (R)0 || kg <= (R)0) return (R)1;
+  if (dp <= (R)0 || rhop <= (R)0 || gamma <= (R)1) return (R)1;
+  R cpg = gamma*Rg/(gamma - (R)1);
+  R Pr = mug*cpg/kg;
+  R taud = rhop*dp*dp/((R)18*mug);
+  R b = -(R)1.5*Pr*taud*mdot/mp;
+  if (b != b || b <= (R)1e-10) return (R)1;
+  if (b > (R)500) return (R)0;
+  return b/(exp(b) - (R)1);
+}
+
+template <typename R> __device__ __forceinline__ R molar2mass(R Xs, R Mv, R Mg) { return Xs*Mv/(Xs*Mv + ((R)1 - Xs)*Mg); }
+template <typename R> __device__ __forceinline__ R mass2molar(R Ys, R Mv, R Mg) { return Ys*Mg/(Ys*Mg + ((R)1 - Ys)*Mv); }
+template <typename R> __device__ __forceinline__ R Fcorr(R B) { return B > (R)1.0e-10 ? pow((R)1 + B, (R)0.7)*log((R)1 + B)/B : (R)1; }
+
+template <typename R> struct EvapEnv {
+  R rhog, Tg, gamma, Rg, mug, kg, Tp, dp, cpg, p, Mg, Pr, Sc, Re05;
+  int evap;
+  const double* ep;
+};
+
+// gasSideRate with the five gas-side models (Lib_Evaporation.f90:205-224, 287-521)
+template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, R& md, R& Qd, bool& ovr) {
+  const R pi = (R)kPi;
+  md = (R)0; Qd = (R)0; ovr = false;
+  const double* ep = e.ep;
+  switch (e.evap) {
+    case 1: {
+      R BT = e.cpg*(e.Tg - e.Tp)/(R)ep[EP_LV];
+      if (BT <= (R)0) { md = (R)0; return; }
+      md = -(R)2*pi*e.dp*e.kg/e.cpg*log((R)1 + BT);
+      return;
+    }
+    case 2: {
+      R Dv = e.kg/(e.rhog*e.cpg*(R)ep[EP_LE]);
+      R Sh = (R)2 + (R)0.6*e.Re05*pow(e.Sc, (R)(1.0/3.0));
+      md = -pi*e.dp*e.rhog*Dv*Sh*log((R)1 + BM);
+      return;
+    }
+    case 3: {
+      R Tf = e.Tp + (e.Tg - e.Tp)/(R)3;
+      R rho_f = e.rhog*e.Tg/Tf;
+      R mu_f = e.mug*pow(Tf/e.Tg, (R)0.7);
+      R kl_f = e.kg*pow(Tf/e.Tg, (R)0.7);
+      R cpg_f = e.cpg;
+      R Le = (R)ep[EP_LE];
+      R Dv_f = kl_f/(rho_f*cpg_f*Le);
+      R Sc_f = mu_f*cpg_f*Le/kl_f;
+      R Re_f = e.Re05*e.Re05*rho_f/e.rhog*e.mug/mu_f;
+      R Sh_f = (R)2 + (R)0.6*sqrt(mx(Re_f, (R)0))*pow(Sc_f, (R)(1.0/3.0));
+      md = -pi*e.dp*rho_f*Dv_f*Sh_f*log((R)1 + BM);
+      return;
+    }
+    case 4: {
+      R Le = (R)ep[EP_LE], cpv = (R)ep[EP_CPV];
+      ovr = true;
+      R Dv = e.kg/(e.rhog*e.cpg*Le);
+      R lnBM = log((R)1 + BM);
+      R FM = Fcorr(BM);
+      R Sh0 = (R)2 + (R)0.552*e.Re05*pow(e.Sc, (R)(1.0/3.0));
+      R Shs = (R)2 + (Sh0 - (R)2)/FM;
+      md = -pi*e.dp*e.rhog*Dv*Shs*lnBM;
+      R cpv_eff = cpv > (R)0 ? cpv : e.cpg;
+      R Nu0 = (R)2 + (R)0.552*e.Re05*pow(e.Pr, (R)(1.0/3.0));
+      R Nus = Nu0, BT = (R)0;
+      for (int it = 1; it <= 5; ++it) {
+        R phi = cpv_eff/e.cpg*Shs/Nus/Le;
+        BT = pow((R)1 + BM, phi) - (R)1;
+        if (BT <= (R)0) { BT = BM; Nus = Nu0; break; }
+        R FT = Fcorr(BT);
+        Nus = (R)2 + (Nu0 - (R)2)/FT;
+      }
+      Qd = BT > (R)0 ? -md*cpv_eff*(e.Tg - e.Tp)/BT : (R)0;
+      return;
+    }
+    case 5: {
+      R Le = (R)ep[EP_LE], cpv = (R)ep[EP_CPV], Yinf = (R)ep[EP_YINF], Mv = (R)ep[EP_MV];
+      R Dv = e.kg/(e.rhog*e.cpg*Le);
+      R cpv_eff = cpv > (R)0 ? cpv : e.cpg;
+      R Xs = mn(mass2molar(Ys, Mv, e.Mg), (R)1 - (R)kXsCap);
+      R Xinf = mass2molar(Yinf, Mv, e.Mg);
+      R Minf = Xinf*Mv + ((R)1 - Xinf)*e.Mg;
+      R rhs0 = Mv/Minf*log(((R)1 - Xinf)/((R)1 - Xs));
+      if (rhs0 <= (R)0) return;
+      R Tts = e.Tp/e.Tg;
+      R Lev = e.kg/(cpv_eff*Dv*e.rhog);
+      R mlo = rhs0/mx(Tts, (R)1);
+      R mhi = rhs0/mn(mx(Tts, (R)1.0e-3), (R)1);
+      R mhat = rhs0;
+      for (int it = 1; it <= 30; ++it) {
+        R x = mhat/Lev, f, fp;
+        if (x > (R)1.0e-6) {
+          R E = exp(-x);
+          f = x/((R)1 - E);
+          fp = ((R)1 - E - x*E)/(((R)1 - E)*((R)1 - E));
+        } else {
+          f = (R)1 + (R)0.5*x + x*x/(R)12;
+          fp = (R)0.5 + x/(R)6;
+        }
+        R G = mhat + (Tts - (R)1)*Lev*(f - (R)1) - rhs0;
+        R dG = (R)1 + (Tts - (R)1)*fp;
+        if (fabs(G) <= (R)1.0e-13*mx((R)1, rhs0)) break;
+        if (G > (R)0) mhi = mhat; else mlo = mhat;
+        mhat = mhat - G/dG;
+        if (mhat <= mlo || mhat >= mhi) mhat = (R)0.5*(mlo + mhi);
+      }
+      R Sh = (R)2 + (R)0.6*e.Re05*pow(e.Sc, (R)(1.0/3.0));
+      md = -pi*e.dp*e.rhog*Dv*Sh*mhat;
+      ovr = true;
+      R Nu = (R)2 + (R)0.6*e.Re05*pow(e.Pr, (R)(1.0/3.0));
+      R chi = mn(-md*cpv_eff/(pi*e.dp*e.kg*Nu), (R)700);
+      if (chi > (R)1.0e-9) Qd = -md*cpv_eff*(e.Tg - e.Tp)/(exp(chi) - (R)1);
+      else Qd = pi*e.dp*e.kg*Nu*(e.Tg - e.Tp);
+      return;
+    }
+  }
+}
+
+// evaporation + lkCorrection (Lib_Evaporation.f90:145-261)
+template <typename R> __device__ void evaporation(R rhog, R Tg, R gamma, R Rg, R mug, R kg, R Tp, R dp, R Re,
+                                                  const Mat& m, R& mdot, R& Qd, bool& ovr) {
+  mdot = (R)0; Qd = (R)0; ovr = false;
+  if (m.evap == 0) return;
+  const double* ep = m.ep;
+  EvapEnv<R> e;
+  e.rhog = rhog; e.Tg = Tg; e.gamma = gamma; e.Rg = Rg; e.mug = mug; e.kg = kg; e.Tp = Tp; e.dp = dp;
+  e.evap = m.evap; e.ep = ep;
+  e.cpg = gamma*Rg/(gamma - (R)1);
+  e.p = rhog*Rg*Tg;
+  e.Mg = (R)kRu/Rg;
+  R psat = (R)kPatm*exp(-(R)ep[EP_LVMVRU]*((R)1/Tp - (R)ep[EP_INVTB]));
+  R Xs = psat >= e.p ? (R)1 - (R)kXsCap : mn(psat/e.p, (R)1 - (R)kXsCap);
+  R Ys = molar2mass(Xs, (R)ep[EP_MV], e.Mg);
+  if (Ys <= (R)ep[EP_YINF]) return;
+  R BM = (Ys - (R)ep[EP_YINF])/((R)1 - Ys);
+  if (BM <= (R)0) return;
+  e.Re05 = sqrt(mx(Re, (R)0));
+  e.Pr = mug*e.cpg/kg;
+  e.Sc = e.Pr*(R)ep[EP_LE];
+  gas_side(e, Ys, BM, mdot, Qd, ovr);
+  if (m.intf != 1) return;
+  const R pi = (R)kPi;
+  R LKd2 = (R)2*mug*sqrt((R)2*pi*Tp*(R)kRu/(R)ep[EP_MV])/((R)ep[EP_ALPHAE]*e.Sc*e.p)/dp;
+  R diffPrev = (R)(sizeof(R) == 8 ? 1.79769313486231570e+308 : 3.40282347e+38);
+  R md = mdot, mdNew = (R)0, QdNew = (R)0;
+  bool ovrNew = false;
+  for (int it = 1; it <= 30; ++it) {
+    R beta = -md*e.Pr/((R)2*pi*mug*dp);
+    R XsN = mx(Xs - LKd2*beta, (R)0);
+    R YsN = molar2mass(XsN, (R)ep[EP_MV], e.Mg);
+    mdNew = (R)0; QdNew = (R)0; ovrNew = false;
+    if (YsN > (R)ep[EP_YINF]) {
+      R BMN = (YsN - (R)ep[EP_YINF])/((R)1 - YsN);
+      if (BMN > (R)0) gas_side(e, YsN, BMN, mdNew, QdNew, ovrNew);
+    }
+    R diff = fabs(mdNew - md);
+    if (diff <= (R)1.e-12*fabs(mdNew)) { mdot = mdNew; Qd = QdNew; ovr = ovrNew; return; }
+    if (diff < diffPrev) md = mdNew; else md = (R)0.5*(md + mdNew);
+    diffPrev = diff;
+  }
+  mdot = mdNew; Qd = QdNew; ovr = ovrNew;
+}
+
+// source_make_{MK,IG,AG}
+template <int CL, typename R> __device__ __forceinline__ void source_make(const R* p, const R* F, R* s, R cp, R lv) {
+  const R eps = epsv<R>();
+  s[0] = -F[0];
+  s[1] = -F[0]*p[1] + p[0]*F[1]/(F[5] + eps);
+  s[2] = -F[0]*p[2] + p[0]*F[2]/(F[5] + eps);
+  s[3] = -F[0]*p[3] + p[0]*F[3]/(F[5] + eps);
+  if constexpr (CL == MK) {
+    R n2 = p[1]*p[1] + p[2]*p[2] + p[3]*p[3];
+    s[4] = -F[0]*((R)0.5*n2 + cp*p[4]) - F[0]*lv + F[4] + p[0]*(F[1]*p[1] + F[2]*p[2] + F[3]*p[3])/(F[5] + eps);
+    s[5] = (R)0;
+  } else if constexpr (CL == IG) {
+    R n2 = p[1]*p[1] + p[2]*p[2] + p[3]*p[3];
+    s[4] = -F[0]*(n2 + (R)3*p[4]/p[0]) + (R)2*p[0]*(F[1]*p[1] + F[2]*p[2] + F[3]*p[3])/(F[5] + eps)
+           - (R)6*p[4]/(F[5] + eps);
+    s[5] = -F[0]*cp*p[5] - F[0]*lv + F[4] + (R)0.5*s[4];
+    s[6] = (R)0;
+  } else {
+    s[4] = -F[0]*(p[1]*p[1] + p[4]/p[0]) + p[0]*(F[1]*p[1] + F[1]*p[1])/(F[5] + eps) - (R)2*p[4]/(F[5] + eps);
+    s[5] = -F[0]*(p[1]*p[2] + p[5]/p[0]) + p[0]*(F[2]*p[1] + F[1]*p[2])/(F[5] + eps) - (R)2*p[5]/(F[5] + eps);
+    s[6] = -F[0]*(p[1]*p[3] + p[6]/p[0]) + p[0]*(F[3]*p[1] + F[1]*p[3])/(F[5] + eps) - (R)2*p[6]/(F[5] + eps);
+    s[7] = -F[0]*(p[2]*p[2] + p[7]/p[0]) + p[0]*(F[2]*p[2] + F[2]*p[2])/(F[5] + eps) - (R)2*p[7]/(F[5] + eps);
+    s[8] = -F[0]*(p[2]*p[3] + p[8]/p[0]) + p[0]*(F[3]*p[2] + F[2]*p[3])/(F[5] + eps) - (R)2*p[8]/(F[5] + eps);
+    s[9] = -F[0]*(p[3]*p[3] + p[9]/p[0]) + p[0]*(F[3]*p[3] + F[3]*p[3])/(F[5] + eps) - (R)2*p[9]/(F[5] + eps);
+    s[10] = -F[0]*cp*p[10] - F[0]*lv + F[4] + (R)0.5*s[4] + (R)0.5*s[7] + (R)0.5*s[9];
+    s[11] = (R)0;
+  }
+}
+
+// compute_source_ + cell_surface on the ITC/clamp, non-burning, constant-property path.
+// gas = rho u v w T. Returns tau. INF when Cd == 0.
+template <int CL, typename R> __device__ R cell_source(const R* p, const R* gas, R gR, R ggam, R gk, R gmu,
+                                                      const Mat& m, int drag_sel, int heat_sel, int blow, R* s) {
+  constexpr int nb = NC<CL>::v;
+  const R pi = (R)kPi;
+  R T = p[nb - 2], n = p[nb - 1];
+  R rho_mat = (R)m.rho;
+  R Rp = pow((R)0.75*p[0]/(n*pi*rho_mat), (R)(1.0/3.0));
+  R du = norm2_3(gas[1] - p[1], gas[2] - p[2], gas[3] - p[3]);
+  R Re = (R)2*gas[0]*Rp*du/gmu;
+  R Ma = du/pow(ggam*gR*gas[4], (R)0.5);
+  R Pr = ggam/(ggam - (R)1)*gR*gmu/gk;
+  R Nu = heat(Re, Pr, Ma, heat_sel);
+  R Ts = T;
+  R Tr = Ts/gas[4];
+  R Cd = drag(Re, Ma, ggam, Tr, drag_sel);
+  R F[6];
+  F[1] = gas[1] - p[1]; F[2] = gas[2] - p[2]; F[3] = gas[3] - p[3];
+  R Qconv = (R)2*Nu*gk*pi*Rp*(gas[4] - Ts);
+  R mdot, Qevap; bool ovr;
+  evaporation<R>(gas[0], gas[4], ggam, gR, gmu, gk, Ts, (R)2*Rp, Re, m, mdot, Qevap, ovr);
+  if (ovr) Qconv = Qevap;
+  else if (blow == 1) Qconv = Qconv*blowing<R>(ggam, gR, gmu, gk, rho_mat, (R)2*Rp, (R)(4.0/3.0)*pi*(Rp*Rp*Rp)*rho_mat, mdot);
+  F[0] = -mdot*n;
+  F[4] = Qconv*n;
+  F[4] = F[4] + (R)m.emiss*(R)kSigmaSB*(R)4*pi*Rp*Rp*n*(pow(gas[4], (R)4) - pow(Ts, (R)4));
+  R tau;
+  if (Cd == (R)0) tau = (R)INFINITY;
+  else tau = (R)8*rho_mat*Rp/((R)3*gas[0]*Cd*du + toll_d<R>());
+  F[5] = tau;
+  source_make<CL>(p, F, s, (R)m.cp, (R)m.lv);
+  return tau;
+}
+
+}  // namespace ice

@@ -138,6 +138,8 @@ typedef struct ice_gpu_step_out {
     int32_t have_norm;                  /* residual[] holds the last step's norm          */
     int64_t nfloored;                   /* negative densities floored so far              */
     double  residual[5];                /* residual norm (rho, rho u, rho v, rho w, T)    */
+    double  device_ms;                  /* device time of this call's steps (CUDA events on
+                                           the context's stream)                          */
 } ice_gpu_step_out;
 
 typedef struct ice_gpu_ctx ice_gpu_ctx;

@@ -1,0 +1,174 @@
+"""Parity of the CUDA solve stage (plain FP64 form) with the CPU oracle, through the C ABI.
+
+The bar (the reference's own FP64 CPU path, restated by the oracle): 1e-12 relative L-infinity
+per field after the stated step count, and bit-exact block connectivity and index maps. Where no
+transcendental function enters (no sources, no sensor) the two are bit-identical, and the tests
+say so by asserting equality.
+"""
+import numpy as np
+import pytest
+
+from ice_b200 import abi, configs
+from ice_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from ice_b200 import build
+    build.build()
+    return abi.load_gpu()
+
+
+def groups(nc):
+    g = [[0], [1, 2, 3]]
+    if nc == 12:
+        g.append([4, 5, 6, 7, 8, 9])
+        g += [[10], [11]]
+    else:
+        g += [[v] for v in range(4, nc)]
+    return g
+
+
+def compare(sg, so, case, exact=False):
+    """Largest error of any field relative to the largest value of its group, over every block and
+    family (interior cells)."""
+    worst = 0.0
+    for p, fam in enumerate(case.families):
+        ga = [sg.download(b, p)[2:-2, 2:-2, 2:-2] for b in range(len(case.nodes))]
+        oa = [so.download(b, p)[2:-2, 2:-2, 2:-2] for b in range(len(case.nodes))]
+        for grp in groups(fam.nc):
+            scale = max(max(float(np.abs(o[..., grp]).max()) for o in oa), 1e-300)
+            for v in grp:
+                err = max(float(np.abs(g[..., v] - o[..., v]).max()) for g, o in zip(ga, oa))
+                worst = max(worst, err / scale)
+                if exact:
+                    for g, o in zip(ga, oa):
+                        assert np.array_equal(g[..., v], o[..., v]), (p, v, float(np.abs(g[..., v] - o[..., v]).max()))
+    return worst
+
+
+def run_pair(gpu, orc, make, steps, exact=False, chunks=1):
+    cg, co = make(), make()
+    sg, so = Solver(cg, gpu), Solver(co, orc)
+    for _ in range(chunks):
+        og = sg.step(steps // chunks)
+        oo = so.step(steps // chunks)
+    assert og.status == 0 and oo.status == 0
+    assert og.iter == oo.iter == steps
+    if exact:
+        assert og.time == oo.time and og.dtglobal == oo.dtglobal
+    else:
+        assert abs(og.time - oo.time) <= TOL * abs(oo.time)
+    err = compare(sg, so, cg, exact=exact)
+    assert err <= TOL, err
+    return sg, so, cg
+
+
+def test_riemann_1d_bit_exact(gpu, orc):
+    # config 1 at its full size: 2000 cells, IG, HLLE, minmod, SSP-RK3 (200 of its 1000 steps here;
+    # the full count runs in test_riemann_1d_full_steps)
+    run_pair(gpu, orc, lambda: configs.riemann_1d(n=2000, steps=200), 200, exact=True)
+
+
+@pytest.mark.slow
+def test_riemann_1d_full_steps(gpu, orc):
+    run_pair(gpu, orc, lambda: configs.riemann_1d(n=2000, steps=1000), 1000, exact=True)
+
+
+@pytest.mark.parametrize("closure", ["MK", "IG", "AG"])
+def test_crossing_jets_bit_exact(gpu, orc, closure):
+    # steady (per-cell dt), inlets 402 with injected ghosts, symmetry and extrapolation faces
+    run_pair(gpu, orc, lambda: configs.crossing_jets(closure, steps=300), 300, exact=True)
+
+
+def test_crossing_jets_matches_reference_output(gpu):
+    """The CUDA path against the field the reference's own binary wrote (5000 iterations)."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "crossing_jets_IG.npz")
+    s = Solver(configs.crossing_jets("IG"), gpu)
+    s.step(5000)
+    p = s.download(0, 0)[2, 2:-2, 2:-2]
+    l2 = float(np.sqrt(np.mean((p[..., 0] - g["field"][0]) ** 2)))
+    assert l2 <= 1e-12
+
+
+def test_irs_steady_bit_exact(gpu, orc):
+    def make():
+        c = configs.crossing_jets("IG", steps=100)
+        c.numerics.irs = True
+        c.numerics.irs_beta = 0.5
+        return c
+    run_pair(gpu, orc, make, 100, exact=True)
+
+
+def test_jets_2d_coupled(gpu, orc):
+    # config 2 shape (MK + IG, drag and heat, two 402 jets), reduced to 96^2 for the oracle
+    run_pair(gpu, orc, lambda: configs.jets_2d(n=96, steps=40), 40)
+
+
+def test_cloud_3d_evaporating_ag(gpu, orc):
+    # config 3 shape (AG, Jameson sensor, drag, heat, radiation, evaporation LK + blowing), 24^3
+    run_pair(gpu, orc, lambda: configs.cloud_3d(n=24, steps=12, length=0.0024), 12)
+
+
+def test_multiblock_three_families(gpu, orc):
+    # config 4 shape: a seeded tree of blocks joined by 101 connections, MK + IG + AG
+    run_pair(gpu, orc, lambda: configs.multiblock_tree(nblocks=8, seed=3, lo=5, hi=11, steps=6), 6)
+
+
+def test_index_maps_bit_exact(gpu, orc):
+    case = configs.multiblock_tree(nblocks=10, seed=5, lo=4, hi=9, families=("MK", "AG"), steps=1)
+    sg = Solver(case, gpu, upload=False)
+    so = Solver(configs.multiblock_tree(nblocks=10, seed=5, lo=4, hi=9, families=("MK", "AG"), steps=1), orc,
+                upload=False)
+    for p in range(2):
+        a, b = sg.index_maps(p), so.index_maps(p)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+def test_restart_exact(gpu):
+    """2N steps equal N steps, a download, an upload into a new context and N more, bit for bit
+    (the reference's RestartExact gate)."""
+    make = lambda: configs.multiblock_tree(nblocks=5, seed=7, lo=5, hi=9, steps=10)
+    a = Solver(make(), gpu)
+    a.step(10)
+    ref = a.download_all()
+    b = Solver(make(), gpu)
+    o = b.step(5)
+    mid = b.download_all()
+    c = Solver(make(), gpu, upload=False)
+    c.upload(mid)
+    c.set_time(o.time, o.iter, o.iter)
+    c.step(5)
+    got = c.download_all()
+    for rb, gb in zip(ref, got):
+        for r, g in zip(rb, gb):
+            assert np.array_equal(r[2:-2, 2:-2, 2:-2], g[2:-2, 2:-2, 2:-2])
+
+
+def test_residual_norm(gpu, orc):
+    sg, so, case = run_pair(gpu, orc, lambda: configs.multiblock_tree(nblocks=4, seed=2, lo=5, hi=8, steps=3), 3)
+    tg, fg = sg.residual_norm()
+    to, fo = so.residual_norm()
+    assert np.all(np.abs(tg - to) <= 1e-12 * np.maximum(np.abs(to), 1e-300))
+    assert np.all(np.abs(fg - fo) <= 1e-12 * np.maximum(np.abs(fo), 1e-300))
+
+
+def test_nan_state_is_reported_not_trapped(gpu):
+    """A NaN planted in the state on the host ends the step with ICE_GPU_ESTATE and a status bit
+    (an unphysical first-order face, where the reference's compute_flux stops with error stop 1),
+    and the context stays usable."""
+    case = configs.crossing_jets("IG", n=16, steps=2)
+    st = case.state[0][0].copy()
+    st[2, 5, 5, 0] = 0.5
+    st[2, 5, 5, 1] = np.nan
+    case.state = [[st]]
+    s = Solver(case, gpu)
+    out = s.step(1, check=False)
+    assert out.status & (abi.ST_NAN_STATE | abi.ST_BAD_RECON)
+    assert np.isfinite(s.download(0, 0)[2, 10, 10, 0])

@@ -1,0 +1,152 @@
+"""Pins of the CPU oracle against the reference's own known answers.
+
+- test/Doisneau/{MK,IG,AG}: the fields the reference's binary wrote after 5000 iterations of
+  its crossing-jets validation cases (tests/golden/crossing_jets_*.npz, made by
+  tests/golden/make_golden.py). The reference's gate is L2(rho) <= 1e-4; the oracle is held
+  to 1e-12.
+- test/unit/test_muscl_bounds.f90 B1-B5: the bounds of the limited slopes.
+"""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from ice_b200 import abi, configs
+from ice_b200.solver import Solver
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+ZERO_AT_NEG = ["vanleer", "mc", "superbee", "koren", "umist", "osher", "sweby", "minmod"]
+ALL_LIM = ZERO_AT_NEG + ["vanalbada", "ospre"]
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("closure", ["MK", "IG", "AG"])
+def test_crossing_jets_matches_reference_output(orc, closure):
+    g = np.load(GOLDEN / f"crossing_jets_{closure}.npz")
+    case = configs.crossing_jets(closure)
+    # the case built here is the reference's: same records, codes and inlet angles
+    bc = np.array([(b, i, j, k, f, c, (pay[2] if c == 402 else 0.0)) for (b, i, j, k, f, c, pay) in case.bc_rows])
+    assert np.array_equal(bc[:, :6], g["bc"][:, :6])
+    assert np.allclose(bc[:, 6], g["bc"][:, 6], rtol=0, atol=0)
+    s = Solver(case, orc)
+    out = s.step(5000)
+    assert out.status == 0 and out.iter == 5000
+    p = s.download(0, 0)[2, 2:-2, 2:-2]          # (j, i, v)
+    ref = g["field"]                                 # (v, j, i)
+    l2 = math.sqrt(float(np.mean((p[..., 0] - ref[0]) ** 2)))
+    assert l2 <= 1e-4                                # the reference's own gate
+    assert l2 <= 1e-12
+    # every field on the occupied cells, relative to the largest value of its group (the velocity
+    # components together, the covariance components together)
+    occupied = ref[0] > 1e-6
+    nc = ref.shape[0]
+    groups = [[0], [1, 2, 3]] + ([[4, 5, 6, 7, 8, 9]] if nc == 12 else []) + [[v] for v in range(4 if nc < 12 else 10, nc)]
+    for grp in groups:
+        scale = max(float(np.abs(ref[grp][:, occupied]).max()), 1e-300)
+        for v in grp:
+            err = float(np.abs(p[..., v] - ref[v])[occupied].max()) / scale
+            assert err <= 1e-9, (closure, v, err)
+
+
+def _mk_state(q):
+    return np.array([1.0, q, 0.0, 0.0, 300.0, 1e8])
+
+
+def _faces(orc, lim, q, L, beta=1.0):
+    pl = np.zeros(12); pr = np.zeros(12)
+    st = [_mk_state(x) for x in q]
+    args = [abi.ptr(a) for a in st]
+    rc = orc.reconstruct(abi.CLOSURE["MK"], abi.LIMITER[lim], *args,
+                         0.5 * (L[0] + L[1]), 0.5 * (L[1] + L[2]), 0.5 * (L[2] + L[3]), 0.5 * L[1], 0.5 * L[2],
+                         abi.ptr(pl), abi.ptr(pr), beta)
+    assert rc == 0
+    return pl[1], pr[1]
+
+
+def _between(v, a, b):
+    tol = 8 * np.spacing(max(abs(a), abs(b), np.finfo(float).tiny))
+    return min(a, b) - tol <= v <= max(a, b) + tol
+
+
+@pytest.mark.parametrize("lim", ALL_LIM)
+def test_muscl_bounds_B1(orc, lim):
+    ul, ur = _faces(orc, lim, [1.0, 0.01, 0.0, 0.0], [1.25, 1.25, 1.0, 1.0])
+    assert _between(ul, 0.01, 0.0) and _between(ur, 0.01, 0.0)
+
+
+@pytest.mark.parametrize("lim", ALL_LIM)
+def test_muscl_bounds_B2_random_lines(orc, lim):
+    rng = np.random.default_rng(20261110)
+    bad_face = bad_slope = 0
+    for n in range(2000):
+        r = rng.random(10); sg = rng.random(5)
+        L = 10.0 ** (2.0 * r[:5]); q = 10.0 ** (6.0 * r[5:] - 3.0)
+        monotone = lim not in ZERO_AT_NEG or n % 2 == 1
+        if monotone:
+            q = np.sort(q)
+        else:
+            q = np.where(sg > 0.5, -q, q)
+        ul, ur = _faces(orc, lim, q[:4], L[:4])
+        vl, vr = _faces(orc, lim, q[1:], L[1:])
+        if not (_between(ul, q[1], q[2]) and _between(ur, q[1], q[2]) and _between(vl, q[2], q[3]) and _between(vr, q[2], q[3])):
+            bad_face += 1
+        jump = max(abs(q[2] - q[1]), abs(q[3] - q[2]), np.finfo(float).tiny)
+        if abs((vl - q[2]) - (q[2] - ur)) > max(1e-12 * jump, 4 * np.spacing(abs(q[2]))):
+            bad_slope += 1
+    assert bad_face == 0 and bad_slope == 0
+
+
+@pytest.mark.parametrize("lim", ALL_LIM)
+def test_muscl_bounds_B3_equal_cells_bit_for_bit(orc, lim):
+    rng = np.random.default_rng(7)
+    big = np.finfo(float).max
+    L = abi.LIMITER[lim]
+    for _ in range(500):
+        q = 2.0 * rng.random(4) - 1.0
+        h = 0.01 + rng.random()
+        ul, ur = _faces(orc, lim, q, [h, h, h, h])
+        s0 = (q[1] - q[0]) / (0.5 * (h + h)); s1 = (q[2] - q[1]) / (0.5 * (h + h)); s2 = (q[3] - q[2]) / (0.5 * (h + h))
+        el = q[1] + (orc.limiter(L, s1, s0, big, big) * 1.0) * (0.5 * h)
+        er = q[2] - (orc.limiter(L, s2, s1, big, big) * 1.0) * (0.5 * h)
+        assert ul == el and ur == er
+
+
+@pytest.mark.parametrize("lim", ALL_LIM)
+def test_muscl_bounds_B4_linear_data_exact(orc, lim):
+    rng = np.random.default_rng(11)
+    for _ in range(300):
+        L = 10.0 ** (2.0 * rng.random(4)); a = 2.0 * rng.random() - 1.0
+        x = np.zeros(4)
+        x[0] = 0.5 * L[0]
+        for m in range(1, 4):
+            x[m] = x[m - 1] + 0.5 * (L[m - 1] + L[m])
+        xf = x[1] + 0.5 * L[1]
+        ul, ur = _faces(orc, lim, a * x, L)
+        assert abs(ul - a * xf) <= 1e-12 * abs(a) * x[3] and abs(ur - a * xf) <= 1e-12 * abs(a) * x[3]
+
+
+@pytest.mark.parametrize("lim", ALL_LIM)
+def test_muscl_bounds_B5_injection_side(orc, lim):
+    # dll = 0: the left face of the cell sits on its value (an injected ghost)
+    pl = np.zeros(12); pr = np.zeros(12)
+    st = [_mk_state(x) for x in (0.3, 0.7, 0.2, 0.9)]
+    rc = orc.reconstruct(abi.CLOSURE["MK"], abi.LIMITER[lim], *[abi.ptr(a) for a in st],
+                         1.0, 1.0, 1.0, 0.0, 0.5, abi.ptr(pl), abi.ptr(pr), 1.0)
+    assert rc == 0 and np.isfinite(pl[1]) and np.isfinite(pr[1])
+    assert pl[1] == 0.7 or _between(pl[1], 0.7, 0.2)
+
+
+def test_riemann_1d_runs_and_conserves_mass(orc):
+    case = configs.riemann_1d(n=200, steps=50)
+    s = Solver(case, orc)
+    m0 = float(case.state[0][0][2, 2, 2:-2, 0].sum())
+    out = s.step(50)
+    assert out.status == 0
+    p = s.download(0, 0)[2, 2, 2:-2]
+    assert np.isfinite(p).all()
+    # the waves have not reached the transmissive ends, where the two streams keep entering:
+    # the mass gained per unit section is (rho_L u_L + rho_R |u_R|) t = 1.5 t
+    dx = 1.0 / 200
+    gained = (float(p[:, 0].sum()) - m0) * dx
+    assert abs(gained - 1.5 * out.time) <= 1e-10 * 1.5 * out.time
