@@ -21,9 +21,12 @@ SRC = PKG / "csrc"
 OBJ = PKG / "lib" / "obj"
 OUT = PKG / "lib" / "libice_gpu.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-UNITS = ["ice_gpu.cu", "ice_fam_mk.cu", "ice_fam_ig.cu", "ice_fam_ag.cu"]
-FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-         "--expt-relaxed-constexpr"]
+UNITS = ["ice_gpu.cu", "ice_fam_mk.cu", "ice_fam_ig.cu", "ice_fam_ag.cu"] + [
+    f"ice_stage_{c}_{p}.cu" for c in ("mk", "ig", "ag") for p in ("f64", "f32")]
+# -prec-div=false -prec-sqrt=false -ftz=true act on single precision only: the FP32-flux form
+# divides and takes roots at hardware speed; every FP64 operation stays IEEE and unfused.
+FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-prec-div=false", "-prec-sqrt=false", "-ftz=true", "-lineinfo",
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
 
 
 def nvcc() -> str:
@@ -58,7 +61,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
     hs = headers()
     todo = [u for u in UNITS if force or not _newer(OBJ / (u[:-3] + ".o"), [SRC / u, *hs])]
     if todo:
-        with ThreadPoolExecutor(max_workers=len(todo)) as ex:
+        with ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 4)) as ex:
             logs = list(ex.map(lambda u: _compile(u, verbose, extra), todo))
         if verbose:
             for u, log in zip(todo, logs):

@@ -1,16 +1,23 @@
 // ice_fam.cuh -- the launcher of one family's RK stage, templated on its closure and Riemann
-// solver; each closure's translation unit (ice_fam_mk.cu, ice_fam_ig.cu, ice_fam_ag.cu)
-// instantiates its own, so the heavy FP64 kernels compile in parallel.
+// solver: ghost layers, sensor, connection and boundary fluxes, then the stage kernel of the
+// closure and precision (ice_stage.cuh), and the IRS sweeps when they are on.
 #pragma once
 #include "ice_kernels.cuh"
 
 namespace ice {
 
-inline size_t stage_slots(int TX, int TY, int TZ) {
-  size_t sx = (size_t)(TX + 1) * TY * TZ;
-  size_t sy = TY > 1 ? (size_t)TX * (TY + 1) * TZ : 0;
-  size_t sz = TZ > 1 ? (size_t)TX * TY * (TZ + 1) : 0;
-  return std::max(sx, std::max(sy, sz));
+template <int CL> inline void launch_stage_of(const LaunchArgs& a, bool write_r) {
+  const bool f32 = a.precision == ICE_PREC_FP32FLUX && !write_r;
+  if constexpr (CL == MK) { if (f32) launch_stage_mk_f32(a, write_r); else launch_stage_mk_f64(a, write_r); }
+  else if constexpr (CL == IG) { if (f32) launch_stage_ig_f32(a, write_r); else launch_stage_ig_f64(a, write_r); }
+  else { if (f32) launch_stage_ag_f32(a, write_r); else launch_stage_ag_f64(a, write_r); }
+}
+
+template <int CL> inline void launch_source_of(const LaunchArgs& a) {
+  const bool f32 = a.precision == ICE_PREC_FP32FLUX;
+  if constexpr (CL == MK) { if (f32) launch_source_mk_f32(a); else launch_source_mk_f64(a); }
+  else if constexpr (CL == IG) { if (f32) launch_source_ig_f32(a); else launch_source_ig_f64(a); }
+  else { if (f32) launch_source_ag_f32(a); else launch_source_ag_f64(a); }
 }
 
 template <int CL, int RS>
@@ -19,6 +26,10 @@ void launch_family_t(const LaunchArgs& a) {
   cudaStream_t s = a.s;
   auto tick = [&](int cls) { if (a.tick) a.tick(a.tick_ctx, cls, s); };
   auto grid = [](long long n, int t) { return (unsigned)((n + t - 1) / t); };
+  if (a.F.coupled) {          // compute_source comes first in the stage (Mod_Explicit.f90:111-117)
+    launch_source_of<CL>(a);
+    tick(KC_SOURCE);
+  }
   if (a.nrec > 0) {
     k_ghost1<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
     k_ghost2<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
@@ -31,16 +42,12 @@ void launch_family_t(const LaunchArgs& a) {
   if (a.nown > 0) k_conn<CL, RS><<<grid(a.nown, 64), 64, 0, s>>>(a.G, a.F, a.recs, a.own, a.nown, a.st);
   if (a.nbc > 0) k_bound<CL, RS><<<grid(a.nbc, 64), 64, 0, s>>>(a.G, a.F, a.recs, a.bfirst, a.blist, a.nbc, a.st);
   if (a.nown > 0 || a.nbc > 0) tick(KC_BOUND);
-  size_t sh = sizeof(double) * nc * stage_slots(a.TX, a.TY, a.TZ);
   if (!a.irs) {
-    if (a.precision == ICE_PREC_FP32FLUX)
-      k_stage<CL, RS, false, float><<<a.ntile, 256, sh, s>>>(a.G, a.F, a.tiles, a.ndir, a.TX, a.TY, a.TZ, a.st);
-    else
-      k_stage<CL, RS, false, double><<<a.ntile, 256, sh, s>>>(a.G, a.F, a.tiles, a.ndir, a.TX, a.TY, a.TZ, a.st);
+    launch_stage_of<CL>(a, false);
     tick(KC_STAGE);
     return;
   }
-  k_stage<CL, RS, true, double><<<a.ntile, 256, sh, s>>>(a.G, a.F, a.tiles, a.ndir, a.TX, a.TY, a.TZ, a.st);
+  launch_stage_of<CL>(a, true);
   tick(KC_STAGE);
   // two Jacobi sweeps per direction; each direction smooths the residual the last one left
   const long long NI = a.G.NI;

@@ -65,7 +65,7 @@ struct FamHost {
   DevBuf<unsigned char> inj;
   DevBuf<double> dt, tau, beta;
   DevBuf<int> bmap;
-  DevBuf<double> Rb, connF, resid, resid2, resid3;
+  DevBuf<double> Rb, connF, resid, resid2, resid3, src;
   DevBuf<DRec> recs;
   DevBuf<int> bfirst, blist, own;
   int nrec = 0, nbc = 0, nown = 0, ncf = 0;
@@ -89,7 +89,7 @@ struct ice_gpu_ctx {
   FamHost fam[kMaxF];
   std::vector<HRec> recs;
   DevBuf<Tile> tiles;
-  int ntile = 0, TX = 0, TY = 0, TZ = 0;
+  int ntile = 0, TX = 0, TY = 0, KZ = 0;
   DevBuf<NormChunk> chunks;
   DevBuf<double> npart;
   int nchunk = 0;
@@ -148,6 +148,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   F.dt = c->P.time_accurate ? nullptr : H.dt.p;
   F.dtg = &c->st.p->dtglobal;
   F.tau = H.tau.p;
+  F.S = H.src.p;
   F.bmap = H.bmap.p;
   F.Rb = H.Rb.p; F.Rbw = H.Rb.p;
   F.connF = H.connF.p;
@@ -179,7 +180,7 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   a.recs = H.recs.p; a.nrec = H.nrec;
   a.own = H.own.p; a.nown = H.nown;
   a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc;
-  a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.TZ = c->TZ;
+  a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.KZ = c->KZ;
   a.ndir = c->P.ndir; a.sd = c->P.shock_detector; a.irs = c->P.irs; a.precision = c->P.precision;
   a.irs_beta = c->P.irs_beta;
   a.resid = H.resid.p; a.resid2 = H.resid2.p; a.resid3 = H.resid3.p;
@@ -231,7 +232,7 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
   long long n = 2 + c->P.nfam;
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
-    long long per = (H.nrec > 0 ? 2 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0);
+    long long per = (H.nrec > 0 ? 2 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) + (c->P.coupled ? 1 : 0);
     per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
     n += per * c->P.nrk;
   }
@@ -239,20 +240,27 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
 }
 
 // ---------------------------------------------------------------- set-up helpers
-static void tile_shape(int ndir, int& TX, int& TY, int& TZ) {
-  if (ndir == 1) { TX = 256; TY = 1; TZ = 1; }
-  else if (ndir == 2) { TX = 32; TY = 8; TZ = 1; }
-  else { TX = 32; TY = 4; TZ = 2; }
+// The stage kernel's tiles: TX x TY columns of a block (x faces of TX - 1 cells and y faces of
+// TY - 1 cells per tile, the last column and row being the next tile's), KZ planes per tile.
+static void tile_shape(int ndir, int& TX, int& TY, int& KZ) {
+  if (ndir == 1) { TX = 256; TY = 1; KZ = 1; }
+  else if (ndir == 2) { TX = 32; TY = 8; KZ = 1; }
+  else { TX = 32; TY = 8; KZ = 32; }
+  if (const char* e = getenv("ICE_GPU_TILE")) {        // "TXxTYxKZ", for the tile tuner
+    int a, b, k;
+    if (sscanf(e, "%dx%dx%d", &a, &b, &k) == 3 && a * b == 256 && a >= 2 && k >= 1) { TX = a; TY = b; KZ = k; }
+  }
 }
 
 static int build_tiles(ice_gpu_ctx* c) {
-  tile_shape(c->P.ndir, c->TX, c->TY, c->TZ);
+  tile_shape(c->P.ndir, c->TX, c->TY, c->KZ);
   std::vector<Tile> t;
   for (int b = 0; b < c->nb; ++b) {
     int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
-    for (int k = 0; k < nk; k += c->TZ)
-      for (int j = 0; j < nj; j += c->TY)
-        for (int i = 0; i < ni; i += c->TX) t.push_back(Tile{b, i, j, k});
+    int sx = ni >= 2 ? c->TX - 1 : 1, sy = nj >= 2 ? std::max(c->TY - 1, 1) : 1;
+    for (int k = 0; k < nk; k += c->KZ)
+      for (int j = 0; j < nj; j += sy)
+        for (int i = 0; i < ni; i += sx) t.push_back(Tile{b, i, j, k});
   }
   c->ntile = (int)t.size();
   CK(c->tiles.alloc(t.size()));
@@ -339,6 +347,7 @@ int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims
     std::vector<double> one(I, 1.0);
     CKC(cudaMemcpy(H.beta.p, one.data(), I * sizeof(double), cudaMemcpyHostToDevice));
     CKC(H.bmap.alloc(I)); CKC(cudaMemset(H.bmap.p, 0xFF, I * sizeof(int)));
+    if (P->coupled) CKC(H.src.alloc((size_t)H.nc * I));
     if (P->irs) { CKC(H.resid.alloc((size_t)H.nc * I)); CKC(H.resid2.alloc((size_t)H.nc * I)); CKC(H.resid3.alloc((size_t)H.nc * I)); }
   }
   CKC(c->st.alloc(1));
@@ -555,6 +564,8 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
       d.normal_dir = r.normal_dir != 0.0;
       d.massflux = r.massflux; d.velocity = r.velocity; d.alpha = r.alpha; d.beta = r.beta;
       d.temperature = r.temperature; d.radius = r.radius; d.gfixed = r.gfixed;
+      d.ca = cos(r.alpha); d.sa = sin(r.alpha); d.cb = cos(r.beta); d.sb = sin(r.beta);
+      d.vol_p = 4.0/3.0*kPi*pow(r.radius, 3.0);
     }
     H.nrec = (int)grp.size();
     CK(H.recs.alloc(dr.size()));

@@ -19,33 +19,52 @@ template <typename R> struct CStencil {        // converted to R (FP32-flux form
   __device__ __forceinline__ R operator()(int s, int v) const { return (R)__ldg(P + (long long)v * NG + g0 + s * st); }
 };
 
-// One interior face along d between 0-based cells c (lower, coords ci,cj,ck) and c+1.
+template <typename R, int NC_> struct RegStencil {   // the four cells held in registers (FP32 form)
+  R v[4][NC_];
+  __device__ __forceinline__ R operator()(int s, int q) const { return v[s][q]; }
+};
+
+// One interior face along d between the 0-based cells (i,j,k) and its upper neighbour:
 // face_flux + compute_flux_ (Mod_Fluxes.f90:599-685). Returns true on an unphysical
-// first-order face.
-template <int CL, int RS, typename R>
+// first-order face. The plain form reads the stencil through L1 as the reconstruction needs it;
+// the FP32 form converts it once into registers.
+template <int CL, int RS, int LIM, typename R>
 __device__ __forceinline__ bool face_flux(const Geo& G, const FamDev& F, const DBlock& B, int d, int i, int j, int k,
                                          R* flux) {
   constexpr int nc = NC<CL>::v;
-  int c = d == 0 ? i : d == 1 ? j : k;
-  int n = d == 0 ? B.ni : d == 1 ? B.nj : B.nk;
-  int o0 = d == 0, o1 = d == 1, o2 = d == 2;
+  const int c = d == 0 ? i : d == 1 ? j : k;
+  const int n = d == 0 ? B.ni : d == 1 ? B.nj : B.nk;
+  const int o0 = d == 0, o1 = d == 1, o2 = d == 2;
   R bf = (R)1;
   if (F.beta) bf = (R)mn(F.beta[iidx(B, i, j, k)], F.beta[iidx(B, i + o0, j + o1, k + o2)]);
-  R len[4];
-#pragma unroll
-  for (int s = -1; s <= 2; ++s) len[s + 1] = (R)G.dl[(long long)d * G.NR + ridx(B, i + s * o0, j + s * o1, k + s * o2)];
-  if (c == 0 && F.inj[gidx(B, i - o0, j - o1, k - o2)]) len[0] = (R)0;
-  if (c == n - 2 && F.inj[gidx(B, i + 2 * o0, j + 2 * o1, k + 2 * o2)]) len[3] = (R)0;
-  R dl0 = (R)0.5*(len[0] + len[1]), dl1 = (R)0.5*(len[1] + len[2]), dl2 = (R)0.5*(len[2] + len[3]);
-  R dll = (R)0.5*len[1], dlr = (R)0.5*len[2];
-  long long st = gstride(B, d);
-  CStencil<R> q{F.Up, G.NG, gidx(B, i, j, k) - st, st};
+  const double* dl = G.dl + (long long)d * G.NR;
+  const long long r0 = ridx(B, i, j, k);
+  const long long rs = d == 0 ? 1LL : d == 1 ? (long long)(B.ni + 2) : (long long)(B.ni + 2) * (B.nj + 2);
+  R l0 = (R)dl[r0 - rs], l1 = (R)dl[r0], l2 = (R)dl[r0 + rs], l3 = (R)dl[r0 + 2 * rs];
+  const long long st = gstride(B, d);
+  const long long g0 = gidx(B, i, j, k) - st;
+  if (c == 0 && F.inj[g0]) l0 = (R)0;
+  if (c == n - 2 && F.inj[g0 + 3 * st]) l3 = (R)0;
+  R dl0 = (R)0.5*(l0 + l1), dl1 = (R)0.5*(l1 + l2), dl2 = (R)0.5*(l2 + l3);
+  R dll = (R)0.5*l1, dlr = (R)0.5*l2;
   R pl[nc], pr[nc], fl[nc];
-  bool bad = reconstruct<CL, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
-  long long fi = fidx(B, d, i, j, k, c + 1);
-  long long NF = G.NF[d];
-  R nrm[3] = {(R)G.face[d][fi], (R)G.face[d][NF + fi], (R)G.face[d][2 * NF + fi]};
-  R area = (R)G.face[d][3 * NF + fi];
+  bool bad;
+  if constexpr (sizeof(R) == 8) {
+    CStencil<R> q{F.Up, G.NG, g0, st};
+    bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
+  } else {
+    RegStencil<R, nc> q;
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2)
+#pragma unroll
+      for (int v = 0; v < nc; ++v) q.v[s2][v] = (R)__ldg(F.Up + (long long)v * G.NG + g0 + s2 * st);
+    bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
+  }
+  const long long fi = fidx(B, d, i, j, k, c + 1);
+  const long long NF = G.NF[d];
+  const double* fc = G.face[d];
+  R nrm[3] = {(R)fc[fi], (R)fc[NF + fi], (R)fc[2 * NF + fi]};
+  R area = (R)fc[3 * NF + fi];
   riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
   for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
@@ -82,7 +101,7 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
     if (F.inj[gidx(B, ip, jp, kp)]) dl2 = 0.5*dl_m;
     long long a[4] = {gidx(B, ig2, jg2, kg2), gidx(B, ig, jg, kg), gidx(B, i, j, k), gidx(B, ip, jp, kp)};
     auto q = [&](int s, int v) { return P[(long long)v * G.NG + a[s]]; };
-    bad = reconstruct<CL, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
+    bad = reconstruct<CL, LIM_ANY, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
     riemann<CL, RS, double>(pl, pr, nrm, fl, F.mat.cp);
 #pragma unroll
     for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
@@ -96,7 +115,7 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
     if (F.inj[gidx(B, ip, jp, kp)]) dl0 = 0.5*dl_m;
     long long a[4] = {gidx(B, ip, jp, kp), gidx(B, i, j, k), gidx(B, ig, jg, kg), gidx(B, ig2, jg2, kg2)};
     auto q = [&](int s, int v) { return P[(long long)v * G.NG + a[s]]; };
-    bad = reconstruct<CL, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
+    bad = reconstruct<CL, LIM_ANY, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
     riemann<CL, RS, double>(pl, pr, nrm, fl, F.mat.cp);
 #pragma unroll
     for (int v = 0; v < nc; ++v) flux[v] = -(fl[v] * area);
@@ -266,7 +285,7 @@ __global__ void k_ghost1(Geo G, FamDev F, const DRec* recs, int nrec) {
         double v3[3], speed;
         auto injv = [&](double sp) {
           if (r.normal_dir) { v3[0] = sp*inward[0]; v3[1] = sp*inward[1]; v3[2] = sp*inward[2]; }
-          else { v3[0] = sp*cos(r.beta)*cos(r.alpha); v3[1] = sp*cos(r.beta)*sin(r.alpha); v3[2] = sp*sin(r.beta); }
+          else { v3[0] = sp*r.cb*r.ca; v3[1] = sp*r.cb*r.sa; v3[2] = sp*r.sb; }
         };
         if (r.type == 401) {
           double gu = gas[1 * G.NI + q], gvv = gas[2 * G.NI + q], gw = gas[3 * G.NI + q];
@@ -291,7 +310,7 @@ __global__ void k_ghost1(Geo G, FamDev F, const DRec* recs, int nrec) {
           gv[0] = r.massflux/fabs(vn);
           gv[nc - 2] = r.temperature;
         }
-        gv[nc - 1] = gv[0]/F.mat.rho/(4.0/3.0*kPi*pow(r.radius, 3.0));
+        gv[nc - 1] = gv[0]/F.mat.rho/r.vol_p;
         if constexpr (CL == IG) gv[4] = 1e-6;
         if constexpr (CL == AG) { gv[4] = 1e-6; gv[7] = 1e-6; gv[9] = 1e-6; }
       }
@@ -405,135 +424,191 @@ __global__ void k_bound(Geo G, FamDev F, const DRec* recs, const int* first, con
 
 // ------------------------------------------------------------------ the stage
 
-// One CTA = one tile of TX x TY x TZ cells of one block (256 threads). For each direction the
-// faces of the tile are computed once into shared memory, then every cell takes its two faces in
-// the reference's odd-then-even order; then source, residual and the RK update.
-template <int CL, int RS, bool WRITE_R, typename R>
-__global__ void __launch_bounds__(256)
-k_stage(Geo G, FamDev F, const Tile* tiles, int ndir, int TX, int TY, int TZ, Status* st) {
+// compute_source (Mod_Sources.f90:19-72): the source of every cell of one family, from the state
+// at the start of the stage and the frozen gas; written to S (and tau, on the last stage), which
+// the stage kernel adds to the residual. Its own kernel, so that the iterative closures do not
+// share the stencil kernel's registers.
+template <int CL, typename R>
+__global__ void __launch_bounds__(256) k_source(Geo G, FamDev F) {
   constexpr int nc = NC<CL>::v;
-  const int NT = TX * TY * TZ;
-  extern __shared__ double smem[];   // [nc][slots of the direction]
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.NI) return;
+  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  int i, j, k; decode(B, q, i, j, k);
+  const long long g = gidx(B, i, j, k);
+  R p[nc], gas[5], s[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) p[v] = (R)F.Up[(long long)v * G.NG + g];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) gas[v] = (R)G.gas[(long long)v * G.NI + q];
+  R tau = cell_source<CL, R>(p, gas, (R)G.gas[5 * G.NI + q], (R)G.gas[6 * G.NI + q], (R)G.gas[7 * G.NI + q],
+                             (R)G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, s);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) F.S[(long long)v * G.NI + q] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)s[v];
+  if (F.write_tau) F.tau[q] = (double)tau;
+}
+
+// The stage kernel. One CTA of TX x TY threads (256) owns a column tile of one block and marches
+// up a chunk of KZ planes. On each plane every thread computes exactly one x face (the face below
+// its cell), one y face and one z face (the face above its cell; the one below comes from the
+// plane before, or is computed once at the chunk's first plane) into shared memory, so the work is
+// the same for every thread; then each cell of the tile's (TX-1) x (TY-1) interior takes its two
+// faces per direction in the reference's odd-then-even order (Mod_Fluxes.f90:470-506), adds the
+// source, forms R = (R/vol + S) dt, and applies the RK stage in conservative variables with the
+// reference's floors and checks (Lib_Newstate.f90:198-219).
+#ifndef ICE_STAGE_MINB
+#define ICE_STAGE_MINB 1      // resident CTAs per SM the register allocation is held to
+#endif
+template <int CL, int RS, int LIM, typename R>
+__global__ void __launch_bounds__(256, ICE_STAGE_MINB)
+k_stage(Geo G, FamDev F, const Tile* tiles, int TX, int TY, int KZ, int write_r, Status* st) {
+  constexpr int nc = NC<CL>::v;
+  extern __shared__ double smem[];
+  const int NT = TX * TY;
+  double* Fx = smem;                  // [nc][NT]
+  double* Fy = smem + nc * NT;
+  double* Fz0 = smem + 2 * nc * NT;
+  double* Fz1 = smem + 3 * nc * NT;
   const Tile t = tiles[blockIdx.x];
   const DBlock& B = G.blk[t.b];
   const int tid = threadIdx.x;
-  const int tx = tid % TX, ty = (tid / TX) % TY, tz = tid / (TX * TY);
-  const int i = t.i0 + tx, j = t.j0 + ty, k = t.k0 + tz;
-  const bool inside = i < B.ni && j < B.nj && k < B.nk;
-  const int dims[3] = {B.ni, B.nj, B.nk};
-  const int org[3] = {t.i0, t.j0, t.k0};
+  const int tx = tid % TX, ty = tid / TX;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool ax = B.ni >= 2, ay = B.nj >= 2, az = B.nk >= 2;
+  const bool col = i < B.ni && j < B.nj;
+  const bool owner = col && (ax ? tx < TX - 1 : tx == 0) && (ay ? ty < TY - 1 : ty == 0);
+  const int k1 = min(t.k0 + KZ, B.nk);
   bool bad = false;
-
-  double r[nc];
-  int bc = -1;
-  if (inside) bc = F.bmap[iidx(B, i, j, k)];
+  double* flo = Fz0;
+  double* fhi = Fz1;
+  if (az && col && t.k0 >= 1) {       // the face below the chunk's first plane
+    R fl[nc];
+    bad |= face_flux<CL, RS, LIM, R>(G, F, B, 2, i, j, t.k0 - 1, fl);
 #pragma unroll
-  for (int v = 0; v < nc; ++v) r[v] = (bc >= 0 && inside) ? F.Rb[(long long)bc * nc + v] : 0.0;
-
-  for (int d = 0; d < ndir; ++d) {
-    if (dims[d] < 2) continue;
-    // face slots: the lower cell runs over org[d]-1 .. org[d]+T[d]-1 along d
-    const int sx = d == 0 ? TX + 1 : TX, sy = d == 1 ? TY + 1 : TY, sz = d == 2 ? TZ + 1 : TZ;
-    const int ns = sx * sy * sz;
-    for (int s = tid; s < ns; s += NT) {
-      int a = s % sx, b = (s / sx) % sy, c = s / (sx * sy);
-      int fi = t.i0 + a - (d == 0), fj = t.j0 + b - (d == 1), fk = t.k0 + c - (d == 2);
-      int cl = d == 0 ? fi : d == 1 ? fj : fk;
-      bool ok = cl >= 0 && cl <= dims[d] - 2 && fi < B.ni && fj < B.nj && fk < B.nk && fi >= 0 && fj >= 0 && fk >= 0;
-      if (ok) {
-        R fl[nc];
-        bad |= face_flux<CL, RS, R>(G, F, B, d, fi, fj, fk, fl);
+    for (int v = 0; v < nc; ++v) flo[v * NT + tid] = (double)fl[v];
+  }
+  for (int k = t.k0; k < k1; ++k) {
+    if (ax && col && i >= 1) {        // x face below (i,j,k)
+      R fl[nc];
+      bad |= face_flux<CL, RS, LIM, R>(G, F, B, 0, i - 1, j, k, fl);
 #pragma unroll
-        for (int v = 0; v < nc; ++v) smem[v * ns + s] = (double)fl[v];
-      }
+      for (int v = 0; v < nc; ++v) Fx[v * NT + tid] = (double)fl[v];
+    }
+    if (ay && col && j >= 1) {        // y face below (i,j,k)
+      R fl[nc];
+      bad |= face_flux<CL, RS, LIM, R>(G, F, B, 1, i, j - 1, k, fl);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) Fy[v * NT + tid] = (double)fl[v];
+    }
+    if (az && col && k <= B.nk - 2) { // z face above (i,j,k)
+      R fl[nc];
+      bad |= face_flux<CL, RS, LIM, R>(G, F, B, 2, i, j, k, fl);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) fhi[v * NT + tid] = (double)fl[v];
     }
     __syncthreads();
-    if (inside) {
-      const int c = d == 0 ? i : d == 1 ? j : k;
-      const int n = dims[d];
-      const int tc = d == 0 ? tx : d == 1 ? ty : tz;
-      // slot of the face below the cell (lower cell c-1) and above it (lower cell c)
-      int slo = tx + ty * sx + tz * sx * sy;
-      int sup = slo + (d == 0 ? 1 : d == 1 ? sx : sx * sy);
-      (void)tc;
-      const int ci = c + 1;
-      if (ci % 2 == 1) {
-        if (ci < n) {
+    if (owner) {
+      const long long q = iidx(B, i, j, k);
+      const int bc = F.bmap[q];
+      double r[nc];
 #pragma unroll
-          for (int v = 0; v < nc; ++v) r[v] = r[v] - smem[v * ns + sup];
-        }
-        if (ci > 1) {
+      for (int v = 0; v < nc; ++v) r[v] = bc >= 0 ? F.Rb[(long long)bc * nc + v] : 0.0;
+      // direction 1: face tid+1 is the cell's upper face, face tid its lower one
+      if (ax) {
+        const int ci = i + 1, n = B.ni;
+        if (ci % 2 == 1) {
+          if (ci < n) {
 #pragma unroll
-          for (int v = 0; v < nc; ++v) r[v] = r[v] + smem[v * ns + slo];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - Fx[v * NT + tid + 1];
+          }
+          if (ci > 1) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + Fx[v * NT + tid];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + Fx[v * NT + tid];
+          if (ci < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - Fx[v * NT + tid + 1];
+          }
         }
+      }
+      if (ay) {
+        const int cj = j + 1, n = B.nj;
+        if (cj % 2 == 1) {
+          if (cj < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - Fy[v * NT + tid + TX];
+          }
+          if (cj > 1) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + Fy[v * NT + tid];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + Fy[v * NT + tid];
+          if (cj < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - Fy[v * NT + tid + TX];
+          }
+        }
+      }
+      if (az) {
+        const int ck = k + 1, n = B.nk;
+        if (ck % 2 == 1) {
+          if (ck < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - fhi[v * NT + tid];
+          }
+          if (ck > 1) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + flo[v * NT + tid];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + flo[v * NT + tid];
+          if (ck < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - fhi[v * NT + tid];
+          }
+        }
+      }
+      const long long g = gidx(B, i, j, k);
+      double p[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
+      double s[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) s[v] = F.coupled ? F.S[(long long)v * G.NI + q] : 0.0;
+      const double dt = F.dt ? F.dt[q] : *F.dtg;
+      const double vol = G.vol[q];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) r[v] = (r[v]/vol + s[v]) * dt;
+#pragma unroll
+      for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) r[v] = 0.0;
+      if (write_r) {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) F.resid[(long long)v * G.NI + q] = r[v];
       } else {
+        double po[nc], co[nc], cn[nc];
 #pragma unroll
-        for (int v = 0; v < nc; ++v) r[v] = r[v] + smem[v * ns + slo];
-        if (ci < n) {
+        for (int v = 0; v < nc; ++v) po[v] = F.U0[(long long)v * G.NG + g];
+        prim2cons<CL, double>(po, co, F.mat.cp);
+        prim2cons<CL, double>(p, cn, F.mat.cp);
 #pragma unroll
-          for (int v = 0; v < nc; ++v) r[v] = r[v] - smem[v * ns + sup];
-        }
+        for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + r[v]) * F.rk; cn[v] = co[v] + rr; }
+        if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
+        cons2prim<CL>(cn, p, F.mat.cp);
+        if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
+#pragma unroll
+        for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];
       }
     }
     __syncthreads();
+    double* tmp = flo; flo = fhi; fhi = tmp;
   }
-  (void)org;
   if (bad) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
-  if (!inside) return;
-
-  const long long q = iidx(B, i, j, k);
-  const long long g = gidx(B, i, j, k);
-  double p[nc];
-#pragma unroll
-  for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
-  double s[nc];
-#pragma unroll
-  for (int v = 0; v < nc; ++v) s[v] = 0.0;
-  if (F.coupled) {
-    double gas[5] = {G.gas[q], G.gas[G.NI + q], G.gas[2 * G.NI + q], G.gas[3 * G.NI + q], G.gas[4 * G.NI + q]};
-    if constexpr (sizeof(R) == 8) {
-      double tau = cell_source<CL, double>(p, gas, G.gas[5 * G.NI + q], G.gas[6 * G.NI + q], G.gas[7 * G.NI + q],
-                                           G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, s);
-      if (F.write_tau) F.tau[q] = tau;
-    } else {
-      R pf[nc], gf[5], sf[nc];
-#pragma unroll
-      for (int v = 0; v < nc; ++v) pf[v] = (R)p[v];
-#pragma unroll
-      for (int v = 0; v < 5; ++v) gf[v] = (R)gas[v];
-      R tau = cell_source<CL, R>(pf, gf, (R)G.gas[5 * G.NI + q], (R)G.gas[6 * G.NI + q], (R)G.gas[7 * G.NI + q],
-                                 (R)G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, sf);
-#pragma unroll
-      for (int v = 0; v < nc; ++v) s[v] = (double)sf[v];
-      if (F.write_tau) F.tau[q] = (double)tau;
-    }
-#pragma unroll
-    for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) s[v] = 0.0;
-  }
-  const double dt = F.dt ? F.dt[q] : *F.dtg;
-  const double vol = G.vol[q];
-#pragma unroll
-  for (int v = 0; v < nc; ++v) r[v] = (r[v]/vol + s[v]) * dt;
-#pragma unroll
-  for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) r[v] = 0.0;
-  if constexpr (WRITE_R) {
-#pragma unroll
-    for (int v = 0; v < nc; ++v) F.resid[(long long)v * G.NI + q] = r[v];
-    return;
-  } else {
-    double po[nc], co[nc], cn[nc];
-#pragma unroll
-    for (int v = 0; v < nc; ++v) po[v] = F.U0[(long long)v * G.NG + g];
-    prim2cons<CL, double>(po, co, F.mat.cp);
-    prim2cons<CL, double>(p, cn, F.mat.cp);
-#pragma unroll
-    for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + r[v]) * F.rk; cn[v] = co[v] + rr; }
-    if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
-    cons2prim<CL>(cn, p, F.mat.cp);
-    if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
-#pragma unroll
-    for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];
-  }
 }
 
 // ------------------------------------------------------------------ IRS and the separate update

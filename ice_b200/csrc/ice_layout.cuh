@@ -34,6 +34,9 @@ struct DRec {                // one boundary record, 0-based cells
   int pb, pi, pj, pk;        // the partner's cell (connections)
   int normal_dir;
   double massflux, velocity, alpha, beta, temperature, radius, gfixed;
+  // host-computed once per record (the platform libm of the driver's host, as the
+  // reference's ghost_record evaluates them): cos/sin of the inlet angles and 4/3 pi r^3
+  double ca, sa, cb, sb, vol_p;
 };
 
 struct Status {
@@ -80,6 +83,7 @@ struct FamDev {              // what the kernels of one family read
   const double* dt;          // NI (steady) or null
   const double* dtg;         // &status->dtglobal (time-accurate)
   double* tau;               // NI
+  double* S;                 // [v][NI]: the stage's source (coupled runs)
   const int* bmap;           // NI: boundary-cell index or -1
   const double* Rb;          // [nbcell][nc]
   double* Rbw;
@@ -99,7 +103,7 @@ struct LaunchArgs {
   const DRec* recs; int nrec;
   const int* own; int nown;
   const int* bfirst; const int* blist; int nbc;
-  const Tile* tiles; int ntile; int TX, TY, TZ;
+  const Tile* tiles; int ntile; int TX, TY, KZ;
   int ndir, sd, irs, precision;
   double irs_beta;
   double* resid; double* resid2; double* resid3;
@@ -109,11 +113,24 @@ struct LaunchArgs {
   void* tick_ctx;
 };
 
-enum { KC_DT = 0, KC_GHOST, KC_BETA, KC_BOUND, KC_STAGE, KC_IRS, KC_NORM, KC_N };
+enum { KC_DT = 0, KC_GHOST, KC_BETA, KC_BOUND, KC_STAGE, KC_IRS, KC_NORM, KC_SOURCE, KC_N };
 
+// the boundary and ghost kernels of a family's stage (ice_fam_<closure>.cu), which call the stage
+// kernel of its closure and precision (ice_stage_<closure>_<f64|f32>.cu)
 void launch_family_mk(const LaunchArgs& a);
 void launch_family_ig(const LaunchArgs& a);
 void launch_family_ag(const LaunchArgs& a);
-size_t stage_smem_bytes(int nc, int TX, int TY, int TZ);
+void launch_source_mk_f64(const LaunchArgs& a);
+void launch_source_mk_f32(const LaunchArgs& a);
+void launch_source_ig_f64(const LaunchArgs& a);
+void launch_source_ig_f32(const LaunchArgs& a);
+void launch_source_ag_f64(const LaunchArgs& a);
+void launch_source_ag_f32(const LaunchArgs& a);
+void launch_stage_mk_f64(const LaunchArgs& a, bool write_r);
+void launch_stage_mk_f32(const LaunchArgs& a, bool write_r);
+void launch_stage_ig_f64(const LaunchArgs& a, bool write_r);
+void launch_stage_ig_f32(const LaunchArgs& a, bool write_r);
+void launch_stage_ag_f64(const LaunchArgs& a, bool write_r);
+void launch_stage_ag_f32(const LaunchArgs& a, bool write_r);
 
 }  // namespace ice

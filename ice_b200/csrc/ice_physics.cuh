@@ -26,6 +26,7 @@
 #include <cstdint>
 #include <cmath>
 #include "../../include/ice_gpu.h"
+#include "../../include/ice_math.h"
 
 namespace ice {
 
@@ -61,6 +62,27 @@ __device__ __forceinline__ bool not_finite(float x) { return !isfinite(x); }
 
 template <typename R> __device__ __forceinline__ R mn(R a, R b) { return b < a ? b : a; }
 template <typename R> __device__ __forceinline__ R mx(R a, R b) { return b > a ? b : a; }
+
+// Transcendentals: the deterministic functions of ice_math.h in the plain form (the same bits as
+// the host restatement); the fast single-precision intrinsics in the FP32-flux form (whose budget
+// is 1e-4 relative L1).
+__device__ __forceinline__ double ex(double x) { return ice_exp(x); }
+__device__ __forceinline__ double lg(double x) { return ice_log(x); }
+__device__ __forceinline__ double lg10(double x) { return ice_log10(x); }
+__device__ __forceinline__ double pw(double x, double y) { return ice_pow(x, y); }
+__device__ __forceinline__ double th(double x) { return ice_tanh(x); }
+__device__ __forceinline__ float ex(float x) { return __expf(x); }
+__device__ __forceinline__ float lg(float x) { return __logf(x); }
+__device__ __forceinline__ float lg10(float x) { return __log10f(x); }
+__device__ __forceinline__ float pw(float x, float y) { return __powf(x, y); }
+__device__ __forceinline__ float th(float x) { return tanhf(x); }
+// convergence tolerances of the iterative closures: the reference's in FP64; in FP32 the
+// iterations stop at single-precision resolution instead of running to their caps
+template <typename R> __device__ __forceinline__ R tol_picard() { return sizeof(R) == 8 ? (R)1.e-12 : (R)1.e-6f; }
+template <typename R> __device__ __forceinline__ R tol_newton() { return sizeof(R) == 8 ? (R)1.0e-13 : (R)1.0e-6f; }
+
+// Limiters the kernels specialise at compile time; any other runs through the run-time switch.
+constexpr int LIM_ANY = -1;
 
 // gfortran NORM2 of three values (scaled sum of squares), Mod_dt.f90:269, Mod_Sources.f90:35
 template <typename R> __device__ __forceinline__ R norm2_3(R a, R b, R c) {
@@ -232,7 +254,17 @@ __device__ __forceinline__ void mirror_tensor(const double* p, const double* n, 
 }
 
 // ------------------------------------------------------------------ limiters
-template <typename R> __device__ __forceinline__ R limiter(int lim, R x, R y, R cx, R cy) {
+template <int LIM, typename R> __device__ __forceinline__ R limiter(int lim, R x, R y, R cx, R cy) {
+  if constexpr (LIM == ICE_LIM_VANLEER) {
+    R ru = y / (x + (R)1e-30);
+    R phi = (ru + fabs(ru)) / ((R)1 + fabs(ru));
+    if (ru > (R)0) phi = mn(mn(phi, cx), cy*ru);
+    return phi * x;
+  } else if constexpr (LIM == ICE_LIM_MINMOD) {
+    R ru = y / (x + (R)1e-30);
+    R phi = mx((R)0, mn((R)1, ru));
+    return phi * x;
+  }
   if (lim == ICE_LIM_IORD) return (R)0;
   R ru = y / (x + (R)1e-30), phi;
   switch (lim) {
@@ -255,7 +287,7 @@ template <typename R> __device__ __forceinline__ R limiter(int lim, R x, R y, R 
 // The four cells of a stencil: a source of values q(s, v), s = 0..3 (prev, local, next, next2).
 // state_reconstruction + slope_bounds; returns true when the first-order fallback is itself
 // unphysical (report_stencil).
-template <int CL, typename R, typename Q>
+template <int CL, int LIM, typename R, typename Q>
 __device__ __forceinline__ bool reconstruct(int lim, const Q& q, R dl0, R dl1, R dl2, R dll, R dlr,
                                             R* pl, R* pr, R beta) {
   constexpr int nc = NC<CL>::v;
@@ -285,12 +317,12 @@ __device__ __forceinline__ bool reconstruct(int lim, const Q& q, R dl0, R dl1, R
       R slope1 = (a2 - a1) / dl1;
       if (!first_l) {
         R slope0 = (a1 - q(0, v)) / dl0;
-        R sl = limiter(lim, slope1, slope0, cxl, cyl) * limval;
+        R sl = limiter<LIM>(lim, slope1, slope0, cxl, cyl) * limval;
         pl[v] = a1 + sl*dll;
       }
       if (!first_r) {
         R slope2 = (q(3, v) - a2) / dl2;
-        R sr = limiter(lim, slope2, slope1, cxr, cyr) * limval;
+        R sr = limiter<LIM>(lim, slope2, slope1, cxr, cyr) * limval;
         pr[v] = a2 - sr*dlr;
       }
     }
@@ -385,7 +417,7 @@ __device__ __forceinline__ double sd_rho(double r, double r1, double r2, double 
   double sw = mx(mx(kp1, kp2), kp3);
   if (sw < 1.0/20.0) {
     double phi = mx(sw*20.0, 0.0);
-    return 1.0 - tanh(10.0*phi*phi*phi);
+    return 1.0 - ice_tanh(10.0*phi*phi*phi);
   }
   return 0.0;
 }
@@ -394,24 +426,24 @@ __device__ __forceinline__ double sd_rho(double r, double r1, double r2, double 
 template <typename R> __device__ __forceinline__ R toll_d() { return (R)(double)1e-20f; }
 
 template <typename R> __device__ __forceinline__ R drag_wen_yu(R Re) {
-  if (Re <= (R)1000) return (R)24/(Re + toll_d<R>()) * ((R)1 + (R)0.15*pow(Re, (R)0.687));
+  if (Re <= (R)1000) return (R)24/(Re + toll_d<R>()) * ((R)1 + (R)0.15*pw(Re, (R)0.687));
   return (R)0.43;
 }
 template <typename R> __device__ R henderson1(R Re, R Ma, R G, R Tr) {
   const R t = toll_d<R>();
-  R sg = pow((R)0.5*G, (R)0.5);
-  R X = Re + Ma*sg*((R)4.33 + ((R)3.65 - (R)1.53*Tr)/((R)1 + (R)0.353*Tr)*exp(-(R)0.247*Re/(Ma*sg + t))) + t;
-  R rs = pow(Re, (R)0.5);
-  return (R)24*pow(X, (R)-1)
-       + exp(-(R)0.5*Ma/(rs + t))*(((R)4.5 + (R)0.38*((R)0.03*Re + (R)0.48*rs)) / ((R)1 + (R)0.03*Re + (R)0.48*rs)
-                                   + (R)0.1*(Ma*Ma) + (R)0.2*pow(Ma, (R)8))
-       + (R)0.6*Ma*sg*((R)1 - exp(-Ma/(Re + t)));
+  R sg = pw((R)0.5*G, (R)0.5);
+  R X = Re + Ma*sg*((R)4.33 + ((R)3.65 - (R)1.53*Tr)/((R)1 + (R)0.353*Tr)*ex(-(R)0.247*Re/(Ma*sg + t))) + t;
+  R rs = pw(Re, (R)0.5);
+  return (R)24*pw(X, (R)-1)
+       + ex(-(R)0.5*Ma/(rs + t))*(((R)4.5 + (R)0.38*((R)0.03*Re + (R)0.48*rs)) / ((R)1 + (R)0.03*Re + (R)0.48*rs)
+                                   + (R)0.1*(Ma*Ma) + (R)0.2*pw(Ma, (R)8))
+       + (R)0.6*Ma*sg*((R)1 - ex(-Ma/(Re + t)));
 }
 template <typename R> __device__ R henderson2(R Re, R Ma, R G, R Tr) {
   const R t = toll_d<R>();
-  R q = pow(Ma/(Re + t), (R)0.5);
+  R q = pw(Ma/(Re + t), (R)0.5);
   return ((R)0.9 + (R)0.34/((Ma*Ma) + t) + (R)1.86*q*((R)2 + (R)2/(Ma*Ma*(R)0.5*G + t)
-          + ((R)1.058/(Ma*pow((R)0.5*G, (R)0.5) + t))*pow(Tr, (R)0.5)) - (R)1/(pow(Ma, (R)4)*(G*G)*(R)0.25 + t))
+          + ((R)1.058/(Ma*pw((R)0.5*G, (R)0.5) + t))*pw(Tr, (R)0.5)) - (R)1/(pw(Ma, (R)4)*(G*G)*(R)0.25 + t))
          / ((R)1 + (R)1.86*q);
 }
 template <typename R> __device__ R drag(R Re, R Ma, R G, R Tr, int sel) {
@@ -420,10 +452,10 @@ template <typename R> __device__ R drag(R Re, R Ma, R G, R Tr, int sel) {
     case 1: return (R)0.45;
     case 2: return (R)24/(Re + t);
     case 3: return (R)24/(Re + t) * ((R)1 + (R)3*Re/(R)16);
-    case 4: return (R)24/(Re + t) * ((R)1 + (R)0.15*pow(Re, (R)0.687));
+    case 4: return (R)24/(Re + t) * ((R)1 + (R)0.15*pw(Re, (R)0.687));
     case 5: return drag_wen_yu(Re);
-    case 6: if (Re < (R)1000) return (R)24/(Re + t) * ((R)1 + pow(Re, (R)(2.0/3.0))/(R)6); return (R)0.4392;
-    case 7: return (R)24/(Re + t) * ((R)1 + (R)0.15*pow(Re, (R)0.687) + (R)0.0175*Re/((R)1 + (R)4.25*(R)1e4*pow(Re, (R)-1.16)));
+    case 6: if (Re < (R)1000) return (R)24/(Re + t) * ((R)1 + pw(Re, (R)(2.0/3.0))/(R)6); return (R)0.4392;
+    case 7: return (R)24/(Re + t) * ((R)1 + (R)0.15*pw(Re, (R)0.687) + (R)0.0175*Re/((R)1 + (R)4.25*(R)1e4*pw(Re, (R)-1.16)));
     case 8: {
       R a1, a2, a3;
       if (Re <= (R)0.1) { a1 = 0; a2 = 24; a3 = 0; }
@@ -438,8 +470,8 @@ template <typename R> __device__ R drag(R Re, R Ma, R G, R Tr, int sel) {
     }
     case 9: {
       R Cd0 = drag_wen_yu(Re);
-      return Cd0 * ((R)1 + exp(-(R)0.427/(pow(Ma, (R)4.63) + t) - (R)3/(pow(Re, (R)0.88) + t))) /
-             ((R)1 + Ma/(Re + t)*((R)3.82 + (R)1.28*exp(-(R)1.25*Re/(Ma + t))));
+      return Cd0 * ((R)1 + ex(-(R)0.427/(pw(Ma, (R)4.63) + t) - (R)3/(pw(Re, (R)0.88) + t))) /
+             ((R)1 + Ma/(Re + t)*((R)3.82 + (R)1.28*ex(-(R)1.25*Re/(Ma + t))));
     }
     case 10:
       if (Ma <= (R)1) return henderson1(Re, Ma, G, Tr);
@@ -449,17 +481,17 @@ template <typename R> __device__ R drag(R Re, R Ma, R G, R Tr, int sel) {
         return Cd1 + (R)(4.0/3.0)*(Ma - (R)1)*(Cd2 - Cd1);
       }
     case 11: {
-      R g = (R)1.25*((R)1 + tanh((R)0.77*log10(Re + t) - (R)1.92));
-      g = pow((R)10, g);
-      R h = (R)2.3 + (R)1.7*pow(Tr, (R)0.5) - (R)2.3*tanh((R)1.17*log10(Ma + t));
+      R g = (R)1.25*((R)1 + th((R)0.77*lg10(Re + t) - (R)1.92));
+      g = pw((R)10, g);
+      R h = (R)2.3 + (R)1.7*pw(Tr, (R)0.5) - (R)2.3*th((R)1.17*lg10(Ma + t));
       R Cd0 = drag_wen_yu(Re);
-      return (R)2 + (Cd0 - (R)2)*exp(-(R)3.07*pow(G, (R)0.5)*Ma*g/(Re + t)) + h/(Ma*pow(G, (R)0.5) + t)*exp(-Re/((R)2*Ma + t));
+      return (R)2 + (Cd0 - (R)2)*ex(-(R)3.07*pw(G, (R)0.5)*Ma*g/(Re + t)) + h/(Ma*pw(G, (R)0.5) + t)*ex(-Re/((R)2*Ma + t));
     }
     case 12: {
       R g = ((R)1 + Re*((R)12.278 + (R)0.548*Re)) / ((R)1 + (R)11.278*Re);
-      R h = (R)5.6/((R)1 + Ma) + (R)1.7*pow(Tr, (R)0.5);
+      R h = (R)5.6/((R)1 + Ma) + (R)1.7*pw(Tr, (R)0.5);
       R Cd0 = drag_wen_yu(Re);
-      return (R)2 + (Cd0 - (R)2)*exp(-(R)3.07*pow(G, (R)0.5)*Ma*g/(Re + t)) + h/(Ma*pow(G, (R)0.5) + t)*exp(-Re/((R)2*Ma + t));
+      return (R)2 + (Cd0 - (R)2)*ex(-(R)3.07*pw(G, (R)0.5)*Ma*g/(Re + t)) + h/(Ma*pw(G, (R)0.5) + t)*ex(-Re/((R)2*Ma + t));
     }
     case 13: return (R)0;
   }
@@ -471,13 +503,13 @@ template <typename R> __device__ R heat(R Re, R Pr, R Ma, int sel) {
   const R t = (R)1e-20;
   switch (sel) {
     case 1: return (R)2;
-    case 2: return (R)2.5*pow(Re, (R)0.15) + (R)0.04*Re;
-    case 3: return (R)2 + (R)0.37*pow(Re, (R)0.6)*pow(Pr, (R)(1.0/3.0));
-    case 4: return (R)2 + (R)0.459*pow(Re, (R)0.55)*pow(Pr, (R)(1.0/3.0));
-    case 5: return pow(pow((R)2 + (R)0.654*pow(Re, (R)0.5)*pow(Pr, (R)0.5), (R)-1) + (R)3.42*Ma/(Re*Pr + t), (R)-1);
-    case 6: return (R)2 + (R)0.6*pow(Re, (R)0.5)*pow(Pr, (R)(1.0/3.0));
+    case 2: return (R)2.5*pw(Re, (R)0.15) + (R)0.04*Re;
+    case 3: return (R)2 + (R)0.37*pw(Re, (R)0.6)*pw(Pr, (R)(1.0/3.0));
+    case 4: return (R)2 + (R)0.459*pw(Re, (R)0.55)*pw(Pr, (R)(1.0/3.0));
+    case 5: return pw(pw((R)2 + (R)0.654*pw(Re, (R)0.5)*pw(Pr, (R)0.5), (R)-1) + (R)3.42*Ma/(Re*Pr + t), (R)-1);
+    case 6: return (R)2 + (R)0.6*pw(Re, (R)0.5)*pw(Pr, (R)(1.0/3.0));
     case 7: {
-      R Nu = (R)2 + (R)0.459*pow(Re, (R)0.55)*pow(Pr, (R)0.33);
+      R Nu = (R)2 + (R)0.459*pw(Re, (R)0.55)*pw(Pr, (R)0.33);
       return Nu / ((R)1 + (R)3.42*Ma/(Re*Pr + t)*Nu);
     }
     case 8: return (R)0;
@@ -495,12 +527,12 @@ template <typename R> __device__ __forceinline__ R blowing(R gamma, R Rg, R mug,
   R b = -(R)1.5*Pr*taud*mdot/mp;
   if (b != b || b <= (R)1e-10) return (R)1;
   if (b > (R)500) return (R)0;
-  return b/(exp(b) - (R)1);
+  return b/(ex(b) - (R)1);
 }
 
 template <typename R> __device__ __forceinline__ R molar2mass(R Xs, R Mv, R Mg) { return Xs*Mv/(Xs*Mv + ((R)1 - Xs)*Mg); }
 template <typename R> __device__ __forceinline__ R mass2molar(R Ys, R Mv, R Mg) { return Ys*Mg/(Ys*Mg + ((R)1 - Ys)*Mv); }
-template <typename R> __device__ __forceinline__ R Fcorr(R B) { return B > (R)1.0e-10 ? pow((R)1 + B, (R)0.7)*log((R)1 + B)/B : (R)1; }
+template <typename R> __device__ __forceinline__ R Fcorr(R B) { return B > (R)1.0e-10 ? pw((R)1 + B, (R)0.7)*lg((R)1 + B)/B : (R)1; }
 
 template <typename R> struct EvapEnv {
   R rhog, Tg, gamma, Rg, mug, kg, Tp, dp, cpg, p, Mg, Pr, Sc, Re05;
@@ -517,44 +549,44 @@ template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, 
     case 1: {
       R BT = e.cpg*(e.Tg - e.Tp)/(R)ep[EP_LV];
       if (BT <= (R)0) { md = (R)0; return; }
-      md = -(R)2*pi*e.dp*e.kg/e.cpg*log((R)1 + BT);
+      md = -(R)2*pi*e.dp*e.kg/e.cpg*lg((R)1 + BT);
       return;
     }
     case 2: {
       R Dv = e.kg/(e.rhog*e.cpg*(R)ep[EP_LE]);
-      R Sh = (R)2 + (R)0.6*e.Re05*pow(e.Sc, (R)(1.0/3.0));
-      md = -pi*e.dp*e.rhog*Dv*Sh*log((R)1 + BM);
+      R Sh = (R)2 + (R)0.6*e.Re05*pw(e.Sc, (R)(1.0/3.0));
+      md = -pi*e.dp*e.rhog*Dv*Sh*lg((R)1 + BM);
       return;
     }
     case 3: {
       R Tf = e.Tp + (e.Tg - e.Tp)/(R)3;
       R rho_f = e.rhog*e.Tg/Tf;
-      R mu_f = e.mug*pow(Tf/e.Tg, (R)0.7);
-      R kl_f = e.kg*pow(Tf/e.Tg, (R)0.7);
+      R mu_f = e.mug*pw(Tf/e.Tg, (R)0.7);
+      R kl_f = e.kg*pw(Tf/e.Tg, (R)0.7);
       R cpg_f = e.cpg;
       R Le = (R)ep[EP_LE];
       R Dv_f = kl_f/(rho_f*cpg_f*Le);
       R Sc_f = mu_f*cpg_f*Le/kl_f;
       R Re_f = e.Re05*e.Re05*rho_f/e.rhog*e.mug/mu_f;
-      R Sh_f = (R)2 + (R)0.6*sqrt(mx(Re_f, (R)0))*pow(Sc_f, (R)(1.0/3.0));
-      md = -pi*e.dp*rho_f*Dv_f*Sh_f*log((R)1 + BM);
+      R Sh_f = (R)2 + (R)0.6*sqrt(mx(Re_f, (R)0))*pw(Sc_f, (R)(1.0/3.0));
+      md = -pi*e.dp*rho_f*Dv_f*Sh_f*lg((R)1 + BM);
       return;
     }
     case 4: {
       R Le = (R)ep[EP_LE], cpv = (R)ep[EP_CPV];
       ovr = true;
       R Dv = e.kg/(e.rhog*e.cpg*Le);
-      R lnBM = log((R)1 + BM);
+      R lnBM = lg((R)1 + BM);
       R FM = Fcorr(BM);
-      R Sh0 = (R)2 + (R)0.552*e.Re05*pow(e.Sc, (R)(1.0/3.0));
+      R Sh0 = (R)2 + (R)0.552*e.Re05*pw(e.Sc, (R)(1.0/3.0));
       R Shs = (R)2 + (Sh0 - (R)2)/FM;
       md = -pi*e.dp*e.rhog*Dv*Shs*lnBM;
       R cpv_eff = cpv > (R)0 ? cpv : e.cpg;
-      R Nu0 = (R)2 + (R)0.552*e.Re05*pow(e.Pr, (R)(1.0/3.0));
+      R Nu0 = (R)2 + (R)0.552*e.Re05*pw(e.Pr, (R)(1.0/3.0));
       R Nus = Nu0, BT = (R)0;
       for (int it = 1; it <= 5; ++it) {
         R phi = cpv_eff/e.cpg*Shs/Nus/Le;
-        BT = pow((R)1 + BM, phi) - (R)1;
+        BT = pw((R)1 + BM, phi) - (R)1;
         if (BT <= (R)0) { BT = BM; Nus = Nu0; break; }
         R FT = Fcorr(BT);
         Nus = (R)2 + (Nu0 - (R)2)/FT;
@@ -569,7 +601,7 @@ template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, 
       R Xs = mn(mass2molar(Ys, Mv, e.Mg), (R)1 - (R)kXsCap);
       R Xinf = mass2molar(Yinf, Mv, e.Mg);
       R Minf = Xinf*Mv + ((R)1 - Xinf)*e.Mg;
-      R rhs0 = Mv/Minf*log(((R)1 - Xinf)/((R)1 - Xs));
+      R rhs0 = Mv/Minf*lg(((R)1 - Xinf)/((R)1 - Xs));
       if (rhs0 <= (R)0) return;
       R Tts = e.Tp/e.Tg;
       R Lev = e.kg/(cpv_eff*Dv*e.rhog);
@@ -579,7 +611,7 @@ template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, 
       for (int it = 1; it <= 30; ++it) {
         R x = mhat/Lev, f, fp;
         if (x > (R)1.0e-6) {
-          R E = exp(-x);
+          R E = ex(-x);
           f = x/((R)1 - E);
           fp = ((R)1 - E - x*E)/(((R)1 - E)*((R)1 - E));
         } else {
@@ -588,17 +620,17 @@ template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, 
         }
         R G = mhat + (Tts - (R)1)*Lev*(f - (R)1) - rhs0;
         R dG = (R)1 + (Tts - (R)1)*fp;
-        if (fabs(G) <= (R)1.0e-13*mx((R)1, rhs0)) break;
+        if (fabs(G) <= tol_newton<R>()*mx((R)1, rhs0)) break;
         if (G > (R)0) mhi = mhat; else mlo = mhat;
         mhat = mhat - G/dG;
         if (mhat <= mlo || mhat >= mhi) mhat = (R)0.5*(mlo + mhi);
       }
-      R Sh = (R)2 + (R)0.6*e.Re05*pow(e.Sc, (R)(1.0/3.0));
+      R Sh = (R)2 + (R)0.6*e.Re05*pw(e.Sc, (R)(1.0/3.0));
       md = -pi*e.dp*e.rhog*Dv*Sh*mhat;
       ovr = true;
-      R Nu = (R)2 + (R)0.6*e.Re05*pow(e.Pr, (R)(1.0/3.0));
+      R Nu = (R)2 + (R)0.6*e.Re05*pw(e.Pr, (R)(1.0/3.0));
       R chi = mn(-md*cpv_eff/(pi*e.dp*e.kg*Nu), (R)700);
-      if (chi > (R)1.0e-9) Qd = -md*cpv_eff*(e.Tg - e.Tp)/(exp(chi) - (R)1);
+      if (chi > (R)1.0e-9) Qd = -md*cpv_eff*(e.Tg - e.Tp)/(ex(chi) - (R)1);
       else Qd = pi*e.dp*e.kg*Nu*(e.Tg - e.Tp);
       return;
     }
@@ -617,7 +649,7 @@ template <typename R> __device__ void evaporation(R rhog, R Tg, R gamma, R Rg, R
   e.cpg = gamma*Rg/(gamma - (R)1);
   e.p = rhog*Rg*Tg;
   e.Mg = (R)kRu/Rg;
-  R psat = (R)kPatm*exp(-(R)ep[EP_LVMVRU]*((R)1/Tp - (R)ep[EP_INVTB]));
+  R psat = (R)kPatm*ex(-(R)ep[EP_LVMVRU]*((R)1/Tp - (R)ep[EP_INVTB]));
   R Xs = psat >= e.p ? (R)1 - (R)kXsCap : mn(psat/e.p, (R)1 - (R)kXsCap);
   R Ys = molar2mass(Xs, (R)ep[EP_MV], e.Mg);
   if (Ys <= (R)ep[EP_YINF]) return;
@@ -643,7 +675,7 @@ template <typename R> __device__ void evaporation(R rhog, R Tg, R gamma, R Rg, R
       if (BMN > (R)0) gas_side(e, YsN, BMN, mdNew, QdNew, ovrNew);
     }
     R diff = fabs(mdNew - md);
-    if (diff <= (R)1.e-12*fabs(mdNew)) { mdot = mdNew; Qd = QdNew; ovr = ovrNew; return; }
+    if (diff <= tol_picard<R>()*fabs(mdNew)) { mdot = mdNew; Qd = QdNew; ovr = ovrNew; return; }
     if (diff < diffPrev) md = mdNew; else md = (R)0.5*(md + mdNew);
     diffPrev = diff;
   }
@@ -687,10 +719,10 @@ template <int CL, typename R> __device__ R cell_source(const R* p, const R* gas,
   const R pi = (R)kPi;
   R T = p[nb - 2], n = p[nb - 1];
   R rho_mat = (R)m.rho;
-  R Rp = pow((R)0.75*p[0]/(n*pi*rho_mat), (R)(1.0/3.0));
+  R Rp = pw((R)0.75*p[0]/(n*pi*rho_mat), (R)(1.0/3.0));
   R du = norm2_3(gas[1] - p[1], gas[2] - p[2], gas[3] - p[3]);
   R Re = (R)2*gas[0]*Rp*du/gmu;
-  R Ma = du/pow(ggam*gR*gas[4], (R)0.5);
+  R Ma = du/pw(ggam*gR*gas[4], (R)0.5);
   R Pr = ggam/(ggam - (R)1)*gR*gmu/gk;
   R Nu = heat(Re, Pr, Ma, heat_sel);
   R Ts = T;
@@ -705,7 +737,7 @@ template <int CL, typename R> __device__ R cell_source(const R* p, const R* gas,
   else if (blow == 1) Qconv = Qconv*blowing<R>(ggam, gR, gmu, gk, rho_mat, (R)2*Rp, (R)(4.0/3.0)*pi*(Rp*Rp*Rp)*rho_mat, mdot);
   F[0] = -mdot*n;
   F[4] = Qconv*n;
-  F[4] = F[4] + (R)m.emiss*(R)kSigmaSB*(R)4*pi*Rp*Rp*n*(pow(gas[4], (R)4) - pow(Ts, (R)4));
+  F[4] = F[4] + (R)m.emiss*(R)kSigmaSB*(R)4*pi*Rp*Rp*n*(pw(gas[4], (R)4) - pw(Ts, (R)4));
   R tau;
   if (Cd == (R)0) tau = (R)INFINITY;
   else tau = (R)8*rho_mat*Rp/((R)3*gas[0]*Cd*du + toll_d<R>());

@@ -1,0 +1,42 @@
+// ice_stage.cuh -- the launcher of the stage kernel of one closure and precision: the Riemann
+// solver and the limiter are compile-time parameters of the kernel (van Leer and minmod
+// specialised, every other limiter through the run-time switch).
+#pragma once
+#include "ice_kernels.cuh"
+
+namespace ice {
+
+template <int CL, int RS, int LIM, typename R>
+void launch_stage_k(const LaunchArgs& a, bool write_r) {
+  constexpr int nc = NC<CL>::v;
+  const size_t sh = sizeof(double) * 4 * nc * (size_t)a.TX * a.TY;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_stage<CL, RS, LIM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    attr = true;
+  }
+  k_stage<CL, RS, LIM, R><<<a.ntile, a.TX * a.TY, sh, a.s>>>(a.G, a.F, a.tiles, a.TX, a.TY, a.KZ, write_r ? 1 : 0, a.st);
+}
+
+template <int CL, int RS, typename R>
+void launch_stage_l(const LaunchArgs& a, bool write_r) {
+  if (a.F.limiter == ICE_LIM_VANLEER) launch_stage_k<CL, RS, ICE_LIM_VANLEER, R>(a, write_r);
+  else if (a.F.limiter == ICE_LIM_MINMOD) launch_stage_k<CL, RS, ICE_LIM_MINMOD, R>(a, write_r);
+  else launch_stage_k<CL, RS, LIM_ANY, R>(a, write_r);
+}
+
+template <int CL, typename R>
+void launch_source_t(const LaunchArgs& a) {
+  k_source<CL, R><<<(unsigned)((a.G.NI + 255) / 256), 256, 0, a.s>>>(a.G, a.F);
+}
+
+template <int CL, typename R>
+void launch_stage_t(const LaunchArgs& a, bool write_r) {
+  if constexpr (CL == MK) {
+    if (a.F.riemann == ICE_RIEMANN_SAUREL) { launch_stage_l<CL, ICE_RIEMANN_SAUREL, R>(a, write_r); return; }
+  }
+  if (a.F.riemann == ICE_RIEMANN_HLLE) launch_stage_l<CL, ICE_RIEMANN_HLLE, R>(a, write_r);
+  else launch_stage_l<CL, ICE_RIEMANN_RUSANOV, R>(a, write_r);
+}
+
+}  // namespace ice

@@ -1,0 +1,6 @@
+// The AG family's stage kernels, FP32 reconstruction, fluxes and sources (the chosen form).
+#include "ice_stage.cuh"
+namespace ice {
+void launch_stage_ag_f32(const LaunchArgs& a, bool write_r) { launch_stage_t<AG, float>(a, write_r); }
+void launch_source_ag_f32(const LaunchArgs& a) { launch_source_t<AG, float>(a); }
+}  // namespace ice

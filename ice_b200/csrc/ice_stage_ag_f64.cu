@@ -1,0 +1,6 @@
+// The AG family's stage kernels, FP64 (plain form and the IRS residual).
+#include "ice_stage.cuh"
+namespace ice {
+void launch_stage_ag_f64(const LaunchArgs& a, bool write_r) { launch_stage_t<AG, double>(a, write_r); }
+void launch_source_ag_f64(const LaunchArgs& a) { launch_source_t<AG, double>(a); }
+}  // namespace ice

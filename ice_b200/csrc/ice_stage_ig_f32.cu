@@ -1,0 +1,6 @@
+// The IG family's stage kernels, FP32 reconstruction, fluxes and sources (the chosen form).
+#include "ice_stage.cuh"
+namespace ice {
+void launch_stage_ig_f32(const LaunchArgs& a, bool write_r) { launch_stage_t<IG, float>(a, write_r); }
+void launch_source_ig_f32(const LaunchArgs& a) { launch_source_t<IG, float>(a); }
+}  // namespace ice

@@ -1,0 +1,6 @@
+// The MK family's stage kernels, FP32 reconstruction, fluxes and sources (the chosen form).
+#include "ice_stage.cuh"
+namespace ice {
+void launch_stage_mk_f32(const LaunchArgs& a, bool write_r) { launch_stage_t<MK, float>(a, write_r); }
+void launch_source_mk_f32(const LaunchArgs& a) { launch_source_t<MK, float>(a); }
+}  // namespace ice

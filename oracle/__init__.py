@@ -17,7 +17,9 @@ LIB = HERE / "libice_oracle.so"
 
 def build(force: bool = False) -> Path:
     if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime
-                                        for p in (HERE / "ice_oracle.c", HERE / "ice_oracle_physics.h")):
+                                        for p in (HERE / "ice_oracle.c", HERE / "ice_oracle_physics.h",
+                                                  HERE.parent / "include" / "ice_math.h",
+                                                  HERE.parent / "include" / "ice_gpu.h")):
         subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"], check=True,
                        stdout=subprocess.DEVNULL)
     return LIB
@@ -39,6 +41,7 @@ _EXTRA = [
     ("cons2prim", None, [C.c_int, _dp, _dp, C.POINTER(abi.Family)]),
     ("download_aux", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp, _dp]),
     ("set_threads", C.c_int, [C.c_int]),
+    ("math", C.c_double, [C.c_int, C.c_double, C.c_double]),
 ]
 
 

@@ -1018,4 +1018,16 @@ double orc_blowing(double gamma, double Rg, double mug, double kg, double rhop, 
     return o_blowing(gamma, Rg, mug, kg, rhop, dp, mp, mdot);
 }
 void orc_prim2cons(int cl, const double* p, double* c, const ice_gpu_family* m) { o_prim2cons(cl, p, c, m); }
+/* the elementary functions of include/ice_math.h, for their accuracy test */
+double orc_math(int fn, double x, double y) {
+    switch (fn) {
+    case 0: return ice_exp(x);
+    case 1: return ice_log(x);
+    case 2: return ice_pow(x, y);
+    case 3: return ice_tanh(x);
+    case 4: return ice_expm1(x);
+    case 5: return ice_log10(x);
+    }
+    return 0.0;
+}
 void orc_cons2prim(int cl, const double* c, double* p, const ice_gpu_family* m) { o_cons2prim(cl, c, p, m); }

@@ -14,6 +14,11 @@
  * precision) literals are promoted from float exactly as gfortran does: 1e-25 in
  * the closures, 1e-20 in drag and tau, 1e+5 in compute_dt.
  *
+ * The transcendentals of the sources and the sensor (exp, log, log10, pow, tanh) are the
+ * deterministic functions of include/ice_math.h (within a few ulp of glibc's, tests/test_math.py),
+ * the functions the device computes with, so that the FP64 forms agree to the bit; the reference
+ * calls its platform's libm, which can differ from them in the last bits.
+ *
  * Parity pins: tests/test_oracle_*.py check this restatement against the
  * reference's own known answers (test/unit/test_muscl_bounds.f90 B1-B5,
  * test/Riemann/AG exact solution, test/Doisneau/{MK,IG,AG} stored fields).
@@ -26,6 +31,7 @@
 #include <string.h>
 #include <float.h>
 #include "../include/ice_gpu.h"
+#include "../include/ice_math.h"
 
 #define O_PI        3.14159265358979323846      /* Parameters_m.f90:41                       */
 #define O_SIGMA_SB  5.670374419e-8               /* Parameters_m.f90:42                       */
@@ -376,7 +382,7 @@ static inline double o_sd_rho(double r, double r1, double r2, double r3, double 
     double sw = o_max2(o_max2(kp1, kp2), kp3);
     if (sw < 1.0/20.0) {
         double phi = o_max2(sw*20.0, 0.0);
-        return 1.0 - tanh(10.0*phi*phi*phi);
+        return 1.0 - ice_tanh(10.0*phi*phi*phi);
     }
     return 0.0;
 }
@@ -385,24 +391,24 @@ static inline double o_sd_rho(double r, double r1, double r2, double r3, double 
 /* Lib_Drag.f90:83-324 */
 static inline double o_drag_wen_yu(double Re) {
     const double t = O_TOLL_DRAG;
-    if (Re <= 1000) return 24.0/(Re + t) * (1.0 + 0.15*pow(Re, 0.687));
+    if (Re <= 1000) return 24.0/(Re + t) * (1.0 + 0.15*ice_pow(Re, 0.687));
     return 0.43;
 }
 static inline double o_henderson1(double Re, double Ma, double G, double Tr) {
     const double t = O_TOLL_DRAG;
-    double sg = pow(0.5*G, 0.5);
-    double X = Re + Ma*sg*(4.33 + (3.65 - 1.53*Tr)/(1.0 + 0.353*Tr)*exp(-0.247*Re/(Ma*sg + t))) + t;
-    double rs = pow(Re, 0.5);
-    return 24.0*pow(X, -1.0)
-         + exp(-0.5*Ma/(rs + t))*((4.5 + 0.38*(0.03*Re + 0.48*rs)) / (1.0 + 0.03*Re + 0.48*rs)
-                                  + 0.1*(Ma*Ma) + 0.2*pow(Ma, 8.0))
-         + 0.6*Ma*sg*(1.0 - exp(-Ma/(Re + t)));
+    double sg = ice_pow(0.5*G, 0.5);
+    double X = Re + Ma*sg*(4.33 + (3.65 - 1.53*Tr)/(1.0 + 0.353*Tr)*ice_exp(-0.247*Re/(Ma*sg + t))) + t;
+    double rs = ice_pow(Re, 0.5);
+    return 24.0*ice_pow(X, -1.0)
+         + ice_exp(-0.5*Ma/(rs + t))*((4.5 + 0.38*(0.03*Re + 0.48*rs)) / (1.0 + 0.03*Re + 0.48*rs)
+                                  + 0.1*(Ma*Ma) + 0.2*ice_pow(Ma, 8.0))
+         + 0.6*Ma*sg*(1.0 - ice_exp(-Ma/(Re + t)));
 }
 static inline double o_henderson2(double Re, double Ma, double G, double Tr) {
     const double t = O_TOLL_DRAG;
-    double q = pow(Ma/(Re + t), 0.5);
+    double q = ice_pow(Ma/(Re + t), 0.5);
     return (0.9 + 0.34/((Ma*Ma) + t) + 1.86*q*(2.0 + 2.0/(Ma*Ma*0.5*G + t)
-            + (1.058/(Ma*pow(0.5*G, 0.5) + t))*pow(Tr, 0.5)) - 1.0/(pow(Ma, 4.0)*(G*G)*0.25 + t))
+            + (1.058/(Ma*ice_pow(0.5*G, 0.5) + t))*ice_pow(Tr, 0.5)) - 1.0/(ice_pow(Ma, 4.0)*(G*G)*0.25 + t))
            / (1.0 + 1.86*q);
 }
 static inline double o_drag(double Re, double Ma, double G, double Tr, int sel) {
@@ -411,10 +417,10 @@ static inline double o_drag(double Re, double Ma, double G, double Tr, int sel) 
     case 1: return 0.45;
     case 2: return 24.0/(Re + t);
     case 3: return 24.0/(Re + t) * (1.0 + 3.0*Re/16.0);
-    case 4: return 24.0/(Re + t) * (1.0 + 0.15*pow(Re, 0.687));
+    case 4: return 24.0/(Re + t) * (1.0 + 0.15*ice_pow(Re, 0.687));
     case 5: return o_drag_wen_yu(Re);
-    case 6: if (Re < 1000) return 24.0/(Re + t) * (1.0 + pow(Re, 2.0/3.0)/6.0); return 0.4392;
-    case 7: return 24.0/(Re + t) * (1.0 + 0.15*pow(Re, 0.687) + 0.0175*Re/(1.0 + 4.25*1e4*pow(Re, -1.16)));
+    case 6: if (Re < 1000) return 24.0/(Re + t) * (1.0 + ice_pow(Re, 2.0/3.0)/6.0); return 0.4392;
+    case 7: return 24.0/(Re + t) * (1.0 + 0.15*ice_pow(Re, 0.687) + 0.0175*Re/(1.0 + 4.25*1e4*ice_pow(Re, -1.16)));
     case 8: {
         double a1, a2, a3;
         if (Re <= 0.1) { a1 = 0; a2 = 24; a3 = 0; }
@@ -429,8 +435,8 @@ static inline double o_drag(double Re, double Ma, double G, double Tr, int sel) 
     }
     case 9: {
         double Cd0 = o_drag_wen_yu(Re);
-        return Cd0 * (1.0 + exp(-0.427/(pow(Ma, 4.63) + t) - 3.0/(pow(Re, 0.88) + t))) /
-               (1.0 + Ma/(Re + t)*(3.82 + 1.28*exp(-1.25*Re/(Ma + t))));
+        return Cd0 * (1.0 + ice_exp(-0.427/(ice_pow(Ma, 4.63) + t) - 3.0/(ice_pow(Re, 0.88) + t))) /
+               (1.0 + Ma/(Re + t)*(3.82 + 1.28*ice_exp(-1.25*Re/(Ma + t))));
     }
     case 10:
         if (Ma <= 1) return o_henderson1(Re, Ma, G, Tr);
@@ -440,17 +446,17 @@ static inline double o_drag(double Re, double Ma, double G, double Tr, int sel) 
             return Cd1 + 4.0/3.0*(Ma - 1.0)*(Cd2 - Cd1);
         }
     case 11: {
-        double g = 1.25*(1.0 + tanh(0.77*log10(Re + t) - 1.92));
-        g = pow(10.0, g);
-        double h = 2.3 + 1.7*pow(Tr, 0.5) - 2.3*tanh(1.17*log10(Ma + t));
+        double g = 1.25*(1.0 + ice_tanh(0.77*ice_log10(Re + t) - 1.92));
+        g = ice_pow(10.0, g);
+        double h = 2.3 + 1.7*ice_pow(Tr, 0.5) - 2.3*ice_tanh(1.17*ice_log10(Ma + t));
         double Cd0 = o_drag_wen_yu(Re);
-        return 2.0 + (Cd0 - 2.0)*exp(-3.07*pow(G, 0.5)*Ma*g/(Re + t)) + h/(Ma*pow(G, 0.5) + t)*exp(-Re/(2.0*Ma + t));
+        return 2.0 + (Cd0 - 2.0)*ice_exp(-3.07*ice_pow(G, 0.5)*Ma*g/(Re + t)) + h/(Ma*ice_pow(G, 0.5) + t)*ice_exp(-Re/(2.0*Ma + t));
     }
     case 12: {
         double g = (1.0 + Re*(12.278 + 0.548*Re)) / (1.0 + 11.278*Re);
-        double h = 5.6/(1.0 + Ma) + 1.7*pow(Tr, 0.5);
+        double h = 5.6/(1.0 + Ma) + 1.7*ice_pow(Tr, 0.5);
         double Cd0 = o_drag_wen_yu(Re);
-        return 2.0 + (Cd0 - 2.0)*exp(-3.07*pow(G, 0.5)*Ma*g/(Re + t)) + h/(Ma*pow(G, 0.5) + t)*exp(-Re/(2.0*Ma + t));
+        return 2.0 + (Cd0 - 2.0)*ice_exp(-3.07*ice_pow(G, 0.5)*Ma*g/(Re + t)) + h/(Ma*ice_pow(G, 0.5) + t)*ice_exp(-Re/(2.0*Ma + t));
     }
     case 13: return 0.0;
     }
@@ -463,13 +469,13 @@ static inline double o_heat(double Re, double Pr, double Ma, int sel) {
     const double t = O_TOLL_HEAT;
     switch (sel) {
     case 1: return 2.0;
-    case 2: return 2.5*pow(Re, 0.15) + 0.04*Re;
-    case 3: return 2.0 + 0.37*pow(Re, 0.6)*pow(Pr, 1.0/3.0);
-    case 4: return 2.0 + 0.459*pow(Re, 0.55)*pow(Pr, 1.0/3.0);
-    case 5: return pow(pow(2.0 + 0.654*pow(Re, 0.5)*pow(Pr, 0.5), -1.0) + 3.42*Ma/(Re*Pr + t), -1.0);
-    case 6: return 2.0 + 0.6*pow(Re, 0.5)*pow(Pr, 1.0/3.0);
+    case 2: return 2.5*ice_pow(Re, 0.15) + 0.04*Re;
+    case 3: return 2.0 + 0.37*ice_pow(Re, 0.6)*ice_pow(Pr, 1.0/3.0);
+    case 4: return 2.0 + 0.459*ice_pow(Re, 0.55)*ice_pow(Pr, 1.0/3.0);
+    case 5: return ice_pow(ice_pow(2.0 + 0.654*ice_pow(Re, 0.5)*ice_pow(Pr, 0.5), -1.0) + 3.42*Ma/(Re*Pr + t), -1.0);
+    case 6: return 2.0 + 0.6*ice_pow(Re, 0.5)*ice_pow(Pr, 1.0/3.0);
     case 7: {
-        double Nu = 2.0 + 0.459*pow(Re, 0.55)*pow(Pr, 0.33);
+        double Nu = 2.0 + 0.459*ice_pow(Re, 0.55)*ice_pow(Pr, 0.33);
         return Nu / (1.0 + 3.42*Ma/(Re*Pr + t)*Nu);
     }
     case 8: return 0.0;
@@ -489,12 +495,12 @@ static inline double o_blowing(double gamma, double Rg, double mug, double kg, d
     double b = -1.5*Pr*taud*mdot/mp;
     if (b != b || b <= 1e-10) return 1.0;
     if (b > 500.0) return 0.0;
-    return b/(exp(b) - 1.0);
+    return b/(ice_exp(b) - 1.0);
 }
 
 static inline double o_molar2mass(double Xs, double Mv, double Mg) { return Xs*Mv/(Xs*Mv + (1.0 - Xs)*Mg); }
 static inline double o_mass2molar(double Ys, double Mv, double Mg) { return Ys*Mg/(Ys*Mg + (1.0 - Ys)*Mv); }
-static inline double o_Fcorr(double B) { return B > 1.0e-10 ? pow(1.0 + B, 0.7)*log(1.0 + B)/B : 1.0; }
+static inline double o_Fcorr(double B) { return B > 1.0e-10 ? ice_pow(1.0 + B, 0.7)*ice_log(1.0 + B)/B : 1.0; }
 
 typedef struct {
     double rhog, Tg, gamma, Rg, mug, kg, Tp, dp, cpg, p, Mg, Pr, Sc, Re05;
@@ -511,43 +517,43 @@ static inline void o_gas_side(const o_evap_env* e, double Ys, double BM, double*
     case 1: {
         double BT = e->cpg*(e->Tg - e->Tp)/ep[EP_LV];
         if (BT <= 0.0) { *md = 0.0; return; }
-        *md = -2.0*pi*e->dp*e->kg/e->cpg*log(1.0 + BT);
+        *md = -2.0*pi*e->dp*e->kg/e->cpg*ice_log(1.0 + BT);
         return;
     }
     case 2: {
         double Dv = e->kg/(e->rhog*e->cpg*ep[EP_LE]);
-        double Sh = 2.0 + 0.6*e->Re05*pow(e->Sc, 1.0/3.0);
-        *md = -pi*e->dp*e->rhog*Dv*Sh*log(1.0 + BM);
+        double Sh = 2.0 + 0.6*e->Re05*ice_pow(e->Sc, 1.0/3.0);
+        *md = -pi*e->dp*e->rhog*Dv*Sh*ice_log(1.0 + BM);
         return;
     }
     case 3: {
         double Tf = e->Tp + (e->Tg - e->Tp)/3.0;
         double rho_f = e->rhog*e->Tg/Tf;
-        double mu_f = e->mug*pow(Tf/e->Tg, 0.7);
-        double kl_f = e->kg*pow(Tf/e->Tg, 0.7);
+        double mu_f = e->mug*ice_pow(Tf/e->Tg, 0.7);
+        double kl_f = e->kg*ice_pow(Tf/e->Tg, 0.7);
         double cpg_f = e->cpg;
         double Dv_f = kl_f/(rho_f*cpg_f*ep[EP_LE]);
         double Sc_f = mu_f*cpg_f*ep[EP_LE]/kl_f;
         double Re_f = e->Re05*e->Re05*rho_f/e->rhog*e->mug/mu_f;
-        double Sh_f = 2.0 + 0.6*sqrt(o_max2(Re_f, 0.0))*pow(Sc_f, 1.0/3.0);
-        *md = -pi*e->dp*rho_f*Dv_f*Sh_f*log(1.0 + BM);
+        double Sh_f = 2.0 + 0.6*sqrt(o_max2(Re_f, 0.0))*ice_pow(Sc_f, 1.0/3.0);
+        *md = -pi*e->dp*rho_f*Dv_f*Sh_f*ice_log(1.0 + BM);
         return;
     }
     case 4: {
         double Le = ep[EP_LE], cpv = ep[EP_CPV];
         *ovr = 1;
         double Dv = e->kg/(e->rhog*e->cpg*Le);
-        double lnBM = log(1.0 + BM);
+        double lnBM = ice_log(1.0 + BM);
         double FM = o_Fcorr(BM);
-        double Sh0 = 2.0 + 0.552*e->Re05*pow(e->Sc, 1.0/3.0);
+        double Sh0 = 2.0 + 0.552*e->Re05*ice_pow(e->Sc, 1.0/3.0);
         double Shs = 2.0 + (Sh0 - 2.0)/FM;
         *md = -pi*e->dp*e->rhog*Dv*Shs*lnBM;
         double cpv_eff = cpv > 0.0 ? cpv : e->cpg;
-        double Nu0 = 2.0 + 0.552*e->Re05*pow(e->Pr, 1.0/3.0);
+        double Nu0 = 2.0 + 0.552*e->Re05*ice_pow(e->Pr, 1.0/3.0);
         double Nus = Nu0, BT = 0.0;
         for (int it = 1; it <= 5; ++it) {
             double phi = cpv_eff/e->cpg*Shs/Nus/Le;
-            BT = pow(1.0 + BM, phi) - 1.0;
+            BT = ice_pow(1.0 + BM, phi) - 1.0;
             if (BT <= 0.0) { BT = BM; Nus = Nu0; break; }
             double FT = o_Fcorr(BT);
             Nus = 2.0 + (Nu0 - 2.0)/FT;
@@ -562,7 +568,7 @@ static inline void o_gas_side(const o_evap_env* e, double Ys, double BM, double*
         double Xs = o_min2(o_mass2molar(Ys, Mv, e->Mg), 1.0 - O_XSCAP);
         double Xinf = o_mass2molar(Yinf, Mv, e->Mg);
         double Minf = Xinf*Mv + (1.0 - Xinf)*e->Mg;
-        double rhs0 = Mv/Minf*log((1.0 - Xinf)/(1.0 - Xs));
+        double rhs0 = Mv/Minf*ice_log((1.0 - Xinf)/(1.0 - Xs));
         if (rhs0 <= 0.0) return;
         double Tts = e->Tp/e->Tg;
         double Lev = e->kg/(cpv_eff*Dv*e->rhog);
@@ -572,7 +578,7 @@ static inline void o_gas_side(const o_evap_env* e, double Ys, double BM, double*
         for (int it = 1; it <= 30; ++it) {
             double x = mhat/Lev, f, fp;
             if (x > 1.0e-6) {
-                double E = exp(-x);
+                double E = ice_exp(-x);
                 f = x/(1.0 - E);
                 fp = (1.0 - E - x*E)/((1.0 - E)*(1.0 - E));
             } else {
@@ -586,12 +592,12 @@ static inline void o_gas_side(const o_evap_env* e, double Ys, double BM, double*
             mhat = mhat - G/dG;
             if (mhat <= mlo || mhat >= mhi) mhat = 0.5*(mlo + mhi);
         }
-        double Sh = 2.0 + 0.6*e->Re05*pow(e->Sc, 1.0/3.0);
+        double Sh = 2.0 + 0.6*e->Re05*ice_pow(e->Sc, 1.0/3.0);
         *md = -pi*e->dp*e->rhog*Dv*Sh*mhat;
         *ovr = 1;
-        double Nu = 2.0 + 0.6*e->Re05*pow(e->Pr, 1.0/3.0);
+        double Nu = 2.0 + 0.6*e->Re05*ice_pow(e->Pr, 1.0/3.0);
         double chi = o_min2(-*md*cpv_eff/(pi*e->dp*e->kg*Nu), 700.0);
-        if (chi > 1.0e-9) *Qd = -*md*cpv_eff*(e->Tg - e->Tp)/(exp(chi) - 1.0);
+        if (chi > 1.0e-9) *Qd = -*md*cpv_eff*(e->Tg - e->Tp)/(ice_exp(chi) - 1.0);
         else *Qd = pi*e->dp*e->kg*Nu*(e->Tg - e->Tp);
         return;
     }
@@ -611,7 +617,7 @@ static inline void o_evaporation(double rhog, double Tg, double gamma, double Rg
     e.cpg = gamma*Rg/(gamma - 1.0);
     e.p = rhog*Rg*Tg;
     e.Mg = O_RU/Rg;
-    double psat = O_PATM*exp(-ep[EP_LVMVRU]*(1.0/Tp - ep[EP_INVTB]));
+    double psat = O_PATM*ice_exp(-ep[EP_LVMVRU]*(1.0/Tp - ep[EP_INVTB]));
     double Xs = psat >= e.p ? 1.0 - O_XSCAP : o_min2(psat/e.p, 1.0 - O_XSCAP);
     double Ys = o_molar2mass(Xs, ep[EP_MV], e.Mg);
     if (Ys <= ep[EP_YINF]) return;
@@ -684,10 +690,10 @@ static inline double o_cell_source(int cl, const double* p, const double* gas, d
     int nb = o_nbase(cl);
     double T = p[nb - 2], n = p[nb - 1];
     double rho_mat = m->rho_al;
-    double Rp = pow(0.75*p[0]/(n*pi*rho_mat), 1.0/3.0);
+    double Rp = ice_pow(0.75*p[0]/(n*pi*rho_mat), 1.0/3.0);
     double du = o_norm2(gas[1] - p[1], gas[2] - p[2], gas[3] - p[3]);
     double Re = 2.0*gas[0]*Rp*du/gmu;
-    double Ma = du/pow(ggam*gR*gas[4], 0.5);
+    double Ma = du/ice_pow(ggam*gR*gas[4], 0.5);
     double Pr = ggam/(ggam - 1.0)*gR*gmu/gk;
     double Nu = o_heat(Re, Pr, Ma, heat_sel);
     double Ts = T;                              /* ITC: drop_surface returns the mean temperature */
@@ -702,7 +708,7 @@ static inline double o_cell_source(int cl, const double* p, const double* gas, d
     else if (blow == 1) Qconv = Qconv*o_blowing(ggam, gR, gmu, gk, rho_mat, 2.0*Rp, 4.0/3.0*pi*(Rp*Rp*Rp)*rho_mat, mdot);
     F[0] = -mdot*n;
     F[4] = Qconv*n;
-    F[4] = F[4] + m->emiss*O_SIGMA_SB*4.0*pi*Rp*Rp*n*(pow(gas[4], 4.0) - pow(Ts, 4.0));
+    F[4] = F[4] + m->emiss*O_SIGMA_SB*4.0*pi*Rp*Rp*n*(ice_pow(gas[4], 4.0) - ice_pow(Ts, 4.0));
     double tau;
     if (Cd == 0.0) tau = INFINITY;
     else tau = 8.0*rho_mat*Rp/(3.0*gas[0]*Cd*du + (double)1e-20f);

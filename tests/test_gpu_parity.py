@@ -96,13 +96,46 @@ def test_crossing_jets_matches_reference_output(gpu):
     assert l2 <= 1e-12
 
 
-def test_irs_steady_bit_exact(gpu, orc):
-    def make():
-        c = configs.crossing_jets("IG", steps=100)
-        c.numerics.irs = True
-        c.numerics.irs_beta = 0.5
-        return c
-    run_pair(gpu, orc, make, 100, exact=True)
+def _irs(case):
+    case.numerics.irs = True
+    case.numerics.irs_beta = 0.5
+    case.numerics.time_accurate = False
+    return case
+
+
+def test_irs_steady_1d_bit_exact(gpu, orc):
+    # implicit residual smoothing (steady runs only): the 1-D tube converges with it
+    run_pair(gpu, orc, lambda: _irs(configs.riemann_1d(n=400, steps=100)), 100, exact=True)
+
+
+def test_irs_2d_and_3d_bit_exact(gpu, orc):
+    # both directions of the crossing jets and the three of a block tree, over the steps before
+    # the smoothed residual drives an empty cell negative
+    run_pair(gpu, orc, lambda: _irs(configs.crossing_jets("IG", steps=20)), 20, exact=True)
+    def mb():
+        c = configs.multiblock_tree(nblocks=6, seed=3, lo=6, hi=10, steps=10)
+        c.numerics.coupled = False
+        c.numerics.shock_detector = False
+        c.gas = []
+        return _irs(c)
+    run_pair(gpu, orc, mb, 10, exact=True)
+
+
+def test_irs_failure_at_the_same_iteration(gpu, orc):
+    """Where the reference's algorithm itself breaks down (IRS spreading mass into empty cells),
+    the device stops at the same iteration with the same status as the oracle."""
+    make = lambda: _irs(configs.crossing_jets("IG", steps=100))
+    sg, so = Solver(make(), gpu), Solver(make(), orc)
+    fail_g = fail_o = None
+    for n in range(1, 101):
+        if fail_g is None and sg.step(1, check=False).status:
+            fail_g = (n, sg.last.status)
+        if fail_o is None and so.step(1, check=False).status:
+            fail_o = (n, so.last.status)
+        if fail_g and fail_o:
+            break
+    assert fail_o is not None and fail_g is not None
+    assert fail_g[0] == fail_o[0] and (fail_g[1] & fail_o[1])
 
 
 def test_jets_2d_coupled(gpu, orc):
