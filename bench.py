@@ -1,7 +1,8 @@
 """Benchmark of the solve stage on B200: cell-updates/s of ICE's dispersed-phase time step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload multiblock48|cloud192|jets1024|riemann2000]
+                    [--workload multiblock48|cloud192|cloud96|jets1024|riemann2000]
+                    [--precision fp32flux|fp64] [--no-plain] [--timed-only]
 
 One "step" is one full time step (every family, every RK stage) of the workload. The default
 workload is the 3-D multi-block evaporating case (48 blocks of U[16,160] cells per axis, seed 9,
@@ -39,7 +40,7 @@ from ice_b200 import abi, configs  # noqa: E402
 from ice_b200.solver import Solver  # noqa: E402
 
 KC_STAGE = 4
-KC_NAMES = ["dt", "ghost", "beta", "bound", "stage", "irs", "norm"]
+KC_NAMES = ["dt", "ghost", "beta", "bound", "stage", "irs", "norm", "source"]
 
 
 def peaks():
@@ -55,6 +56,8 @@ def make_workload(name: str, precision: int, steps: int):
         return configs.multiblock_tree(steps=steps, precision=precision)
     if name == "cloud192":
         return configs.cloud_3d(n=192, steps=steps, precision=precision)
+    if name == "cloud96":       # the same recipe at 96^3 (0.88 M cells), the profiling case
+        return configs.cloud_3d(n=96, steps=steps, length=0.0096, precision=precision)
     if name == "jets1024":
         return configs.jets_2d(n=1024, steps=steps, precision=precision)
     if name == "riemann2000":
@@ -66,22 +69,27 @@ def sample_workload(name: str):
     """A bounded sample of the workload for the CPU legs: the first blocks of the same tree, or the
     same case at a reduced size."""
     if name == "multiblock48":
-        return configs.multiblock_tree(nblocks=4, steps=1), "first 4 blocks of the seed-9 tree"
+        return configs.multiblock_tree(nblocks=4, steps=1), "the same recipe with 4 blocks (seed 9)"
     if name == "cloud192":
-        return configs.cloud_3d(n=64, steps=1, length=0.0064), "64^3 cut of the same recipe"
+        return configs.cloud_3d(n=64, steps=1, length=0.0064), "64^3 of the same recipe"
+    if name == "cloud96":
+        return configs.cloud_3d(n=48, steps=1, length=0.0048), "48^3 of the same recipe"
     if name == "jets1024":
         return configs.jets_2d(n=256, steps=1), "256^2 of the same recipe"
     return configs.riemann_1d(n=2000, steps=1), "the whole case"
 
 
 def algorithmic_bytes(case) -> float:
-    """Bytes one launch of the stage kernel must move per cell, FP64 state (SURVEY 8(d) per
-    stage): read U_(k-1) and U_0, write U_k (24 nc); face normals, areas and lengths of each
-    direction and the volume (8 (5 ndir + 1)); the gas and tau of a coupled run (80)."""
+    """Bytes one launch of the stage kernel must move per cell, averaged over the families: read
+    U_(k-1) and U_0 and write U_k (24 nc, FP64 state); the source S of a coupled run (8 nc); per
+    direction the face normal and area (32) and the cell length (8); the volume (8); the boundary
+    map (4); the sensor weight (8) when the shock detector is on; the local dt (8) in steady mode."""
     ndir = case.ndir
     per = []
     for f in case.families:
-        b = 24 * f.nc + 8 * (5 * ndir + 1) + (80 if case.numerics.coupled else 0)
+        b = 24 * f.nc + (8 * f.nc if case.numerics.coupled else 0) + 40 * ndir + 8 + 4
+        if case.numerics.shock_detector:
+            b += 8
         if not case.numerics.time_accurate:
             b += 8
         per.append(b)
@@ -147,140 +155,212 @@ def rel_l1(a_states, b_states, case):
     return out
 
 
-def cpu_sample(name, steps=1, threads=0):
-    """The oracle (OpenMP, every host core) on a bounded sample: cell-updates/s."""
-    import oracle
-    orc = oracle.load()
-    n = orc.set_threads(threads)
-    case, what = sample_workload(name)
-    s = Solver(case, orc)
-    t = time.perf_counter()
-    out = s.step(steps)
-    dt = time.perf_counter() - t
-    assert out.status == 0
-    return case.ncells * steps / dt, n, f"{what}: {case.ncells} cells, {steps} step(s), {dt:.2f} s"
+class CpuSample:
+    """The oracle (OpenMP, every host core) on a bounded sample of the workload."""
+
+    def __init__(self, name, threads=0):
+        import oracle
+        self.orc = oracle.load()
+        self.cores = self.orc.set_threads(threads)
+        self.case, self.what = sample_workload(name)
+        self.solver = Solver(self.case, self.orc)
+
+    def step(self):
+        t = time.perf_counter()
+        out = self.solver.step(1)
+        dt = time.perf_counter() - t
+        if out.status != 0:
+            raise SystemExit(f"oracle step status {out.status}")
+        return self.case.ncells / dt, dt
+
+    def describe(self, secs):
+        return f"{self.what}: {self.case.ncells} cells, 1 step per sample, {secs:.2f} s"
 
 
 def run_reference(args, rank, world):
+    """The reference arm: rank 0 alone times the FP64 CPU restatement; other ranks do nothing."""
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
-    rates = []
+    cs = CpuSample(args.workload, os.cpu_count() or 1)
     for _ in range(args.warmup):
-        cpu_sample(args.workload, 1, cores)
-    t_total = 0.0
-    desc = ""
+        cs.step()
+    rates, secs = [], []
     for _ in range(args.steps):
-        r, n, desc = cpu_sample(args.workload, 1, cores)
+        r, dt = cs.step()
         rates.append(r)
+        secs.append(dt)
     v = float(statistics.median(rates))
     line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": args.workload, "form": "FP64 CPU (oracle restatement, OpenMP)"},
-            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": n, "kind": "port", "sample": desc},
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(statistics.median(secs)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": args.workload, "form": "FP64 CPU restatement of the reference (OpenMP)"},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cs.cores, "kind": "port",
+                             "sample": cs.describe(float(statistics.median(secs)))},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def pinned_like(arrays):
+    """Page-locked host copies of the state arrays (torch's pinned allocator), or plain copies."""
+    try:
+        import torch
+        out = []
+        for a in arrays:
+            t = torch.empty(a.shape, dtype=torch.float64).pin_memory()
+            v = t.numpy()
+            v[...] = a
+            out.append((t, v))
+        return [v for _, v in out], [t for t, _ in out], True
+    except Exception:
+        return [np.array(a) for a in arrays], [], False
+
+
+def e2e_run(lib, case, steps):
+    """The step through the C ABI with host buffers, as a driver that keeps its state on the host
+    would call it: every step uploads every block and family from page-locked host memory, steps
+    once and downloads the new state; wall time over the whole loop."""
+    flat = [a for per in case.state for a in per]
+    host, keep, pinned = pinned_like(flat)
+    nfam = len(case.families)
+    states = [host[b * nfam:(b + 1) * nfam] for b in range(len(case.state))]
+    outs, _, _ = pinned_like(flat)
+    s = Solver(case, lib)
+    s.step(1)
+    h2d = d2h = 0
+    t = time.perf_counter()
+    for _ in range(steps):
+        for b, per in enumerate(states):
+            for p, a in enumerate(per):
+                s._check(lib.upload_state(s.ctx, b + 1, p + 1, abi.ptr(a), None), "upload_state")
+                h2d += a.nbytes
+        s.step(1)
+        for q, a in enumerate(outs):
+            b, p = divmod(q, nfam)
+            s._check(lib.download_state(s.ctx, b + 1, p + 1, abi.ptr(a)), "download_state")
+            d2h += a.nbytes
+    secs = time.perf_counter() - t
+    s.close()
+    del keep
+    return case.ncells * steps / secs, h2d // steps, d2h // steps, pinned
+
+
+def allmax(dist, x: float) -> float:
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, dist):
     lib = abi.load_gpu()
-    # the chosen form and, beside it, the plain FP64 form on the same inputs
+    prec = abi.PREC_FP32FLUX if args.precision == "fp32flux" else abi.PREC_FP64
     t0 = time.perf_counter()
-    case = make_workload(args.workload, abi.PREC_FP32FLUX if args.precision == "fp32flux" else abi.PREC_FP64,
-                         args.warmup + args.steps)
+    case = make_workload(args.workload, prec, args.warmup + args.steps)
     setup_s = time.perf_counter() - t0
+    cells = case.ncells
+
+    # the timed region: K steps of the chosen form, device time on the library's stream
     chosen = Solver(case, lib)
     chosen.step(args.warmup)
     if dist:
         dist.barrier()
     with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         out = chosen.step(args.steps)
-    ms = out.device_ms
     if out.status != 0:
         raise SystemExit(f"step status {out.status}")
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    cells = case.ncells
+    ms = allmax(dist, out.device_ms)
     value = cells * args.steps * world / (ms * 1e-3)
+    if args.timed_only:         # the timed region alone (profiler runs)
+        chosen.close()
+        if rank == 0:
+            print(json.dumps({"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                              "config": {"workload": args.workload, "cells": cells, "form": args.precision},
+                              "note": "timed region only"}), flush=True)
+        return
 
     extra = {}
     if rank == 0:
         states_chosen = chosen.download_all()
-        # plain FP64 form, same inputs, same steps
-        plain_rate = None
-        l1 = None
-        if args.precision == "fp32flux" and not args.no_plain:
+        chosen.close()
+        # the plain FP64 form on the same inputs, and the L1 error of the chosen form against it
+        plain_rate = l1 = None
+        if prec == abi.PREC_FP32FLUX and not args.no_plain:
             case.numerics.precision = abi.PREC_FP64
-            P = case.params()
-            chosen.close()
             plain = Solver(case, lib)
             plain.step(args.warmup)
             o2 = plain.step(args.steps)
             plain_rate = cells * args.steps / (o2.device_ms * 1e-3)
             l1 = rel_l1(states_chosen, plain.download_all(), case)
             plain.close()
-            case.numerics.precision = abi.PREC_FP32FLUX
-        else:
-            chosen.close()
-        # stage-kernel roofline: per-class device time of a profiled pass
+            case.numerics.precision = prec
+        del states_chosen
+        # per-class device time of a profiled pass (CUDA events around every launch)
         prof = Solver(case, lib)
         prof.step(args.warmup)
         lib.set_profiling(prof.ctx, 1)
         nprof = max(2, min(args.steps, 5))
         prof.step(nprof)
-        kt = np.zeros(7)
+        kt = np.zeros(len(KC_NAMES))
         nl = C.c_int64()
-        lib.kernel_times(prof.ctx, abi.ptr(kt), 7, C.byref(nl))
+        lib.kernel_times(prof.ctx, abi.ptr(kt), len(KC_NAMES), C.byref(nl))
+        prof.close()
         launches_per_step = nl.value / nprof
         nfam, nrk = len(case.families), case.params().nrk
         stage_ms = kt[KC_STAGE] / (nprof * nfam * nrk)
         bpc = algorithmic_bytes(case)
         achieved = bpc * cells / (stage_ms * 1e-3) / 1e9
         peak, peak_kind = peaks()
-        # e2e through the C ABI with host buffers: upload of the states, K steps, download
-        states_host = case.state
-        h2d = sum(a.nbytes for per in states_host for a in per)
-        t_e = time.perf_counter()
-        prof.upload(states_host)
-        lib.set_profiling(prof.ctx, 0)
-        o3 = prof.step(args.steps)
-        back = prof.download_all()
-        e2e_s = time.perf_counter() - t_e
-        d2h = sum(a.nbytes for per in back for a in per)
-        prof.close()
-        cpu_v, cpu_n, cpu_desc = cpu_sample(args.workload, 1, os.cpu_count() or 1)
         extra = {
-            "e2e": {"value": cells * args.steps / e2e_s, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": "k_stage", "bytes_per_cell": bpc,
-                         "note": f"peak of {peak_kind}; achieved = algorithmic bytes / CUDA-event time of the stage kernel"},
-            "cpu_baseline": {"value": cpu_v, "unit": "cell-updates/s", "cores": cpu_n, "kind": "port",
-                             "sample": cpu_desc},
+                         "launch_ms": stage_ms,
+                         "note": f"peak of {peak_kind}; achieved = algorithmic bytes per launch / mean CUDA-event "
+                                 f"duration of the stage kernel's launches"},
             "plain_fp64": {"value": plain_rate, "unit": "cell-updates/s"} if plain_rate else None,
             "chosen_vs_plain": (value / world / plain_rate) if plain_rate else None,
             "l1_error_vs_plain": l1,
             "kernel_ms_per_step": {n: round(float(x) / nprof, 4) for n, x in zip(KC_NAMES, kt)},
-            "gpu_launches": int(launches_per_step * args.steps),
+            "gpu_launches": int(round(launches_per_step * args.steps)),
             "setup_s": round(setup_s, 1),
         }
-        line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32 flux / f64 accumulate" if args.precision == "fp32flux" else "f64",
-                "data": "synthetic (seeded)",
-                "config": {"workload": args.workload, "cells": cells, "families": [f.closure for f in case.families],
-                           "form": args.precision, "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (state of every family in HBM, several GB)"},
-                "clocks": clk.summary()}
-        line.update(extra)
-        print(json.dumps(line), flush=True)
     else:
         chosen.close()
+    if dist:
+        dist.barrier()
+
+    # end to end through the C ABI with host buffers, every rank, slowest rank
+    e2e_v, h2d, d2h, pinned = e2e_run(lib, case, args.steps)
+    e2e_secs = allmax(dist, cells * args.steps / e2e_v)
+    if rank != 0:
+        return
+    extra["e2e"] = {"value": cells * args.steps * world / e2e_secs, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "host_memory": "pinned" if pinned else "pageable",
+                    "form": "every step: upload of every block and family, one step, download"}
+    if world == 1:
+        cs = CpuSample(args.workload, os.cpu_count() or 1)
+        cs.step()
+        n, secs = 0, 0.0
+        while secs < 10.0 and n < 50:          # about ten seconds of host work
+            secs += cs.step()[1]
+            n += 1
+        extra["cpu_baseline"] = {"value": cs.case.ncells * n / secs, "unit": "cell-updates/s", "cores": cs.cores,
+                                 "kind": "port", "sample": f"{cs.what}: {cs.case.ncells} cells, {n} step(s), "
+                                                           f"{secs:.1f} s"}
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 flux / f64 accumulate" if prec == abi.PREC_FP32FLUX else "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "cells": cells, "families": [f.closure for f in case.families],
+                       "form": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (the state of every family is several GB in HBM)"},
+            "clocks": clk.summary()}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -291,22 +371,23 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="multiblock48")
     ap.add_argument("--precision", default="fp32flux", choices=["fp64", "fp32flux"])
-    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 form beside the chosen one")
+    ap.add_argument("--timed-only", action="store_true", help="only the timed steps (for profiler runs)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
     if world > 1:
         import datetime
         import torch
         import torch.distributed as tdist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        tdist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=600))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = tdist
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-    else:
-        run_ours(args, rank, world, dist)
+    run_ours(args, rank, world, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

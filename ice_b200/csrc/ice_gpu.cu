@@ -41,6 +41,7 @@ using namespace ice;
 namespace {
 
 constexpr int kMaxF = ICE_GPU_MAX_FAMILIES;
+constexpr int kMaxNC = 12;     // variables of the largest closure (AG)
 
 // ------------------------------------------------------------------ host side
 struct HRec {
@@ -103,10 +104,23 @@ struct ice_gpu_ctx {
   double kms[KC_N] = {0};
   long long nlaunch = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf<double> xfer;    // one block of one family in the caller's layout (upload/download)
+  long long ng_max = 0;
   std::string err;
 };
 
 static std::string g_create_err;
+
+// The caller's prim(nc, -1:ni+2, -1:nj+2, -1:nk+2) (variable fastest) <-> one block of the SoA pool.
+__global__ void k_aos2soa(const double* __restrict__ a, double* __restrict__ s, long long NG, long long n, int nc) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    for (int v = 0; v < nc; ++v) s[(long long)v * NG + q] = a[(long long)nc * q + v];
+}
+__global__ void k_soa2aos(const double* __restrict__ s, double* __restrict__ a, long long NG, long long n, int nc) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    for (int v = 0; v < nc; ++v) a[(long long)nc * q + v] = s[(long long)v * NG + q];
+}
+static unsigned grid_of(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
 
 static int fail(ice_gpu_ctx* c, int code, const char* fmt, ...) {
   char buf[1024];
@@ -245,7 +259,7 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
 static void tile_shape(int ndir, int& TX, int& TY, int& KZ) {
   if (ndir == 1) { TX = 256; TY = 1; KZ = 1; }
   else if (ndir == 2) { TX = 32; TY = 8; KZ = 1; }
-  else { TX = 32; TY = 8; KZ = 32; }
+  else { TX = 16; TY = 16; KZ = 32; }
   if (const char* e = getenv("ICE_GPU_TILE")) {        // "TXxTYxKZ", for the tile tuner
     int a, b, k;
     if (sscanf(e, "%dx%dx%d", &a, &b, &k) == 3 && a * b == 256 && a >= 2 && k >= 1) { TX = a; TY = b; KZ = k; }
@@ -314,6 +328,7 @@ int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims
     B.ni = ni; B.nj = nj; B.nk = nk; B.pad = 0;
     B.goff = G; B.ioff = I; B.roff = R; B.foff[0] = F0; B.foff[1] = F1; B.foff[2] = F2;
     G += (long long)(ni + 4) * (nj + 4) * (nk + 4);
+    c->ng_max = std::max(c->ng_max, (long long)(ni + 4) * (nj + 4) * (nk + 4));
     I += (long long)ni * nj * nk;
     R += (long long)(ni + 2) * (nj + 2) * (nk + 2);
     F0 += (long long)(ni + 1) * nj * nk; F1 += (long long)ni * (nj + 1) * nk; F2 += (long long)ni * nj * (nk + 1);
@@ -441,13 +456,13 @@ int ice_gpu_upload_state(ice_gpu_ctx* c, int32_t b1, int32_t p1, const double* p
   const DBlock& B = c->hblk[b1 - 1];
   FamHost& H = c->fam[p1 - 1];
   long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
-  std::vector<double> tmp(ng);
+  if (!c->xfer.p) CK(c->xfer.alloc((size_t)c->ng_max * kMaxNC));
   CK(cudaStreamSynchronize(c->stream));
-  for (int v = 0; v < H.nc; ++v) {
-    for (long long q = 0; q < ng; ++q) tmp[q] = prim[(long long)H.nc * q + v];
-    CK(cudaMemcpy(H.S[c->phase].p + (long long)v * c->NG + B.goff, tmp.data(), ng * sizeof(double), cudaMemcpyHostToDevice));
-  }
-  if (inj) CK(cudaMemcpy(H.inj.p + B.goff, inj, ng, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(c->xfer.p, prim, (size_t)ng * H.nc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_aos2soa<<<grid_of(ng), 256, 0, c->stream>>>(c->xfer.p, H.S[c->phase].p + B.goff, c->NG, ng, H.nc);
+  CK(cudaGetLastError());
+  if (inj) CK(cudaMemcpyAsync(H.inj.p + B.goff, inj, ng, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   c->prev_phase = -1;
   return 0;
 }
@@ -458,12 +473,12 @@ int ice_gpu_download_state(ice_gpu_ctx* c, int32_t b1, int32_t p1, double* prim)
   const DBlock& B = c->hblk[b1 - 1];
   FamHost& H = c->fam[p1 - 1];
   long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
-  std::vector<double> tmp(ng);
+  if (!prim) return fail(c, ICE_GPU_EINVAL, "download_state: null prim");
+  if (!c->xfer.p) CK(c->xfer.alloc((size_t)c->ng_max * kMaxNC));
+  k_soa2aos<<<grid_of(ng), 256, 0, c->stream>>>(H.S[c->phase].p + B.goff, c->xfer.p, c->NG, ng, H.nc);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(prim, c->xfer.p, (size_t)ng * H.nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int v = 0; v < H.nc; ++v) {
-    CK(cudaMemcpy(tmp.data(), H.S[c->phase].p + (long long)v * c->NG + B.goff, ng * sizeof(double), cudaMemcpyDeviceToHost));
-    for (long long q = 0; q < ng; ++q) prim[(long long)H.nc * q + v] = tmp[q];
-  }
   return 0;
 }
 

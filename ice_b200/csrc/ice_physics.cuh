@@ -239,6 +239,28 @@ template <int CL, typename R> __device__ __forceinline__ void flux_make(const R*
   }
 }
 
+// The pressure part P of a flux, f = un*c + P (zero for MK), as the FP32-flux form splits it.
+// Derived from flux_make and prim2cons: IG P_i = p n_i, P_4 = 2 p un, P_5 = p un; AG P_i = (P n)_i,
+// P_ij = u_i (P n)_j + u_j (P n)_i, P_10 = u.(P n) - tr(P) un eps / 2(rho + eps).
+template <int CL, typename R> __device__ __forceinline__ void press_part(const R* p, const R* n, R un, R* P) {
+  constexpr int nc = NC<CL>::v;
+#pragma unroll
+  for (int v = 0; v < nc; ++v) P[v] = (R)0;
+  if constexpr (CL == IG) {
+    P[1] = p[4]*n[0]; P[2] = p[4]*n[1]; P[3] = p[4]*n[2];
+    P[4] = (R)2*p[4]*un; P[5] = p[4]*un;
+  } else if constexpr (CL == AG) {
+    R p1n = p[4]*n[0] + p[5]*n[1] + p[6]*n[2];
+    R p2n = p[5]*n[0] + p[7]*n[1] + p[8]*n[2];
+    R p3n = p[6]*n[0] + p[8]*n[1] + p[9]*n[2];
+    P[1] = p1n; P[2] = p2n; P[3] = p3n;
+    P[4] = (R)2*p[1]*p1n; P[5] = p[1]*p2n + p[2]*p1n; P[6] = p[1]*p3n + p[3]*p1n;
+    P[7] = (R)2*p[2]*p2n; P[8] = p[2]*p3n + p[3]*p2n; P[9] = (R)2*p[3]*p3n;
+    P[10] = p[1]*p1n + p[2]*p2n + p[3]*p3n
+          - (R)0.5*(p[4] + p[7] + p[9])*un*(epsv<R>()/(p[0] + epsv<R>()));
+  }
+}
+
 // H P H, H = I - 2 n n^T (Lib_Model_AG.f90:181-200)
 __device__ __forceinline__ void mirror_tensor(const double* p, const double* n, double* pm) {
   double t0 = p[0]*n[0] + p[1]*n[1] + p[2]*n[2];
@@ -254,19 +276,29 @@ __device__ __forceinline__ void mirror_tensor(const double* p, const double* n, 
 }
 
 // ------------------------------------------------------------------ limiters
+// The slope ratio y / (x + 1e-30). In single precision it is clamped to |r| <= 1e15: a zero slope
+// beside a steep one (number densities reach 1e19 m^-4) would overflow to infinity and every
+// limiter would return inf/inf; all of them have reached their limit value long before 1e15
+// (and cy r > 2 there), so the clamp changes no limited slope.
+template <typename R> __device__ __forceinline__ R slope_ratio(R y, R x) {
+  R ru = y / (x + (R)1e-30);
+  if constexpr (sizeof(R) == 4) ru = fmaxf(fminf(ru, 1e15f), -1e15f);
+  return ru;
+}
+
 template <int LIM, typename R> __device__ __forceinline__ R limiter(int lim, R x, R y, R cx, R cy) {
   if constexpr (LIM == ICE_LIM_VANLEER) {
-    R ru = y / (x + (R)1e-30);
+    R ru = slope_ratio(y, x);
     R phi = (ru + fabs(ru)) / ((R)1 + fabs(ru));
     if (ru > (R)0) phi = mn(mn(phi, cx), cy*ru);
     return phi * x;
   } else if constexpr (LIM == ICE_LIM_MINMOD) {
-    R ru = y / (x + (R)1e-30);
+    R ru = slope_ratio(y, x);
     R phi = mx((R)0, mn((R)1, ru));
     return phi * x;
   }
   if (lim == ICE_LIM_IORD) return (R)0;
-  R ru = y / (x + (R)1e-30), phi;
+  R ru = slope_ratio(y, x), phi;
   switch (lim) {
     case ICE_LIM_MINMOD: phi = mx((R)0, mn((R)1, ru)); return phi * x;
     case ICE_LIM_VANALBADA: phi = (ru*ru + ru) / (ru*ru + (R)1); break;
@@ -340,6 +372,13 @@ __device__ __forceinline__ bool reconstruct(int lim, const Q& q, R dl0, R dl1, R
 }
 
 // ------------------------------------------------------------------ Riemann
+// The plain form evaluates the reference's formulas in its order. The FP32-flux form evaluates
+// Rusanov and the HLLE mixed state in the upwind-split form sum_s ((un_s - S_s) c_s + P_s), which
+// is the same expression regrouped: the mass flux it gives from a state is zero exactly when that
+// state's weight (un_s - S_s) is, and its other fluxes stay in proportion. Unsplit, a full cell
+// moving away from an empty neighbour leaves f - A c = one single-precision rounding of its
+// momentum flux with no mass flux beside it, and the neighbour's velocity becomes that residual
+// over its near-zero density.
 template <typename R> __device__ __forceinline__ void saurel(const R* p1, const R* p4, const R* n, R* f, R cp) {
   R vn1 = p1[1]*n[0] + p1[2]*n[1] + p1[3]*n[2];
   R vn4 = p4[1]*n[0] + p4[2]*n[1] + p4[3]*n[2];
@@ -366,11 +405,18 @@ template <int CL, typename R> __device__ __forceinline__ void rusanov(const R* p
   R vn4 = p4[1]*n[0] + p4[2]*n[1] + p4[3]*n[2];
   R s1 = wavespeed<CL>(p1, n), s4 = wavespeed<CL>(p4, n);
   prim2cons<CL>(p1, c1, cp); prim2cons<CL>(p4, c4, cp);
-  flux_make<CL>(p1, n, f1, cp); flux_make<CL>(p4, n, f4, cp);
   R A = fabs(vn1 - s1);
   A = mx(A, (R)fabs(vn4 - s4)); A = mx(A, (R)fabs(vn1 + s1)); A = mx(A, (R)fabs(vn4 + s4));
+  if constexpr (sizeof(R) == 4) {
+    press_part<CL>(p1, n, vn1, f1); press_part<CL>(p4, n, vn4, f4);
+    R a1 = vn1 + A, a4 = vn4 - A;
 #pragma unroll
-  for (int v = 0; v < nc; ++v) f[v] = (R)0.5 * (f1[v] + f4[v] - A*(c4[v] - c1[v]));
+    for (int v = 0; v < nc; ++v) f[v] = (R)0.5 * ((a1*c1[v] + f1[v]) + (a4*c4[v] + f4[v]));
+  } else {
+    flux_make<CL>(p1, n, f1, cp); flux_make<CL>(p4, n, f4, cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) f[v] = (R)0.5 * (f1[v] + f4[v] - A*(c4[v] - c1[v]));
+  }
 }
 
 template <int CL, typename R> __device__ __forceinline__ void hlle(const R* p1, const R* p4, const R* n, R* f, R cp) {
@@ -396,10 +442,17 @@ template <int CL, typename R> __device__ __forceinline__ void hlle(const R* p1, 
     flux_make<CL>(p4, n, f, cp);
   } else {
     R f1[nc], f4[nc], c1[nc], c4[nc];
-    flux_make<CL>(p1, n, f1, cp); flux_make<CL>(p4, n, f4, cp);
     prim2cons<CL>(p1, c1, cp); prim2cons<CL>(p4, c4, cp);
+    if constexpr (sizeof(R) == 4) {
+      press_part<CL>(p1, n, vn1, f1); press_part<CL>(p4, n, vn4, f4);
+      R a1 = vn1 - S1, a4 = vn4 - S4;
 #pragma unroll
-    for (int v = 0; v < nc; ++v) f[v] = (S4*f1[v] - S1*f4[v] + S1*S4*(c4[v] - c1[v])) / (S4 - S1);
+      for (int v = 0; v < nc; ++v) f[v] = (S4*(a1*c1[v] + f1[v]) - S1*(a4*c4[v] + f4[v])) / (S4 - S1);
+    } else {
+      flux_make<CL>(p1, n, f1, cp); flux_make<CL>(p4, n, f4, cp);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) f[v] = (S4*f1[v] - S1*f4[v] + S1*S4*(c4[v] - c1[v])) / (S4 - S1);
+    }
   }
 }
 
