@@ -44,10 +44,20 @@ def _newer(target: Path, deps) -> bool:
     return target.exists() and all(p.stat().st_mtime <= target.stat().st_mtime for p in deps)
 
 
+def flags_of(unit: str):
+    """The FP32-flux units (*_f32.cu) keep no bit-for-bit tie to the reference's order of operations:
+    they contract a*b + c into fused multiply-adds and take single-precision divisions, square roots
+    and elementary functions at hardware speed (--use_fast_math, which leaves double precision
+    alone). Every other unit keeps --fmad=false."""
+    if unit.endswith("_f32.cu"):
+        return [f if f != "--fmad=false" else "--fmad=true" for f in FLAGS] + ["--use_fast_math"]
+    return FLAGS
+
+
 def _compile(unit: str, verbose: bool, extra) -> str:
     src = SRC / unit
     obj = OBJ / (unit[:-3] + ".o")
-    cmd = [nvcc(), *ARCH, *FLAGS, "-c", "-o", str(obj), str(src), *extra]
+    cmd = [nvcc(), *ARCH, *flags_of(unit), "-c", "-o", str(obj), str(src), *extra]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -26,8 +26,8 @@ void launch_family_t(const LaunchArgs& a) {
   cudaStream_t s = a.s;
   auto tick = [&](int cls) { if (a.tick) a.tick(a.tick_ctx, cls, s); };
   auto grid = [](long long n, int t) { return (unsigned)((n + t - 1) / t); };
-  if (a.F.coupled) {          // compute_source comes first in the stage (Mod_Explicit.f90:111-117)
-    launch_source_of<CL>(a);
+  if (a.F.coupled && a.ntile3 == 0) {   // compute_source comes first in the stage (Mod_Explicit.f90:111-117);
+    launch_source_of<CL>(a);              // the staged stage kernel evaluates it per cell itself
     tick(KC_SOURCE);
   }
   if (a.nrec > 0) {

@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <memory>
 #include "ice_kernels.cuh"
+#include "ice_stage3.cuh"
 #include "../../include/ice_gpu.h"
 
 using namespace ice;
@@ -69,6 +70,9 @@ struct FamHost {
   DevBuf<double> Rb, connF, resid, resid2, resid3, src;
   DevBuf<DRec> recs;
   DevBuf<int> bfirst, blist, own;
+  DevBuf<CUtensorMap> maps[3];               // per state buffer, per block: the staged kernel's TMA maps
+  DevBuf<Tile> tiles3;                       // the staged kernel's tiles (the tile shape is the closure's)
+  int ntile3 = 0;
   int nrec = 0, nbc = 0, nown = 0, ncf = 0;
   std::vector<int> h_first, h_list, h_own;   // 0-based record numbers of the whole table
 };
@@ -91,6 +95,7 @@ struct ice_gpu_ctx {
   std::vector<HRec> recs;
   DevBuf<Tile> tiles;
   int ntile = 0, TX = 0, TY = 0, KZ = 0;
+  bool staged = false;    // 2-D and 3-D runs: the staged stage kernel (ice_stage3.cuh)
   DevBuf<NormChunk> chunks;
   DevBuf<double> npart;
   int nchunk = 0;
@@ -111,14 +116,30 @@ struct ice_gpu_ctx {
 
 static std::string g_create_err;
 
-// The caller's prim(nc, -1:ni+2, -1:nj+2, -1:nk+2) (variable fastest) <-> one block of the SoA pool.
-__global__ void k_aos2soa(const double* __restrict__ a, double* __restrict__ s, long long NG, long long n, int nc) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    for (int v = 0; v < nc; ++v) s[(long long)v * NG + q] = a[(long long)nc * q + v];
+// The caller's prim(nc, -1:ni+2, -1:nj+2, -1:nk+2) (variable fastest) <-> one block of the SoA pool,
+// whose rows are px long (the row padding is never read).
+__device__ __forceinline__ long long pool_of(long long q, int ni4, int nj4, int px) {
+  long long x = q % ni4, r = q / ni4;
+  return (r / nj4) * ((long long)px * nj4) + (r % nj4) * px + x;
 }
-__global__ void k_soa2aos(const double* __restrict__ s, double* __restrict__ a, long long NG, long long n, int nc) {
+__global__ void k_aos2soa(const double* __restrict__ a, double* __restrict__ s, long long NG, long long n, int nc,
+                          int ni4, int nj4, int px) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    long long d = pool_of(q, ni4, nj4, px);
+    for (int v = 0; v < nc; ++v) s[(long long)v * NG + d] = a[(long long)nc * q + v];
+  }
+}
+__global__ void k_soa2aos(const double* __restrict__ s, double* __restrict__ a, long long NG, long long n, int nc,
+                          int ni4, int nj4, int px) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    long long d = pool_of(q, ni4, nj4, px);
+    for (int v = 0; v < nc; ++v) a[(long long)nc * q + v] = s[(long long)v * NG + d];
+  }
+}
+__global__ void k_inj2pool(const unsigned char* __restrict__ a, unsigned char* __restrict__ s, long long n,
+                           int ni4, int nj4, int px) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    for (int v = 0; v < nc; ++v) a[(long long)nc * q + v] = s[(long long)v * NG + q];
+    s[pool_of(q, ni4, nj4, px)] = a[q];
 }
 static unsigned grid_of(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
 
@@ -138,6 +159,11 @@ static void free_graphs(ice_gpu_ctx* c) {
   for (auto& g : c->graph) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
+// The buffer stage srk reads as its stencil (U_{k-1}) when the step starts from buffer `phase`.
+static int stencil_buffer(const ice_gpu_ctx*, int srk, int phase) {
+  return srk == 1 ? phase : srk == 2 ? (phase + 1) % 3 : (phase + 2) % 3;
+}
+
 static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   FamHost& H = c->fam[p];
   const ice_gpu_family& pf = c->P.fam[p];
@@ -152,9 +178,9 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   F.mat.evap = pf.evap; F.mat.intf = pf.intf;
   for (int q = 0; q < ICE_GPU_NEP; ++q) F.mat.ep[q] = pf.ep[q];
   // buffer roles (see the rotation in step_graph)
-  int a = phase, b = (phase + 1) % 3, cc = (phase + 2) % 3;
-  int up = srk == 1 ? a : srk == 2 ? b : cc;
-  int out = srk == 1 ? b : srk == 2 ? cc : b;
+  int a = phase, b = (phase + 1) % 3;
+  int up = stencil_buffer(c, srk, phase);
+  int out = srk == 1 ? b : srk == 2 ? (phase + 2) % 3 : b;
   F.U0 = H.S[a].p; F.Up = H.S[up].p; F.Ug = H.S[up].p; F.Uo = H.S[out].p;
   F.inj = H.inj.p;
   F.beta = c->P.shock_detector ? H.beta.p : nullptr;
@@ -195,6 +221,8 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   a.own = H.own.p; a.nown = H.nown;
   a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc;
   a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.KZ = c->KZ;
+  a.tiles3 = H.tiles3.p; a.ntile3 = H.ntile3;
+  a.maps = H.maps[stencil_buffer(c, srk, phase)].p;
   a.ndir = c->P.ndir; a.sd = c->P.shock_detector; a.irs = c->P.irs; a.precision = c->P.precision;
   a.irs_beta = c->P.irs_beta;
   a.resid = H.resid.p; a.resid2 = H.resid2.p; a.resid3 = H.resid3.p;
@@ -246,7 +274,8 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
   long long n = 2 + c->P.nfam;
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
-    long long per = (H.nrec > 0 ? 2 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) + (c->P.coupled ? 1 : 0);
+    long long per = (H.nrec > 0 ? 2 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
+                    (c->P.coupled && !c->staged ? 1 : 0);
     per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
     n += per * c->P.nrk;
   }
@@ -269,16 +298,41 @@ static void tile_shape(int ndir, int& TX, int& TY, int& KZ) {
 static int build_tiles(ice_gpu_ctx* c) {
   tile_shape(c->P.ndir, c->TX, c->TY, c->KZ);
   std::vector<Tile> t;
-  for (int b = 0; b < c->nb; ++b) {
-    int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
-    int sx = ni >= 2 ? c->TX - 1 : 1, sy = nj >= 2 ? std::max(c->TY - 1, 1) : 1;
-    for (int k = 0; k < nk; k += c->KZ)
-      for (int j = 0; j < nj; j += sy)
-        for (int i = 0; i < ni; i += sx) t.push_back(Tile{b, i, j, k});
+  if (c->P.ndir == 1) {
+    for (int b = 0; b < c->nb; ++b) {
+      int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
+      int sx = ni >= 2 ? c->TX - 1 : 1, sy = nj >= 2 ? std::max(c->TY - 1, 1) : 1;
+      for (int k = 0; k < nk; k += c->KZ)
+        for (int j = 0; j < nj; j += sy)
+          for (int i = 0; i < ni; i += sx) t.push_back(Tile{b, i, j, k, std::min(c->KZ, nk - k)});
+    }
+    c->ntile = (int)t.size();
+    CK(c->tiles.alloc(t.size()));
+    CK(cudaMemcpy(c->tiles.p, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  } else {
+    // the staged kernel: column tiles of (ST_TX - 1) x (TY - 1) cells (TY of the family's closure),
+    // each block's height cut into equal chunks of at most ST_KZ planes; the longest chunks first
+    c->staged = true;
+    for (int p = 0; p < c->P.nfam; ++p) {
+      FamHost& H = c->fam[p];
+      t.clear();
+      for (int b = 0; b < c->nb; ++b) {
+        int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
+        int sx = ni >= 2 ? ST_TX - 1 : 1, sy = nj >= 2 ? st_ty(H.closure) - 1 : 1;
+        int nch = (nk + ST_KZ - 1) / ST_KZ, base = nk / nch, extra = nk % nch;
+        for (int ch = 0, k = 0; ch < nch; ++ch) {
+          int h = base + (ch < extra ? 1 : 0);
+          for (int j = 0; j < nj; j += sy)
+            for (int i = 0; i < ni; i += sx) t.push_back(Tile{b, i, j, k, h});
+          k += h;
+        }
+      }
+      std::stable_sort(t.begin(), t.end(), [](const Tile& x, const Tile& y) { return x.nkz > y.nkz; });
+      H.ntile3 = (int)t.size();
+      CK(H.tiles3.alloc(t.size()));
+      CK(cudaMemcpy(H.tiles3.p, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    }
   }
-  c->ntile = (int)t.size();
-  CK(c->tiles.alloc(t.size()));
-  CK(cudaMemcpy(c->tiles.p, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
   // norm chunks: 2048 cells of one block each
   std::vector<NormChunk> ch;
   c->chunk_block.clear();
@@ -293,6 +347,52 @@ static int build_tiles(ice_gpu_ctx* c) {
   CK(c->chunks.alloc(ch.size()));
   CK(cudaMemcpy(c->chunks.p, ch.data(), ch.size() * sizeof(NormChunk), cudaMemcpyHostToDevice));
   CK(c->npart.alloc((size_t)c->nchunk * 5));
+  return 0;
+}
+
+// The staged stage kernel's TMA maps: per family, state buffer and block, a 4-D view (x, y, z,
+// variable) of the block's ghost-cell pool, strides row px, plane pxy and variable NG (all multiples
+// of 16 bytes by the padding of the layout), box ST_BX x ST_BY x 1 x nc.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)f;
+  }
+  return fn;
+}
+
+static int build_maps(ice_gpu_ctx* c) {
+  if (!c->staged) return 0;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return fail(c, ICE_GPU_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  std::vector<CUtensorMap> h(c->nb);
+  for (int p = 0; p < c->P.nfam; ++p) {
+    FamHost& H = c->fam[p];
+    for (int buf = 0; buf < 3; ++buf) {
+      for (int b = 0; b < c->nb; ++b) {
+        const DBlock& B = c->hblk[b];
+        cuuint64_t dims[4] = {(cuuint64_t)B.px, (cuuint64_t)(B.nj + 4), (cuuint64_t)(B.nk + 4), (cuuint64_t)H.nc};
+        cuuint64_t strides[3] = {(cuuint64_t)B.px * 8, (cuuint64_t)B.pxy * 8, (cuuint64_t)c->NG * 8};
+        cuuint32_t box[4] = {(cuuint32_t)ST_BX, (cuuint32_t)(st_ty(H.closure) + 3), 1, (cuuint32_t)H.nc};
+        cuuint32_t es[4] = {1, 1, 1, 1};
+        CUresult r = enc(&h[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)(H.S[buf].p + B.goff), dims, strides, box,
+                         es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(c, ICE_GPU_ECUDA, "cuTensorMapEncodeTiled: error %d (family %d, block %d)",
+                                           (int)r, p + 1, b + 1);
+      }
+      CK(H.maps[buf].alloc(c->nb));
+      CK(cudaMemcpy(H.maps[buf].p, h.data(), c->nb * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    }
+  }
   return 0;
 }
 
@@ -325,9 +425,11 @@ int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims
     int ni = dims[3 * b], nj = dims[3 * b + 1], nk = dims[3 * b + 2];
     if (ni < 1 || nj < 1 || nk < 1) return fail(nullptr, ICE_GPU_EINVAL, "block %d: dims %d %d %d", b + 1, ni, nj, nk);
     DBlock B;
-    B.ni = ni; B.nj = nj; B.nk = nk; B.pad = 0;
+    B.ni = ni; B.nj = nj; B.nk = nk;
+    B.px = (ni + 4 + 1) & ~1;
+    B.pxy = (long long)B.px * (nj + 4);
     B.goff = G; B.ioff = I; B.roff = R; B.foff[0] = F0; B.foff[1] = F1; B.foff[2] = F2;
-    G += (long long)(ni + 4) * (nj + 4) * (nk + 4);
+    G += B.pxy * (nk + 4);
     c->ng_max = std::max(c->ng_max, (long long)(ni + 4) * (nj + 4) * (nk + 4));
     I += (long long)ni * nj * nk;
     R += (long long)(ni + 2) * (nj + 2) * (nk + 2);
@@ -371,6 +473,7 @@ int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims
   CKC(cudaEventCreate(&c->ev0)); CKC(cudaEventCreate(&c->ev1));
 #undef CKC
   if (build_tiles(c)) { g_create_err = c->err; return ICE_GPU_ECUDA; }
+  if (build_maps(c)) { g_create_err = c->err; return ICE_GPU_ECUDA; }
   *out = u.release();
   return 0;
 }
@@ -459,9 +562,16 @@ int ice_gpu_upload_state(ice_gpu_ctx* c, int32_t b1, int32_t p1, const double* p
   if (!c->xfer.p) CK(c->xfer.alloc((size_t)c->ng_max * kMaxNC));
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpyAsync(c->xfer.p, prim, (size_t)ng * H.nc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  k_aos2soa<<<grid_of(ng), 256, 0, c->stream>>>(c->xfer.p, H.S[c->phase].p + B.goff, c->NG, ng, H.nc);
+  k_aos2soa<<<grid_of(ng), 256, 0, c->stream>>>(c->xfer.p, H.S[c->phase].p + B.goff, c->NG, ng, H.nc,
+                                                 B.ni + 4, B.nj + 4, B.px);
   CK(cudaGetLastError());
-  if (inj) CK(cudaMemcpyAsync(H.inj.p + B.goff, inj, ng, cudaMemcpyHostToDevice, c->stream));
+  if (inj) {
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpyAsync(c->xfer.p, inj, ng, cudaMemcpyHostToDevice, c->stream));
+    k_inj2pool<<<grid_of(ng), 256, 0, c->stream>>>((const unsigned char*)c->xfer.p, H.inj.p + B.goff, ng,
+                                                   B.ni + 4, B.nj + 4, B.px);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->prev_phase = -1;
   return 0;
@@ -475,7 +585,8 @@ int ice_gpu_download_state(ice_gpu_ctx* c, int32_t b1, int32_t p1, double* prim)
   long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
   if (!prim) return fail(c, ICE_GPU_EINVAL, "download_state: null prim");
   if (!c->xfer.p) CK(c->xfer.alloc((size_t)c->ng_max * kMaxNC));
-  k_soa2aos<<<grid_of(ng), 256, 0, c->stream>>>(H.S[c->phase].p + B.goff, c->xfer.p, c->NG, ng, H.nc);
+  k_soa2aos<<<grid_of(ng), 256, 0, c->stream>>>(H.S[c->phase].p + B.goff, c->xfer.p, c->NG, ng, H.nc,
+                                                 B.ni + 4, B.nj + 4, B.px);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(prim, c->xfer.p, (size_t)ng * H.nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

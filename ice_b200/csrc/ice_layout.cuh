@@ -1,6 +1,7 @@
 // ice_layout.cuh -- the device layout of the solve stage: blocks, geometry, records, status,
 // the per-family view the kernels read, and the launch interface of the per-closure units.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "ice_physics.cuh"
 
@@ -9,7 +10,10 @@ namespace ice {
 
 // ------------------------------------------------------------------ device layout
 struct DBlock {
-  int ni, nj, nk, pad;
+  int ni, nj, nk;
+  int px;             // row pitch of the ghost-cell pools: ni + 4 rounded up to even, so that every row,
+                      // plane and block starts on a 16-byte boundary (the TMA tensor maps need it)
+  long long pxy;      // plane pitch, px * (nj + 4)
   long long goff;     // ghost-cell pools (1-gc:n+gc)^3
   long long ioff;     // interior pools
   long long roff;     // ring pools (0:n+1)^3
@@ -51,7 +55,7 @@ struct Status {
 };
 
 __device__ __forceinline__ long long gidx(const DBlock& B, int i, int j, int k) {
-  return B.goff + ((long long)(k + 2) * (B.nj + 4) + (j + 2)) * (B.ni + 4) + (i + 2);
+  return B.goff + (long long)(k + 2) * B.pxy + (long long)(j + 2) * B.px + (i + 2);
 }
 __device__ __forceinline__ long long iidx(const DBlock& B, int i, int j, int k) {
   return B.ioff + ((long long)k * B.nj + j) * B.ni + i;
@@ -66,7 +70,7 @@ __device__ __forceinline__ long long fidx(const DBlock& B, int d, int i, int j, 
   return B.foff[2] + ((long long)F * B.nj + j) * B.ni + i;
 }
 __device__ __forceinline__ long long gstride(const DBlock& B, int d) {
-  return d == 0 ? 1LL : d == 1 ? (long long)(B.ni + 4) : (long long)(B.ni + 4) * (B.nj + 4);
+  return d == 0 ? 1LL : d == 1 ? (long long)B.px : B.pxy;
 }
 
 struct FamDev {              // what the kernels of one family read
@@ -93,7 +97,7 @@ struct FamDev {              // what the kernels of one family read
   int write_tau;
 };
 
-struct Tile { int b, i0, j0, k0; };
+struct Tile { int b, i0, j0, k0, nkz; };   // a column tile of a block and its chunk of nkz planes
 struct NormChunk { int b; long long q0, q1; };
 
 // Everything one family's stage needs, for the launcher of its closure's translation unit.
@@ -103,7 +107,9 @@ struct LaunchArgs {
   const DRec* recs; int nrec;
   const int* own; int nown;
   const int* bfirst; const int* blist; int nbc;
-  const Tile* tiles; int ntile; int TX, TY, KZ;
+  const Tile* tiles; int ntile; int TX, TY, KZ;     // the 1-D stage kernel's tiles
+  const Tile* tiles3; int ntile3;                    // the staged stage kernel's tiles (2-D and 3-D runs)
+  const CUtensorMap* maps;                           // per block: the TMA map of U_{k-1} (the stencil buffer)
   int ndir, sd, irs, precision;
   double irs_beta;
   double* resid; double* resid2; double* resid3;

@@ -123,11 +123,17 @@ template <int CL, typename R> __device__ __forceinline__ void prim2cons(const R*
   }
 }
 
-// cons -> prim with the reference's floors (Lib_Model_*: cons_2_prim_*)
-template <int CL> __device__ __forceinline__ void cons2prim(const double* c, double* p, double cp) {
+// cons -> prim with the reference's floors (Lib_Model_*: cons_2_prim_*). FAST (the FP32-flux form):
+// the velocities multiply by one reciprocal of the density instead of three divisions.
+template <int CL, bool FAST = false> __device__ __forceinline__ void cons2prim(const double* c, double* p, double cp) {
   const double eps = epsv<double>();
   p[0] = c[0];
-  p[1] = c[1] / (p[0] + eps); p[2] = c[2] / (p[0] + eps); p[3] = c[3] / (p[0] + eps);
+  if constexpr (FAST) {
+    const double inv = 1.0 / (p[0] + eps);
+    p[1] = c[1] * inv; p[2] = c[2] * inv; p[3] = c[3] * inv;
+  } else {
+    p[1] = c[1] / (p[0] + eps); p[2] = c[2] / (p[0] + eps); p[3] = c[3] / (p[0] + eps);
+  }
   double n2 = p[1]*p[1] + p[2]*p[2] + p[3]*p[3];
   if constexpr (CL == MK) {
     p[4] = (c[4] - 0.5*p[0]*n2) / (cp*p[0] + eps);
@@ -286,7 +292,30 @@ template <typename R> __device__ __forceinline__ R slope_ratio(R y, R x) {
   return ru;
 }
 
+// Single-precision reciprocal by the hardware approximation (relative error about 2^-23): the
+// FP32-flux form's divisions by lengths and by the limiter's harmonic sum.
+__device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
+
+// The FP32-flux form's van Leer and minmod: the same limited slope phi(r) x, r = y / x, written
+// without the ratio. Van Leer: for x, y of one sign phi x = 2xy / (x + y), capped as the reference
+// caps phi by cx and cy r, i.e. |.| <= cx |x| and <= cy |y|; zero otherwise. Minmod: the smaller of
+// x and y in magnitude when they share a sign, else zero. One reciprocal (van Leer) or none
+// (minmod) in place of two divisions, and no product x y that could overflow single precision.
+__device__ __forceinline__ float vanleer_f(float x, float y, float cx, float cy) {
+  const float a = fabsf(x), b = fabsf(y);
+  if (!((x > 0.f && y > 0.f) || (x < 0.f && y < 0.f))) return 0.f;
+  float h = 2.f * a * (b * rcp_fast(a + b));
+  h = fminf(h, fminf(cx * a, cy * b));
+  return x > 0.f ? h : -h;
+}
+__device__ __forceinline__ float minmod_f(float x, float y) {
+  if (!((x > 0.f && y > 0.f) || (x < 0.f && y < 0.f))) return 0.f;
+  return fabsf(x) < fabsf(y) ? x : y;
+}
+
 template <int LIM, typename R> __device__ __forceinline__ R limiter(int lim, R x, R y, R cx, R cy) {
+  if constexpr (sizeof(R) == 4 && LIM == ICE_LIM_VANLEER) return vanleer_f(x, y, cx, cy);
+  if constexpr (sizeof(R) == 4 && LIM == ICE_LIM_MINMOD) return minmod_f(x, y);
   if constexpr (LIM == ICE_LIM_VANLEER) {
     R ru = slope_ratio(y, x);
     R phi = (ru + fabs(ru)) / ((R)1 + fabs(ru));
@@ -339,6 +368,9 @@ __device__ __forceinline__ bool reconstruct(int lim, const Q& q, R dl0, R dl1, R
     for (int v = 0; v < nc; ++v) pr[v] = q(2, v);
   }
   bool st_l = first_l, st_r = first_r;
+  // FP32-flux form: the three lengths' reciprocals once per face in place of a division per variable
+  R i0 = (R)1, i1 = (R)1, i2 = (R)1;
+  if constexpr (sizeof(R) == 4) { i0 = rcp_fast(dl0); i1 = rcp_fast(dl1); i2 = rcp_fast(dl2); }
   // the weight halves each pass: from any weight <= 1 it is below 1e-18 within 61 passes; the
   // cap only guards a non-finite weight, for which the reference would not end
   for (int pass = 0; (!st_l || !st_r) && pass < 256; ++pass) {
@@ -346,14 +378,14 @@ __device__ __forceinline__ bool reconstruct(int lim, const Q& q, R dl0, R dl1, R
 #pragma unroll
     for (int v = 0; v < nc; ++v) {
       R a1 = q(1, v), a2 = q(2, v);
-      R slope1 = (a2 - a1) / dl1;
+      R slope1 = sizeof(R) == 4 ? (a2 - a1) * i1 : (a2 - a1) / dl1;
       if (!first_l) {
-        R slope0 = (a1 - q(0, v)) / dl0;
+        R slope0 = sizeof(R) == 4 ? (a1 - q(0, v)) * i0 : (a1 - q(0, v)) / dl0;
         R sl = limiter<LIM>(lim, slope1, slope0, cxl, cyl) * limval;
         pl[v] = a1 + sl*dll;
       }
       if (!first_r) {
-        R slope2 = (q(3, v) - a2) / dl2;
+        R slope2 = sizeof(R) == 4 ? (q(3, v) - a2) * i2 : (q(3, v) - a2) / dl2;
         R sr = limiter<LIM>(lim, slope2, slope1, cxr, cyr) * limval;
         pr[v] = a2 - sr*dlr;
       }

@@ -3,19 +3,33 @@
 // specialised, every other limiter through the run-time switch).
 #pragma once
 #include "ice_kernels.cuh"
+#include "ice_stage3.cuh"
 
 namespace ice {
 
+// 2-D and 3-D runs: the staged kernel (ice_stage3.cuh); 1-D runs: the plane kernel of ice_kernels.cuh
+// (one tile of 256 cells per CTA) with the source in its own kernel before it.
 template <int CL, int RS, int LIM, typename R>
 void launch_stage_k(const LaunchArgs& a, bool write_r) {
   constexpr int nc = NC<CL>::v;
+  if (a.ntile3 > 0) {
+    constexpr size_t sh = StageSmem<CL, R>::bytes;
+    static bool attr3 = false;
+    if (!attr3) {
+      cudaFuncSetAttribute(k_stage3<CL, RS, LIM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+      attr3 = true;
+    }
+    k_stage3<CL, RS, LIM, R><<<a.ntile3, Shape<CL>::NT, sh, a.s>>>(a.G, a.F, a.maps, a.tiles3, write_r ? 1 : 0, a.st);
+    return;
+  }
   const size_t sh = sizeof(double) * 4 * nc * (size_t)a.TX * a.TY;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_stage<CL, RS, LIM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaFuncSetAttribute(k_stage<CL, RS, LIM_ANY, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 98304);
     attr = true;
   }
-  k_stage<CL, RS, LIM, R><<<a.ntile, a.TX * a.TY, sh, a.s>>>(a.G, a.F, a.tiles, a.TX, a.TY, a.KZ, write_r ? 1 : 0, a.st);
+  k_stage<CL, RS, LIM_ANY, R><<<a.ntile, a.TX * a.TY, sh, a.s>>>(a.G, a.F, a.tiles, a.TX, a.TY, a.KZ,
+                                                                 write_r ? 1 : 0, a.st);
 }
 
 template <int CL, int RS, typename R>

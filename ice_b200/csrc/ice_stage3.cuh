@@ -1,0 +1,450 @@
+// ice_stage3.cuh -- the stage kernel of 2-D and 3-D runs: the state planes staged in shared memory
+// by TMA, a z-march over a column tile, every face flux of the tile computed once, the residual
+// gathered per cell in the reference's order, the cell source, R = (R/vol + S) dt and the RK stage
+// fused in one launch per family and stage.
+//
+// One CTA of ST_TX x ST_TY threads owns a tile of (ST_TX - 1) x (ST_TY - 1) cells of one block and
+// marches up a chunk of planes. Each plane of the family's state U_{k-1} (every variable, two halo
+// cells below and one above the tile in x and y) arrives by one 4-D TMA load (x, y, z, variable) into
+// an FP64 staging buffer, issued one plane ahead; the CTA converts it into a ring of three planes of
+// the reconstruction type R (float in the FP32-flux form, double in the plain form). On each plane:
+//  - z: the limited slope of the cell above (the slope the reference's state_reconstruction computes
+//    for both faces of a cell, Lib_Reconstruction.f90:17-78) from planes k, k+1, k+2, kept in
+//    registers, and the z face above the cell from the two cells' slopes: the same operations on the
+//    same operands as the reference's per-face reconstruction, so the plain form keeps its bits;
+//  - x and y: the face below the thread's cell, reconstructed from the staged plane (face_flux,
+//    Mod_Fluxes.f90:599-685);
+//  - each owned cell adds its boundary-record fluxes, then its two faces per direction in the
+//    odd-then-even order of tile_sweep (Mod_Fluxes.f90:470-506), evaluates its source
+//    (Mod_Sources.f90:465-622), forms R = (R/vol + S) dt (Lib_Residual.f90:147-156) and applies the
+//    RK stage in conservative variables with the reference's floors (Lib_Newstate.f90:198-219).
+#pragma once
+#include "ice_kernels.cuh"
+#include "ice_tma.cuh"
+
+namespace ice {
+
+// The tile of a closure: ST_TX x TY threads, (ST_TX - 1) x (TY - 1) owned cells. AG's twelve
+// variables take 12 rows, so that two CTAs fit an SM with 168 registers per thread; MK and IG take 15.
+constexpr int ST_TX = 16;
+constexpr int ST_BX = ST_TX + 4;                // staged columns: 2 below, 1 above, 1 for the even x start
+constexpr int ST_KZ = 32;                       // planes per tile chunk at most
+__host__ __device__ constexpr int st_ty(int closure) { return closure == ICE_CLOSURE_AG ? 12 : 15; }
+
+template <int CL> struct Shape {
+  static constexpr int TY = st_ty(CL);
+  static constexpr int NT = ST_TX * TY;         // threads
+  static constexpr int BY = TY + 3;             // staged rows: 2 below, 1 above
+  static constexpr int P = ST_BX * BY;          // positions of one variable of one staged plane
+};
+
+__host__ __device__ constexpr size_t st_align(size_t n) { return (n + 127) & ~(size_t)127; }
+
+template <int CL, typename R> struct StageSmem {
+  static constexpr int nc = NC<CL>::v, P = Shape<CL>::P, NT = Shape<CL>::NT;
+  static constexpr size_t stg = 0;                                          // double [nc][P]
+  static constexpr size_t ring = st_align(stg + sizeof(double) * nc * P);  // R [3][nc][P]
+  static constexpr size_t fx = st_align(ring + sizeof(R) * 3 * nc * P);    // R [nc][NT]
+  static constexpr size_t fy = st_align(fx + sizeof(R) * nc * NT);         // R [nc][NT]
+  static constexpr size_t bar = st_align(fy + sizeof(R) * nc * NT);        // mbarrier
+  static constexpr size_t bytes = bar + 16 + 128;   // + the alignment of the base to 128 bytes
+};
+
+// The limited slope of cell c along one direction, before the face's limval: q(s, v) reads the cells
+// c-1, c, c+1 (s = 0, 1, 2); lm, l0, lp are their lengths after the injection rule. It is the `sl`
+// that state_reconstruction computes for the left state of the face above c and the `sr` it
+// computes for the right state of the face below c (the two are the same expression). `first` is
+// the first-order test of either side (density at or below rho_empty in one of the three cells).
+template <int CL, int LIM, typename R, typename Q>
+__device__ __forceinline__ void cell_slope(int lim, const Q& q, R lm, R l0, R lp, R* s, R& dlc, bool& first) {
+  constexpr int nc = NC<CL>::v;
+  const R dlb = (R)0.5*(lm + l0), dlf = (R)0.5*(l0 + lp);
+  dlc = (R)0.5*l0;
+  R cx, cy;
+  if (dlc > (R)0) { cx = dlf/dlc; cy = dlb/dlc; } else { cx = (R)2; cy = (R)2; }
+  const R re = (R)kRhoEmpty;
+  first = q(0, 0) <= re || q(1, 0) <= re || q(2, 0) <= re;
+  R ib = (R)1, iff = (R)1;        // FP32-flux form: reciprocals of the two lengths once per cell
+  if constexpr (sizeof(R) == 4) { ib = rcp_fast(dlb); iff = rcp_fast(dlf); }
+#pragma unroll
+  for (int v = 0; v < nc; ++v) {
+    const R a = q(1, v);
+    const R sf = sizeof(R) == 4 ? (q(2, v) - a) * iff : (q(2, v) - a) / dlf;
+    const R sb = sizeof(R) == 4 ? (a - q(0, v)) * ib : (a - q(0, v)) / dlb;
+    s[v] = first ? (R)0 : limiter<LIM>(lim, sf, sb, cx, cy);
+  }
+}
+
+// The two states of a face from its cells' limited slopes, with state_reconstruction's fallback:
+// the weight halves until both states are physical, and the first-order states are taken below
+// 1e-18 (Lib_Reconstruction.f90:40-76). Returns true when the first-order states are unphysical.
+template <int CL, typename R, typename QL, typename QR>
+__device__ __forceinline__ bool states_from_slopes(const QL& ql, const R* sl, R dll, bool fl,
+                                                   const QR& qr, const R* sr, R dlr, bool fr, R beta,
+                                                   R* pl, R* pr) {
+  constexpr int nc = NC<CL>::v;
+  R limval = beta;
+#pragma unroll
+  for (int v = 0; v < nc; ++v) { pl[v] = ql[v]; pr[v] = qr[v]; }
+  bool st_l = fl, st_r = fr;
+  for (int pass = 0; (!st_l || !st_r) && pass < 256; ++pass) {
+    if (pass == 255) limval = (R)0;
+#pragma unroll
+    for (int v = 0; v < nc; ++v) {
+      if (!fl) pl[v] = ql[v] + (sl[v]*limval)*dll;
+      if (!fr) pr[v] = qr[v] - (sr[v]*limval)*dlr;
+    }
+    if (!fl) st_l = check_prim<CL>(pl);
+    if (!fr) st_r = check_prim<CL>(pr);
+    limval = (R)0.5*limval;
+    if (limval < (R)1e-18 && !(st_l && st_r)) {
+#pragma unroll
+      for (int v = 0; v < nc; ++v) { pl[v] = ql[v]; pr[v] = qr[v]; }
+      if (!(check_prim<CL>(pl) && check_prim<CL>(pr))) return true;
+      break;
+    }
+  }
+  return false;
+}
+
+template <typename S, int NP> struct SmemStencil {     // q(s, v): stencil cell s of a staged plane
+  const S* P; int base, st;
+  __device__ __forceinline__ S operator()(int s, int v) const { return P[v * NP + base + s * st]; }
+};
+
+template <typename S, int NP> struct SmemCell {        // c[v]: one cell of a staged plane
+  const S* P; int pos;
+  __device__ __forceinline__ S operator[](int v) const { return P[v * NP + pos]; }
+};
+
+// One interior face along d (0: x, 1: y) between the 0-based cells (i,j,k) and its upper neighbour,
+// its four-cell stencil from a staged plane (base = the position of cell c - 1): face_flux +
+// compute_flux_ (Mod_Fluxes.f90:599-685).
+template <int CL, int RS, int LIM, typename R>
+__device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, const DBlock& B, int d,
+                                                 int i, int j, int k, const R* P, int base, int st, R* flux) {
+  constexpr int nc = NC<CL>::v;
+  const int c = d == 0 ? i : j;
+  const int n = d == 0 ? B.ni : B.nj;
+  const int o0 = d == 0, o1 = d == 1;
+  R bf = (R)1;
+  if (F.beta) bf = (R)mn(F.beta[iidx(B, i, j, k)], F.beta[iidx(B, i + o0, j + o1, k)]);
+  const double* dl = G.dl + (long long)d * G.NR;
+  const long long r0 = ridx(B, i, j, k);
+  const long long rs = d == 0 ? 1LL : (long long)(B.ni + 2);
+  R l0 = (R)dl[r0 - rs], l1 = (R)dl[r0], l2 = (R)dl[r0 + rs], l3 = (R)dl[r0 + 2 * rs];
+  if (c == 0 || c == n - 2) {
+    const long long gs = gstride(B, d);
+    const long long g0 = gidx(B, i, j, k) - gs;
+    if (c == 0 && F.inj[g0]) l0 = (R)0;
+    if (c == n - 2 && F.inj[g0 + 3 * gs]) l3 = (R)0;
+  }
+  R dl0 = (R)0.5*(l0 + l1), dl1 = (R)0.5*(l1 + l2), dl2 = (R)0.5*(l2 + l3);
+  R dll = (R)0.5*l1, dlr = (R)0.5*l2;
+  R pl[nc], pr[nc], fl[nc];
+  SmemStencil<R, Shape<CL>::P> q{P, base, st};
+  const bool bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
+  const long long fi = fidx(B, d, i, j, k, c + 1);
+  const long long NF = G.NF[d];
+  const double* fc = G.face[d];
+  R nrm[3] = {(R)fc[fi], (R)fc[NF + fi], (R)fc[2 * NF + fi]};
+  R area = (R)fc[3 * NF + fi];
+  riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
+  return bad;
+}
+
+// The stage kernel (see the head of this file). write_r: store R instead of updating (IRS runs).
+template <int CL, int RS, int LIM, typename R>
+__global__ void __launch_bounds__(Shape<CL>::NT, (sizeof(R) == 4) ? 2 : 1)
+k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __restrict__ tiles, int write_r,
+         Status* st) {
+  constexpr int nc = NC<CL>::v;
+  constexpr int ST_TY = Shape<CL>::TY, ST_NT = Shape<CL>::NT, ST_P = Shape<CL>::P;
+  using L = StageSmem<CL, R>;
+  extern __shared__ __align__(128) unsigned char smdyn[];
+  // the TMA destination must sit on a 128-byte boundary: align the base explicitly
+  unsigned char* smraw = smdyn + ((128u - (smem_u32(smdyn) & 127u)) & 127u);
+  double* stg = (double*)(smraw + L::stg);
+  R* ring = (R*)(smraw + L::ring);
+  R* Fx = (R*)(smraw + L::fx);
+  R* Fy = (R*)(smraw + L::fy);
+  uint64_t* bar = (uint64_t*)(smraw + L::bar);
+
+  const Tile t = tiles[blockIdx.x];
+  const DBlock B = G.blk[t.b];
+  const CUtensorMap* map = maps + t.b;
+  const int tid = threadIdx.x;
+  const int tx = tid % ST_TX, ty = tid / ST_TX;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool ax = B.ni >= 2, ay = B.nj >= 2, az = B.nk >= 2;
+  const bool col = i < B.ni && j < B.nj;
+  const bool owner = col && (ax ? tx < ST_TX - 1 : tx == 0) && (ay ? ty < ST_TY - 1 : ty == 0);
+  const int xa = t.i0 & ~1;                      // staged box start (ghost-inclusive x of cell i0 - 2, made even)
+  const int pos = (ty + 2) * ST_BX + (tx + 2 + (t.i0 - xa));
+  const int k0 = t.k0, k1 = t.k0 + t.nkz;
+  constexpr uint32_t kBoxBytes = (uint32_t)(sizeof(double) * nc * ST_P);
+
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    prefetch_tmap(map);
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  auto issue = [&](int kp) {                    // plane kp (cell index) into the staging buffer
+    if (tid == 0) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(bar, kBoxBytes);
+      tma_load_4d(stg, map, bar, xa, t.j0, kp + 2, 0);
+    }
+  };
+  // Waits for the staged plane and converts it into a ring slot. False, for every thread of the CTA,
+  // when a wait gave up: the threads that gave up wait once more (bounded) for the copy in flight,
+  // and the caller leaves the tile with the timeout bit set.
+  auto land = [&](int slot) -> bool {
+    const bool ok = mbar_wait(bar, parity);
+    if (__syncthreads_or(!ok)) {
+      if (!ok) mbar_wait(bar, parity);
+      return false;
+    }
+    parity ^= 1u;
+    R* dst = ring + slot * nc * ST_P;
+    for (int q = tid; q < nc * ST_P; q += ST_NT) dst[q] = (R)stg[q];
+    __syncthreads();
+    return true;
+  };
+  auto stall = [&]() { if (tid == 0) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_TIMEOUT); };
+  auto plane = [&](int slot) { return (const R*)(ring + slot * nc * ST_P); };
+
+  // z: slope of the thread's cell at plane c from three ring slots (c-1, c, c+1)
+  R sz[nc], flo[nc], fhi[nc];
+  R dlz = (R)0;
+  bool fz = true;
+  bool bad = false;
+  auto zslope = [&](int sm, int s0, int sp, int c, R* s, R& dlc, bool& first) {
+    const double* dl = G.dl + 2 * G.NR;
+    const long long r0 = ridx(B, i, j, c);
+    const long long rs = (long long)(B.ni + 2) * (B.nj + 2);
+    R lm = (R)dl[r0 - rs], l0 = (R)dl[r0], lp = (R)dl[r0 + rs];
+    const long long g = gidx(B, i, j, c);
+    if (c == 0 && F.inj[g - B.pxy]) lm = (R)0;
+    if (c == B.nk - 1 && F.inj[g + B.pxy]) lp = (R)0;
+    const R* Pm = plane(sm); const R* P0 = plane(s0); const R* Pp = plane(sp);
+    auto q = [&](int s, int v) { return (s == 0 ? Pm : s == 1 ? P0 : Pp)[v * ST_P + pos]; };
+    cell_slope<CL, LIM, R>(F.limiter, q, lm, l0, lp, s, dlc, first);
+  };
+  // z face between c and c + 1 from the ring slots of the two cells and their slopes
+  auto zface = [&](int sl, int sr, int c, const R* sa, R da, bool fa, const R* sb, R db, bool fb, R* out) {
+    R pl[nc], pr[nc];
+    const SmemCell<R, ST_P> ql{plane(sl), pos}, qr{plane(sr), pos};
+    R bf = (R)1;
+    if (F.beta) bf = (R)mn(F.beta[iidx(B, i, j, c)], F.beta[iidx(B, i, j, c + 1)]);
+    bad |= states_from_slopes<CL, R>(ql, sa, da, fa, qr, sb, db, fb, bf, pl, pr);
+    const long long fi = fidx(B, 2, i, j, c, c + 1);
+    const long long NF = G.NF[2];
+    const double* fc = G.face[2];
+    R nrm[3] = {(R)fc[fi], (R)fc[NF + fi], (R)fc[2 * NF + fi]};
+    R area = (R)fc[3 * NF + fi];
+    R fl[nc];
+    riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) out[v] = fl[v] * area;
+  };
+
+  // prologue: the ring holds planes k0, k0+1, k0+2; sz the slope at k0; flo the face below k0
+  // (z work is done for the owned cells only: no other thread reads a z face)
+  int cur, nx1, nx2;
+  if (!az) {
+    issue(k0);
+    if (!land(0)) { stall(); return; }
+    cur = 0; nx1 = 1; nx2 = 2;
+  } else if (k0 >= 1) {
+    issue(k0 - 2);
+    if (!land(0)) { stall(); return; }
+    issue(k0 - 1);
+    if (!land(1)) { stall(); return; }
+    issue(k0);
+    if (!land(2)) { stall(); return; }
+    R sm1[nc]; R dm1 = (R)0; bool fm1 = true;
+    if (owner) zslope(0, 1, 2, k0 - 1, sm1, dm1, fm1);
+    issue(k0 + 1);
+    __syncthreads();                            // slot 0 (plane k0-2) is read by every thread before reuse
+    if (!land(0)) { stall(); return; }
+    if (owner) {
+      zslope(1, 2, 0, k0, sz, dlz, fz);
+      zface(1, 2, k0 - 1, sm1, dm1, fm1, sz, dlz, fz, flo);
+    }
+    issue(k0 + 2);
+    __syncthreads();
+    if (!land(1)) { stall(); return; }
+    cur = 2; nx1 = 0; nx2 = 1;
+  } else {
+    issue(-1);
+    if (!land(0)) { stall(); return; }
+    issue(0);
+    if (!land(1)) { stall(); return; }
+    issue(1);
+    if (!land(2)) { stall(); return; }
+    if (owner) zslope(0, 1, 2, 0, sz, dlz, fz);
+    issue(2);
+    __syncthreads();
+    if (!land(0)) { stall(); return; }
+    cur = 1; nx1 = 2; nx2 = 0;
+  }
+
+  for (int k = k0; k < k1; ++k) {
+    const bool more = k + 1 < k1;
+    if (more) issue(k + 3);                     // lands at the end of this plane, into the slot of k
+    const R* P = plane(cur);
+    if (ax && col && i >= 1) {                  // x face below (i,j,k)
+      R fl[nc];
+      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 0, i - 1, j, k, P, pos - 2, 1, fl);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) Fx[v * ST_NT + tid] = fl[v];
+    }
+    if (ay && col && j >= 1) {                  // y face below (i,j,k)
+      R fl[nc];
+      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 1, i, j - 1, k, P, pos - 2 * ST_BX, ST_BX, fl);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) Fy[v * ST_NT + tid] = fl[v];
+    }
+    // z: the face above the cell, from the slopes at k (carried) and k + 1
+    R szn[nc]; R dlzn = (R)0; bool fzn = true;
+    if (az && owner && k <= B.nk - 2) {
+      zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
+      zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, fhi);
+    }
+    __syncthreads();
+    if (owner) {
+      const long long q = iidx(B, i, j, k);
+      const int bc = F.bmap[q];
+      // the cell's residual, summed in the reference's order: in FP64 in the plain form, in FP32
+      // (the type of the fluxes) in the FP32-flux form
+      using A = R;
+      A r[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) r[v] = bc >= 0 ? (A)F.Rb[(long long)bc * nc + v] : (A)0;
+      if (ax) {
+        const int ci = i + 1, n = B.ni;
+        if (ci % 2 == 1) {
+          if (ci < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fx[v * ST_NT + tid + 1];
+          }
+          if (ci > 1) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fx[v * ST_NT + tid];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fx[v * ST_NT + tid];
+          if (ci < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fx[v * ST_NT + tid + 1];
+          }
+        }
+      }
+      if (ay) {
+        const int cj = j + 1, n = B.nj;
+        if (cj % 2 == 1) {
+          if (cj < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fy[v * ST_NT + tid + ST_TX];
+          }
+          if (cj > 1) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fy[v * ST_NT + tid];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fy[v * ST_NT + tid];
+          if (cj < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fy[v * ST_NT + tid + ST_TX];
+          }
+        }
+      }
+      if (az) {
+        const int ck = k + 1, n = B.nk;
+        if (ck % 2 == 1) {
+          if (ck < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)fhi[v];
+          }
+          if (ck > 1) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)flo[v];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)flo[v];
+          if (ck < n) {
+#pragma unroll
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)fhi[v];
+          }
+        }
+      }
+      const long long g = gidx(B, i, j, k);
+      double p[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
+      double s[nc];
+#pragma unroll
+      for (int v = 0; v < nc; ++v) s[v] = 0.0;
+      if (F.coupled) {                          // compute_source_ on the stage's state
+        R pr_[nc], gas[5], sr[nc];
+#pragma unroll
+        for (int v = 0; v < nc; ++v) pr_[v] = (R)p[v];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) gas[v] = (R)G.gas[(long long)v * G.NI + q];
+        R tau = cell_source<CL, R>(pr_, gas, (R)G.gas[5 * G.NI + q], (R)G.gas[6 * G.NI + q], (R)G.gas[7 * G.NI + q],
+                                   (R)G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, sr);
+#pragma unroll
+        for (int v = 0; v < nc; ++v) s[v] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)sr[v];
+        if (F.write_tau) F.tau[q] = (double)tau;
+      }
+      const double dt = F.dt ? F.dt[q] : *F.dtg;
+      const double vol = G.vol[q];
+      double rd[nc];
+      if constexpr (sizeof(R) == 8) {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) rd[v] = (r[v]/vol + s[v]) * dt;
+      } else {
+        const double ivol = 1.0 / vol;
+#pragma unroll
+        for (int v = 0; v < nc; ++v) rd[v] = ((double)r[v]*ivol + s[v]) * dt;
+      }
+#pragma unroll
+      for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) rd[v] = 0.0;
+      if (write_r) {
+#pragma unroll
+        for (int v = 0; v < nc; ++v) F.resid[(long long)v * G.NI + q] = rd[v];
+      } else {
+        double po[nc], co[nc], cn[nc];
+#pragma unroll
+        for (int v = 0; v < nc; ++v) po[v] = F.U0[(long long)v * G.NG + g];
+        prim2cons<CL, double>(po, co, F.mat.cp);
+        prim2cons<CL, double>(p, cn, F.mat.cp);
+#pragma unroll
+        for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + rd[v]) * F.rk; cn[v] = co[v] + rr; }
+        if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
+        cons2prim<CL, sizeof(R) == 4>(cn, p, F.mat.cp);
+        if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
+#pragma unroll
+        for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];
+      }
+    }
+    if (!more) break;
+    __syncthreads();                            // every read of Fx and Fy is done
+    if (!land(cur)) { stall(); break; }         // plane k + 3 replaces plane k (read by nobody since)
+    const int o = cur; cur = nx1; nx1 = nx2; nx2 = o;
+#pragma unroll
+    for (int v = 0; v < nc; ++v) { flo[v] = fhi[v]; sz[v] = szn[v]; }
+    dlz = dlzn; fz = fzn;
+  }
+  if (bad) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
+}
+
+}  // namespace ice
