@@ -194,6 +194,26 @@ int ice_gpu_step(ice_gpu_ctx* ctx, int32_t nsteps, ice_gpu_step_out* out);
  * replaces: residual_norm (diagnostic/Mod_Diagnostic.f90:22-83). */
 int ice_gpu_residual_norm(ice_gpu_ctx* ctx, double* total, double* fam);
 
+/* The residual-norm sums of one block of one family for a caller that cannot allocate device
+ * memory: a driver whose device memory all belongs to the host application's own allocator (a
+ * coupler inside a gas solver with a fixed device-memory budget, a Fortran/OpenACC runtime that
+ * owns the state arrays) and so may create no solve context, whose set-up allocates. No counterpart
+ * in the reference: it is the per-block part of residual_norm without a context.
+ * prim_new, prim_old: DEVICE arrays of the block in the driver's layout prim(nc, 1-gc:ni+gc,
+ * 1-gc:nj+gc, 1-gc:nk+gc), gc = 2; t_slot the 1-based temperature slot (nbase - 1); dims ni nj nk.
+ * sums[5] (host): the sums over interior cells of (new - old)^2 of rho, u, v, w, T; the residual
+ * norm is the square root of their sum over blocks and families (the same bits as
+ * ice_gpu_residual_norm for the same states). stream: a cudaStream_t, or NULL.
+ * It allocates nothing: its scratch is a static device array of 4096 x 5 partial sums (plus 5),
+ * which every GPU that loads the library holds until exit; a block of more than 8,388,608 cells is
+ * refused with ICE_GPU_EINVAL. The first call on a device looks the array up on that device (make
+ * it before any stream capture). Every call overwrites all the scratch it reads, so nothing carries
+ * over between calls; two calls that overlap on the GPU (other streams) share the array and race.
+ * Errors: a message in err[errlen]. */
+int ice_gpu_residual_sq_noalloc(const double* prim_new, const double* prim_old, int32_t nc,
+                                int32_t t_slot, const int32_t* dims, double* sums, void* stream,
+                                char* err, int32_t errlen);
+
 /* A runtime re-read of input.ini (Wrap_Postprocess.f90:255 -> Read_Ini.f90:61): the
  * numerics may change between steps; nfam, closures and ndir may not. */
 int ice_gpu_update_params(ice_gpu_ctx* ctx, const ice_gpu_params* params);
