@@ -13,6 +13,13 @@ template <int CL> inline void launch_stage_of(const LaunchArgs& a, bool write_r)
   else { if (f32) launch_stage_ag_f32(a, write_r); else launch_stage_ag_f64(a, write_r); }
 }
 
+template <int CL> inline void launch_bound_of(const LaunchArgs& a) {
+  const bool f32 = a.precision == ICE_PREC_FP32FLUX && !a.irs;
+  if constexpr (CL == MK) { if (f32) launch_bound_mk_f32(a); else launch_bound_mk_f64(a); }
+  else if constexpr (CL == IG) { if (f32) launch_bound_ig_f32(a); else launch_bound_ig_f64(a); }
+  else { if (f32) launch_bound_ag_f32(a); else launch_bound_ag_f64(a); }
+}
+
 template <int CL> inline void launch_source_of(const LaunchArgs& a) {
   const bool f32 = a.precision == ICE_PREC_FP32FLUX;
   if constexpr (CL == MK) { if (f32) launch_source_mk_f32(a); else launch_source_mk_f64(a); }
@@ -31,17 +38,17 @@ void launch_family_t(const LaunchArgs& a) {
     tick(KC_SOURCE);
   }
   if (a.nrec > 0) {
-    k_ghost1<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
-    k_ghost2<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
+    k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
     tick(KC_GHOST);
   }
   if (a.sd) {
     k_beta<<<grid(a.G.NI, 256), 256, 0, s>>>(a.G, a.F);
     tick(KC_BETA);
   }
-  if (a.nown > 0) k_conn<CL, RS><<<grid(a.nown, 64), 64, 0, s>>>(a.G, a.F, a.recs, a.own, a.nown, a.st);
-  if (a.nbc > 0) k_bound<CL, RS><<<grid(a.nbc, 64), 64, 0, s>>>(a.G, a.F, a.recs, a.bfirst, a.blist, a.nbc, a.st);
-  if (a.nown > 0 || a.nbc > 0) tick(KC_BOUND);
+  if (a.nown > 0 || a.nbc > 0) {
+    launch_bound_of<CL>(a);
+    tick(KC_BOUND);
+  }
   if (!a.irs) {
     launch_stage_of<CL>(a, false);
     tick(KC_STAGE);

@@ -71,8 +71,10 @@ __device__ __forceinline__ bool face_flux(const Geo& G, const FamDev& F, const D
   return bad;
 }
 
-// record_flux (Mod_BC_Fluxes.f90:180-272): the flux through a record's face into its cell.
-template <int CL, int RS>
+// record_flux (Mod_BC_Fluxes.f90:180-272): the flux through a record's face into its cell. R is the
+// reconstruction and Riemann type (double in the plain form, float in the FP32-flux form); LIM the
+// limiter the kernel is specialised for (the same formulas as the run-time switch in double).
+template <int CL, int RS, int LIM, typename R>
 __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double* flux, const double* beta_face) {
   constexpr int nc = NC<CL>::v;
   const DBlock& B = G.blk[r.b];
@@ -82,43 +84,43 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
   int ig2 = i - 2 * g0, jg2 = j - 2 * g1, kg2 = k - 2 * g2;
   int ip = i + g0, jp = j + g1, kp = k + g2;
   int dir = (f + 1) / 2 - 1;
-  double bv = beta_face ? *beta_face : (F.beta ? F.beta[iidx(B, i, j, k)] : 1.0);
-  double dl_g1 = G.dl[(long long)dir * G.NR + ridx(B, ig, jg, kg)];
-  double dl_m = G.dl[(long long)dir * G.NR + ridx(B, i, j, k)];
-  double dl_4 = G.dl[(long long)dir * G.NR + ridx(B, ip, jp, kp)];
-  double dl0, dl1, dl2, dll, dlr;
-  double pl[nc], pr[nc], fl[nc];
+  R bv = (R)(beta_face ? *beta_face : (F.beta ? F.beta[iidx(B, i, j, k)] : 1.0));
+  R dl_g1 = (R)G.dl[(long long)dir * G.NR + ridx(B, ig, jg, kg)];
+  R dl_m = (R)G.dl[(long long)dir * G.NR + ridx(B, i, j, k)];
+  R dl_4 = (R)G.dl[(long long)dir * G.NR + ridx(B, ip, jp, kp)];
+  R dl0, dl1, dl2, dll, dlr;
+  R pl[nc], pr[nc], fl[nc];
   bool bad;
   const double* P = F.Up;
   long long NF = G.NF[dir];
   if (f % 2 == 1) {
     long long fi = fidx(B, dir, i, j, k, (dir == 0 ? i : dir == 1 ? j : k));   // the face below the cell
-    double nrm[3] = {G.face[dir][fi], G.face[dir][NF + fi], G.face[dir][2 * NF + fi]};
-    double area = G.face[dir][3 * NF + fi];
-    dl0 = dl_g1; dl1 = 0.5*(dl_g1 + dl_m); dl2 = 0.5*(dl_m + dl_4);
-    dll = 0.5*dl_g1; dlr = 0.5*dl_m;
-    if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = 0.5*dl_m; dll = 0.0; }
-    if (F.inj[gidx(B, ip, jp, kp)]) dl2 = 0.5*dl_m;
+    R nrm[3] = {(R)G.face[dir][fi], (R)G.face[dir][NF + fi], (R)G.face[dir][2 * NF + fi]};
+    R area = (R)G.face[dir][3 * NF + fi];
+    dl0 = dl_g1; dl1 = (R)0.5*(dl_g1 + dl_m); dl2 = (R)0.5*(dl_m + dl_4);
+    dll = (R)0.5*dl_g1; dlr = (R)0.5*dl_m;
+    if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = (R)0.5*dl_m; dll = (R)0; }
+    if (F.inj[gidx(B, ip, jp, kp)]) dl2 = (R)0.5*dl_m;
     long long a[4] = {gidx(B, ig2, jg2, kg2), gidx(B, ig, jg, kg), gidx(B, i, j, k), gidx(B, ip, jp, kp)};
-    auto q = [&](int s, int v) { return P[(long long)v * G.NG + a[s]]; };
-    bad = reconstruct<CL, LIM_ANY, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
-    riemann<CL, RS, double>(pl, pr, nrm, fl, F.mat.cp);
+    auto q = [&](int s, int v) { return (R)P[(long long)v * G.NG + a[s]]; };
+    bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
+    riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
-    for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
+    for (int v = 0; v < nc; ++v) flux[v] = (double)(fl[v] * area);
   } else {
     long long fi = fidx(B, dir, i, j, k, (dir == 0 ? i : dir == 1 ? j : k) + 1);  // the face above the cell
-    double nrm[3] = {G.face[dir][fi], G.face[dir][NF + fi], G.face[dir][2 * NF + fi]};
-    double area = G.face[dir][3 * NF + fi];
-    dl0 = 0.5*(dl_4 + dl_m); dl1 = 0.5*(dl_m + dl_g1); dl2 = dl_g1;
-    dll = 0.5*dl_m; dlr = 0.5*dl_g1;
-    if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = 0.5*dl_m; dlr = 0.0; }
-    if (F.inj[gidx(B, ip, jp, kp)]) dl0 = 0.5*dl_m;
+    R nrm[3] = {(R)G.face[dir][fi], (R)G.face[dir][NF + fi], (R)G.face[dir][2 * NF + fi]};
+    R area = (R)G.face[dir][3 * NF + fi];
+    dl0 = (R)0.5*(dl_4 + dl_m); dl1 = (R)0.5*(dl_m + dl_g1); dl2 = dl_g1;
+    dll = (R)0.5*dl_m; dlr = (R)0.5*dl_g1;
+    if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = (R)0.5*dl_m; dlr = (R)0; }
+    if (F.inj[gidx(B, ip, jp, kp)]) dl0 = (R)0.5*dl_m;
     long long a[4] = {gidx(B, ip, jp, kp), gidx(B, i, j, k), gidx(B, ig, jg, kg), gidx(B, ig2, jg2, kg2)};
-    auto q = [&](int s, int v) { return P[(long long)v * G.NG + a[s]]; };
-    bad = reconstruct<CL, LIM_ANY, double>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
-    riemann<CL, RS, double>(pl, pr, nrm, fl, F.mat.cp);
+    auto q = [&](int s, int v) { return (R)P[(long long)v * G.NG + a[s]]; };
+    bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
+    riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
-    for (int v = 0; v < nc; ++v) flux[v] = -(fl[v] * area);
+    for (int v = 0; v < nc; ++v) flux[v] = (double)(-(fl[v] * area));
   }
   return bad;
 }
@@ -213,11 +215,8 @@ __device__ __forceinline__ void rec_normal(const Geo& G, const DBlock& B, const 
 
 // ghost_record (Lib_Ghost.f90:76-267), every record type but 102
 template <int CL>
-__global__ void k_ghost1(Geo G, FamDev F, const DRec* recs, int nrec) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nrec) return;
+__device__ __forceinline__ void ghost1_rec(const Geo& G, const FamDev& F, const DRec& r) {
   constexpr int nc = NC<CL>::v;
-  const DRec r = recs[n];
   const DBlock& B = G.blk[r.b];
   int g0 = (r.f == 1) - (r.f == 2), g1 = (r.f == 3) - (r.f == 4), g2 = (r.f == 5) - (r.f == 6);
   long long gg = gidx(B, r.i - g0, r.j - g1, r.k - g2);
@@ -324,11 +323,8 @@ __global__ void k_ghost1(Geo G, FamDev F, const DRec* recs, int nrec) {
 
 // second_ghost_record (Lib_Ghost.f90:312-387)
 template <int CL>
-__global__ void k_ghost2(Geo G, FamDev F, const DRec* recs, int nrec) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nrec) return;
+__device__ __forceinline__ void ghost2_rec(const Geo& G, const FamDev& F, const DRec& r) {
   constexpr int nc = NC<CL>::v;
-  const DRec r = recs[n];
   if (r.type == 0) return;
   const DBlock& B = G.blk[r.b];
   int g0 = (r.f == 1) - (r.f == 2), g1 = (r.f == 3) - (r.f == 4), g2 = (r.f == 5) - (r.f == 6);
@@ -378,9 +374,22 @@ __global__ void k_ghost2(Geo G, FamDev F, const DRec* recs, int nrec) {
   }
 }
 
+// Both ghost layers of every record, one thread per record. compute_ghost fills layer 1 of every
+// record and then fill_second_ghost layer 2 (Lib_Ghost.f90:29-387); a record's layer 2 reads only its
+// own layer-1 cell and interior cells (of its block, or of the source block of a connection), never a
+// cell another record writes, so one thread can do both in turn with the same result.
+template <int CL>
+__global__ void k_ghost(Geo G, FamDev F, const DRec* recs, int nrec) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nrec) return;
+  const DRec r = recs[n];
+  ghost1_rec<CL>(G, F, r);
+  ghost2_rec<CL>(G, F, r);
+}
+
 // ------------------------------------------------------------------ boundary fluxes
-template <int CL, int RS>
-__global__ void k_conn(Geo G, FamDev F, const DRec* recs, const int* own, int nown, Status* st) {
+template <int CL, int RS, int LIM, typename R>
+__global__ void __launch_bounds__(128, 4) k_conn(Geo G, FamDev F, const DRec* recs, const int* own, int nown, Status* st) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nown) return;
   constexpr int nc = NC<CL>::v;
@@ -392,13 +401,14 @@ __global__ void k_conn(Geo G, FamDev F, const DRec* recs, const int* own, int no
   }
   double bf = mn(bo, bq);
   double fl[nc];
-  if (record_flux<CL, RS>(G, F, r, fl, &bf)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
+  if (record_flux<CL, RS, LIM, R>(G, F, r, fl, &bf)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
 #pragma unroll
   for (int v = 0; v < nc; ++v) F.connF[(long long)r.cf * nc + v] = fl[v];
 }
 
-template <int CL, int RS>
-__global__ void k_bound(Geo G, FamDev F, const DRec* recs, const int* first, const int* list, int nbc, Status* st) {
+template <int CL, int RS, int LIM, typename R>
+__global__ void __launch_bounds__(128, 4) k_bound(Geo G, FamDev F, const DRec* recs, const int* first, const int* list,
+                                                  int nbc, Status* st) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nbc) return;
   constexpr int nc = NC<CL>::v;
@@ -413,7 +423,7 @@ __global__ void k_bound(Geo G, FamDev F, const DRec* recs, const int* first, con
 #pragma unroll
       for (int v = 0; v < nc; ++v) { double x = F.connF[(long long)r.cf * nc + v]; fl[v] = r.owner ? x : -x; }
     } else {
-      if (record_flux<CL, RS>(G, F, r, fl, nullptr)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
+      if (record_flux<CL, RS, LIM, R>(G, F, r, fl, nullptr)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
     }
 #pragma unroll
     for (int v = 0; v < nc; ++v) acc[v] = acc[v] + fl[v];

@@ -132,6 +132,12 @@ void launch_source_ig_f64(const LaunchArgs& a);
 void launch_source_ig_f32(const LaunchArgs& a);
 void launch_source_ag_f64(const LaunchArgs& a);
 void launch_source_ag_f32(const LaunchArgs& a);
+void launch_bound_mk_f64(const LaunchArgs& a);
+void launch_bound_mk_f32(const LaunchArgs& a);
+void launch_bound_ig_f64(const LaunchArgs& a);
+void launch_bound_ig_f32(const LaunchArgs& a);
+void launch_bound_ag_f64(const LaunchArgs& a);
+void launch_bound_ag_f32(const LaunchArgs& a);
 void launch_stage_mk_f64(const LaunchArgs& a, bool write_r);
 void launch_stage_mk_f32(const LaunchArgs& a, bool write_r);
 void launch_stage_ig_f64(const LaunchArgs& a, bool write_r);

@@ -39,6 +39,31 @@ void launch_stage_l(const LaunchArgs& a, bool write_r) {
   else launch_stage_k<CL, RS, LIM_ANY, R>(a, write_r);
 }
 
+// connection-face fluxes by their owners, then every boundary cell's records in face order
+template <int CL, int RS, int LIM, typename R>
+void launch_bound_k(const LaunchArgs& a) {
+  auto grid = [](long long n, int t) { return (unsigned)((n + t - 1) / t); };
+  if (a.nown > 0) k_conn<CL, RS, LIM, R><<<grid(a.nown, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.own, a.nown, a.st);
+  if (a.nbc > 0)
+    k_bound<CL, RS, LIM, R><<<grid(a.nbc, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.bfirst, a.blist, a.nbc, a.st);
+}
+
+template <int CL, int RS, typename R>
+void launch_bound_l(const LaunchArgs& a) {
+  if (a.F.limiter == ICE_LIM_VANLEER) launch_bound_k<CL, RS, ICE_LIM_VANLEER, R>(a);
+  else if (a.F.limiter == ICE_LIM_MINMOD) launch_bound_k<CL, RS, ICE_LIM_MINMOD, R>(a);
+  else launch_bound_k<CL, RS, LIM_ANY, R>(a);
+}
+
+template <int CL, typename R>
+void launch_bound_t(const LaunchArgs& a) {
+  if constexpr (CL == MK) {
+    if (a.F.riemann == ICE_RIEMANN_SAUREL) { launch_bound_l<CL, ICE_RIEMANN_SAUREL, R>(a); return; }
+  }
+  if (a.F.riemann == ICE_RIEMANN_HLLE) launch_bound_l<CL, ICE_RIEMANN_HLLE, R>(a);
+  else launch_bound_l<CL, ICE_RIEMANN_RUSANOV, R>(a);
+}
+
 template <int CL, typename R>
 void launch_source_t(const LaunchArgs& a) {
   k_source<CL, R><<<(unsigned)((a.G.NI + 255) / 256), 256, 0, a.s>>>(a.G, a.F);

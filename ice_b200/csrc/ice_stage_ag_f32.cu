@@ -3,4 +3,5 @@
 namespace ice {
 void launch_stage_ag_f32(const LaunchArgs& a, bool write_r) { launch_stage_t<AG, float>(a, write_r); }
 void launch_source_ag_f32(const LaunchArgs& a) { launch_source_t<AG, float>(a); }
+void launch_bound_ag_f32(const LaunchArgs& a) { launch_bound_t<AG, float>(a); }
 }  // namespace ice

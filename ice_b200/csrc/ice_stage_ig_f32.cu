@@ -3,4 +3,5 @@
 namespace ice {
 void launch_stage_ig_f32(const LaunchArgs& a, bool write_r) { launch_stage_t<IG, float>(a, write_r); }
 void launch_source_ig_f32(const LaunchArgs& a) { launch_source_t<IG, float>(a); }
+void launch_bound_ig_f32(const LaunchArgs& a) { launch_bound_t<IG, float>(a); }
 }  // namespace ice

@@ -3,4 +3,5 @@
 namespace ice {
 void launch_stage_ig_f64(const LaunchArgs& a, bool write_r) { launch_stage_t<IG, double>(a, write_r); }
 void launch_source_ig_f64(const LaunchArgs& a) { launch_source_t<IG, double>(a); }
+void launch_bound_ig_f64(const LaunchArgs& a) { launch_bound_t<IG, double>(a); }
 }  // namespace ice

@@ -3,4 +3,5 @@
 namespace ice {
 void launch_stage_mk_f32(const LaunchArgs& a, bool write_r) { launch_stage_t<MK, float>(a, write_r); }
 void launch_source_mk_f32(const LaunchArgs& a) { launch_source_t<MK, float>(a); }
+void launch_bound_mk_f32(const LaunchArgs& a) { launch_bound_t<MK, float>(a); }
 }  // namespace ice
