@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload multiblock48|cloud192|cloud96|jets1024|riemann2000]
-                    [--precision fp32flux|fp64] [--no-plain] [--timed-only]
+                    [--precision fp32flux|fp64] [--no-plain] [--timed-only] [--surrogate]
 
 One "step" is one full time step (every family, every RK stage) of the workload. The default
 workload is the 3-D multi-block evaporating case (48 blocks of U[16,160] cells per axis, seed 9,
@@ -257,6 +257,65 @@ def allmax(dist, x: float) -> float:
     return float(t.item())
 
 
+def run_surrogate(args, rank, world, dist):
+    """The surrogate-evaporation workload (the 48-block, three-family geometry): every evaporating family
+    gets a network trained on 4,194,304 pairs from the plain closure over the envelope of the initial
+    state; the steps then run with it, beside the same steps with the plain FP32 closure. value: cell-
+    updates/s with the surrogate; the line adds the fraction of cells the network served and each
+    family's training report."""
+    lib = abi.load_gpu()
+    if args.workload == "multiblock48":        # evaporation active in every cell: droplets everywhere
+        case = configs.multiblock_tree(steps=args.warmup + args.steps, precision=abi.PREC_FP32FLUX,
+                                       evaporation_everywhere=True)
+    else:
+        case = make_workload(args.workload, abi.PREC_FP32FLUX, args.warmup + args.steps)
+    cells = case.ncells
+    sur = Solver(case, lib)
+    reports = {}
+    for p, fam in enumerate(case.families):
+        if fam.evap == "none":
+            continue
+        o = abi.SurrogateOpts(nsamples=1 << 22, epochs=20, batch=8192, lr=2e-3, jitter=0.05, seed=17 + p, val_frac=0.02)
+        rep = abi.SurrogateReport()
+        rc = lib.surrogate_train(sur.ctx, p + 1, C.byref(o), C.byref(rep))
+        if rc != 0:
+            raise SystemExit(f"surrogate_train: {lib.error(sur.ctx)}")
+        reports[fam.closure] = {"train_s": round(rep.seconds, 1), "steps": rep.steps, "val_loss": rep.val_loss,
+                                "mdot_rel_median": rep.mdot_rel_median, "mdot_rel_p99": rep.mdot_rel_p99,
+                                "q_rel_median": rep.q_rel_median, "q_rel_p99": rep.q_rel_p99}
+    sur.step(args.warmup)
+    c0 = (C.c_int64 * 3)()
+    lib.surrogate_stats(sur.ctx, c0)
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        out = sur.step(args.steps)
+    c1 = (C.c_int64 * 3)()
+    lib.surrogate_stats(sur.ctx, c1)
+    ms = allmax(dist, out.device_ms)
+    value = cells * args.steps * world / (ms * 1e-3)
+    st_sur = sur.download_all()
+    sur.close()
+    plain = Solver(case, lib)
+    plain.step(args.warmup)
+    o2 = plain.step(args.steps)
+    l1 = rel_l1(st_sur, plain.download_all(), case)
+    plain.close()
+    n_eval, n_env, n_res = (c1[q] - c0[q] for q in range(3))
+    if rank != 0:
+        return
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 flux / f64 accumulate, bf16 surrogate",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload + "+surrogate", "cells": cells,
+                       "families": [f.closure for f in case.families], "form": "fp32flux + surrogate evaporation"},
+            "clocks": clk.summary(),
+            "surrogate": {"cells_evaluated": n_eval, "served_by_network": n_eval - n_env - n_res,
+                          "outside_envelope": n_env, "failed_check": n_res,
+                          "plain_closure_value": cells * args.steps / (o2.device_ms * 1e-3),
+                          "l1_vs_plain_closure": l1, "training": reports}}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, rank, world, dist):
     lib = abi.load_gpu()
     prec = abi.PREC_FP32FLUX if args.precision == "fp32flux" else abi.PREC_FP64
@@ -377,6 +436,7 @@ def main():
     ap.add_argument("--precision", default="fp32flux", choices=["fp64", "fp32flux"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 form beside the chosen one")
     ap.add_argument("--timed-only", action="store_true", help="only the timed steps (for profiler runs)")
+    ap.add_argument("--surrogate", action="store_true", help="the surrogate-evaporation workload (networks trained first)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -391,7 +451,10 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = tdist
-    run_ours(args, rank, world, dist)
+    if args.surrogate:
+        run_surrogate(args, rank, world, dist)
+    else:
+        run_ours(args, rank, world, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

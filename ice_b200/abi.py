@@ -60,8 +60,23 @@ class StepOut(C.Structure):
                 ("residual", C.c_double * 5), ("device_ms", C.c_double)]
 
 
+class SurrogateOpts(C.Structure):
+    _fields_ = [("nsamples", C.c_int64), ("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_double),
+                ("jitter", C.c_double), ("seed", C.c_uint64), ("val_frac", C.c_double)]
+
+
+class SurrogateReport(C.Structure):
+    _fields_ = [("train_loss", C.c_double), ("val_loss", C.c_double), ("mdot_rel_median", C.c_double),
+                ("mdot_rel_p99", C.c_double), ("q_rel_median", C.c_double), ("q_rel_p99", C.c_double),
+                ("seconds", C.c_double), ("nsamples", C.c_int64), ("steps", C.c_int64),
+                ("env_lo", C.c_double * 7), ("env_hi", C.c_double * 7)]
+
+
+MLP_NPARAM = 7 * 128 + 128 + 3 * (128 * 128 + 128) + 128 * 2 + 2
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
+_fp = C.POINTER(C.c_float)
 _u8p = C.POINTER(C.c_uint8)
 _vp = C.c_void_p
 
@@ -91,6 +106,11 @@ GPU_ONLY = [
     ("set_profiling", C.c_int, [_vp, C.c_int32]),
     ("kernel_times", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(C.c_int64)]),
     ("residual_sq_noalloc", C.c_int, [_vp, _vp, C.c_int32, C.c_int32, _ip, _dp, _vp, C.c_char_p, C.c_int32]),
+    ("surrogate_train", C.c_int, [_vp, C.c_int32, C.POINTER(SurrogateOpts), C.POINTER(SurrogateReport)]),
+    ("surrogate_enable", C.c_int, [_vp, C.c_int32, C.c_int32]),
+    ("surrogate_stats", C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    ("mlp_grad", C.c_int, [_fp, _fp, _fp, C.c_int32, _fp, _fp]),
+    ("mlp_infer", C.c_int, [_fp, _fp, C.c_int32, _fp]),
 ]
 
 # every symbol include/ice_gpu.h declares

@@ -21,7 +21,7 @@ SRC = PKG / "csrc"
 OBJ = PKG / "lib" / "obj"
 OUT = PKG / "lib" / "libice_gpu.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-UNITS = ["ice_gpu.cu", "ice_noalloc.cu", "ice_fam_mk.cu", "ice_fam_ig.cu", "ice_fam_ag.cu"] + [
+UNITS = ["ice_gpu.cu", "ice_noalloc.cu", "ice_mlp_f32.cu", "ice_fam_mk.cu", "ice_fam_ig.cu", "ice_fam_ag.cu"] + [
     f"ice_stage_{c}_{p}.cu" for c in ("mk", "ig", "ag") for p in ("f64", "f32")]
 # -prec-div=false -prec-sqrt=false -ftz=true act on single precision only: the FP32-flux form
 # divides and takes roots at hardware speed; every FP64 operation stays IEEE and unfused.

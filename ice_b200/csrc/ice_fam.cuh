@@ -3,6 +3,7 @@
 // closure and precision (ice_stage.cuh), and the IRS sweeps when they are on.
 #pragma once
 #include "ice_kernels.cuh"
+#include "ice_mlp.cuh"
 
 namespace ice {
 
@@ -33,8 +34,13 @@ void launch_family_t(const LaunchArgs& a) {
   cudaStream_t s = a.s;
   auto tick = [&](int cls) { if (a.tick) a.tick(a.tick_ctx, cls, s); };
   auto grid = [](long long n, int t) { return (unsigned)((n + t - 1) / t); };
-  if (a.F.coupled && a.ntile3 == 0) {   // compute_source comes first in the stage (Mod_Explicit.f90:111-117);
-    launch_source_of<CL>(a);              // the staged stage kernel evaluates it per cell itself
+  // compute_source comes first in the stage (Mod_Explicit.f90:111-117): the staged stage kernel
+  // evaluates it per cell itself, unless the evaporation surrogate's source kernel runs first
+  if (a.F.coupled && a.mlp_img) {
+    launch_source_mlp(CL, a, a.mlp_img, *a.mlp_norm);
+    tick(KC_SOURCE);
+  } else if (a.F.coupled && a.ntile3 == 0) {
+    launch_source_of<CL>(a);
     tick(KC_SOURCE);
   }
   if (a.nrec > 0) {

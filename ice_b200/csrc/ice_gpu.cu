@@ -35,6 +35,7 @@
 #include <memory>
 #include "ice_kernels.cuh"
 #include "ice_stage3.cuh"
+#include "ice_mlp.cuh"
 #include "../../include/ice_gpu.h"
 
 using namespace ice;
@@ -73,6 +74,12 @@ struct FamHost {
   DevBuf<CUtensorMap> maps[3];               // per state buffer, per block: the staged kernel's TMA maps
   DevBuf<Tile> tiles3;                       // the staged kernel's tiles (the tile shape is the closure's)
   int ntile3 = 0;
+  // the evaporation surrogate (FP32-flux form): the network's BF16 image, its standardisation and
+  // envelope, its FP32 parameters; on = the stage's source comes from the surrogate source kernel
+  DevBuf<unsigned char> mlp_img;
+  MlpNorm mlp_norm;
+  std::vector<float> mlp_w;
+  bool sur_on = false;
   int nrec = 0, nbc = 0, nown = 0, ncf = 0;
   std::vector<int> h_first, h_list, h_own;   // 0-based record numbers of the whole table
 };
@@ -115,6 +122,11 @@ struct ice_gpu_ctx {
 };
 
 static std::string g_create_err;
+
+static bool sur_active(const ice_gpu_ctx* c, int p) {
+  const FamHost& H = c->fam[p];
+  return H.sur_on && H.mlp_img.p && c->P.coupled && c->P.precision == ICE_PREC_FP32FLUX && !c->P.irs;
+}
 
 // The caller's prim(nc, -1:ni+2, -1:nj+2, -1:nk+2) (variable fastest) <-> one block of the SoA pool,
 // whose rows are px long (the row padding is never read).
@@ -159,6 +171,9 @@ static void free_graphs(ice_gpu_ctx* c) {
   for (auto& g : c->graph) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
+// The surrogate source runs for family p: on, trained, a coupled run in the FP32-flux form.
+static bool sur_active(const ice_gpu_ctx* c, int p);
+
 // The buffer stage srk reads as its stencil (U_{k-1}) when the step starts from buffer `phase`.
 static int stencil_buffer(const ice_gpu_ctx*, int srk, int phase) {
   return srk == 1 ? phase : srk == 2 ? (phase + 1) % 3 : (phase + 2) % 3;
@@ -196,6 +211,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
   F.rk = RKC[c->P.nrk - 1][srk - 1];
   F.write_tau = srk == c->P.nrk;
+  F.src_ready = sur_active(c, p) ? 1 : 0;
   return F;
 }
 
@@ -223,6 +239,8 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.KZ = c->KZ;
   a.tiles3 = H.tiles3.p; a.ntile3 = H.ntile3;
   a.maps = H.maps[stencil_buffer(c, srk, phase)].p;
+  a.mlp_img = sur_active(c, p) ? H.mlp_img.p : nullptr;
+  a.mlp_norm = &H.mlp_norm;
   a.ndir = c->P.ndir; a.sd = c->P.shock_detector; a.irs = c->P.irs; a.precision = c->P.precision;
   a.irs_beta = c->P.irs_beta;
   a.resid = H.resid.p; a.resid2 = H.resid2.p; a.resid3 = H.resid3.p;
@@ -275,7 +293,7 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
     long long per = (H.nrec > 0 ? 1 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
-                    (c->P.coupled && !c->staged ? 1 : 0);
+                    (c->P.coupled && (!c->staged || sur_active(c, p)) ? 1 : 0);
     per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
     n += per * c->P.nrk;
   }
@@ -869,6 +887,80 @@ int ice_gpu_kernel_times(const ice_gpu_ctx* c, double* ms, int32_t nclass, int64
   if (!c) return ICE_GPU_EINVAL;
   for (int q = 0; q < nclass && q < KC_N; ++q) ms[q] = c->kms[q];
   if (nlaunch) *nlaunch = c->profiling ? c->nlaunch : 0;
+  return 0;
+}
+
+// ---------------------------------------------------------------- the evaporation surrogate
+int ice_gpu_surrogate_train(ice_gpu_ctx* c, int32_t p1, const ice_gpu_surrogate_opts* o, ice_gpu_surrogate_report* rep) {
+  if (!c || !o) return ICE_GPU_EINVAL;
+  if (p1 < 1 || p1 > c->P.nfam) return fail(c, ICE_GPU_EINVAL, "surrogate_train: family %d out of range", p1);
+  if (int rc = check_ready(c)) return rc;
+  if (!c->P.coupled) return fail(c, ICE_GPU_EINVAL, "surrogate_train: the run is not coupled (no source to replace)");
+  const ice_gpu_family& pf = c->P.fam[p1 - 1];
+  if (pf.evap == 0) return fail(c, ICE_GPU_EINVAL, "surrogate_train: family %d has no evaporation", p1);
+  if (o->nsamples < 1024 || o->nsamples > (1LL << 26) || o->epochs < 1 || o->batch < 64 || o->batch > 65536 ||
+      !(o->lr > 0) || !(o->val_frac > 0 && o->val_frac < 0.5))
+    return fail(c, ICE_GPU_EINVAL, "surrogate_train: options out of range");
+  FamHost& H = c->fam[p1 - 1];
+  DevBuf<float> X, T;
+  CK(X.alloc((size_t)o->nsamples * MLP_IN));
+  CK(T.alloc((size_t)o->nsamples * 2));
+  FamDev F = make_famdev(c, p1 - 1, 1, c->phase);
+  if (mlp_make_samples(H.closure, make_geo(c), F, c->P.drag, c->P.heat, c->P.blow, o->nsamples, o->seed, o->jitter,
+                       X.p, T.p, c->stream))
+    return fail(c, ICE_GPU_ECUDA, "surrogate_train: sample kernel: %s", cudaGetErrorString(cudaGetLastError()));
+  MlpTrainOpts to{o->nsamples, o->epochs, o->batch, o->lr, o->jitter, o->seed, o->val_frac};
+  MlpTrainReport tr{};
+  std::string err;
+  if (mlp_train(X.p, T.p, o->nsamples, to, H.mlp_w, H.mlp_norm, tr, c->stream, err))
+    return fail(c, ICE_GPU_ECUDA, "%s: %s", err.c_str(), cudaGetErrorString(cudaGetLastError()));
+  std::vector<unsigned char> img;
+  mlp_image(H.mlp_w.data(), img);
+  CK(H.mlp_img.alloc(img.size()));
+  CK(cudaMemcpy(H.mlp_img.p, img.data(), img.size(), cudaMemcpyHostToDevice));
+  H.sur_on = true;
+  free_graphs(c);
+  if (rep) {
+    rep->train_loss = tr.train_loss; rep->val_loss = tr.val_loss;
+    rep->mdot_rel_median = tr.mdot_rel_median; rep->mdot_rel_p99 = tr.mdot_rel_p99;
+    rep->q_rel_median = tr.q_rel_median; rep->q_rel_p99 = tr.q_rel_p99;
+    rep->seconds = tr.seconds; rep->nsamples = tr.nsamples; rep->steps = tr.steps;
+    for (int a = 0; a < MLP_IN; ++a) { rep->env_lo[a] = H.mlp_norm.env_lo[a]; rep->env_hi[a] = H.mlp_norm.env_hi[a]; }
+  }
+  return 0;
+}
+
+int ice_gpu_surrogate_enable(ice_gpu_ctx* c, int32_t p1, int32_t on) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (p1 < 1 || p1 > c->P.nfam) return fail(c, ICE_GPU_EINVAL, "surrogate_enable: family %d out of range", p1);
+  FamHost& H = c->fam[p1 - 1];
+  if (on && !H.mlp_img.p) return fail(c, ICE_GPU_ENOTREADY, "surrogate_enable: family %d has no trained network", p1);
+  CK(cudaStreamSynchronize(c->stream));
+  H.sur_on = on != 0;
+  free_graphs(c);
+  return 0;
+}
+
+int ice_gpu_surrogate_stats(const ice_gpu_ctx* c, int64_t* counts) {
+  if (!c || !counts) return ICE_GPU_EINVAL;
+  Status h;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+      cudaMemcpy(&h, c->st.p, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return ICE_GPU_ECUDA;
+  counts[0] = (int64_t)h.sur_cells; counts[1] = (int64_t)h.sur_env; counts[2] = (int64_t)h.sur_res;
+  return 0;
+}
+
+int ice_gpu_mlp_grad(const float* w, const float* x, const float* t, int32_t n, float* grad, float* loss) {
+  if (!w || !x || !t || !grad || !loss || n < 1 || n > 65536) return fail(nullptr, ICE_GPU_EINVAL, "mlp_grad: bad arguments");
+  std::string err;
+  if (mlp_grad_host(w, x, t, n, grad, loss, err)) return fail(nullptr, ICE_GPU_ECUDA, "%s", err.c_str());
+  return 0;
+}
+
+int ice_gpu_mlp_infer(const float* w, const float* x, int32_t n, float* y) {
+  if (!w || !x || !y || n < 1) return fail(nullptr, ICE_GPU_EINVAL, "mlp_infer: bad arguments");
+  std::string err;
+  if (mlp_infer_host(w, x, n, y, err)) return fail(nullptr, ICE_GPU_ECUDA, "%s", err.c_str());
   return 0;
 }
 

@@ -52,6 +52,7 @@ struct Status {
   double time;
   int iter;
   int iter_from_call;
+  unsigned long long sur_cells, sur_env, sur_res;   // surrogate: cells, envelope and check fallbacks
 };
 
 __device__ __forceinline__ long long gidx(const DBlock& B, int i, int j, int k) {
@@ -95,9 +96,11 @@ struct FamDev {              // what the kernels of one family read
   double* resid;             // IRS: [v][NI]
   double rk;
   int write_tau;
+  int src_ready;             // S holds this stage's source already (the surrogate source kernel ran)
 };
 
-struct Tile { int b, i0, j0, k0, nkz; };   // a column tile of a block and its chunk of nkz planes
+struct Tile { int b, i0, j0, k0, nkz; };
+struct MlpNorm;   // a column tile of a block and its chunk of nkz planes
 struct NormChunk { int b; long long q0, q1; };
 
 // Everything one family's stage needs, for the launcher of its closure's translation unit.
@@ -110,6 +113,8 @@ struct LaunchArgs {
   const Tile* tiles; int ntile; int TX, TY, KZ;     // the 1-D stage kernel's tiles
   const Tile* tiles3; int ntile3;                    // the staged stage kernel's tiles (2-D and 3-D runs)
   const CUtensorMap* maps;                           // per block: the TMA map of U_{k-1} (the stencil buffer)
+  const unsigned char* mlp_img;                      // the family's surrogate network (null: the plain closure)
+  const MlpNorm* mlp_norm;
   int ndir, sd, irs, precision;
   double irs_beta;
   double* resid; double* resid2; double* resid3;

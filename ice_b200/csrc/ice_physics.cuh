@@ -796,39 +796,70 @@ template <int CL, typename R> __device__ __forceinline__ void source_make(const 
   }
 }
 
+// The per-particle quantities compute_source_ forms before the evaporation call (Mod_Sources.f90:
+// 465-519), the ITC/clamp, non-burning, constant-property path.
+template <typename R> struct CellPhys {
+  R T, n, rho_mat, Rp, du, Re, Ma, Pr, Nu, Cd;
+};
+template <int CL, typename R> __device__ __forceinline__ CellPhys<R> cell_phys(const R* p, const R* gas, R gR, R ggam,
+                                                                              R gk, R gmu, const Mat& m, int drag_sel,
+                                                                              int heat_sel) {
+  constexpr int nb = NC<CL>::v;
+  const R pi = (R)kPi;
+  CellPhys<R> c;
+  c.T = p[nb - 2]; c.n = p[nb - 1];
+  c.rho_mat = (R)m.rho;
+  c.Rp = pw((R)0.75*p[0]/(c.n*pi*c.rho_mat), (R)(1.0/3.0));
+  c.du = norm2_3(gas[1] - p[1], gas[2] - p[2], gas[3] - p[3]);
+  c.Re = (R)2*gas[0]*c.Rp*c.du/gmu;
+  c.Ma = c.du/pw(ggam*gR*gas[4], (R)0.5);
+  c.Pr = ggam/(ggam - (R)1)*gR*gmu/gk;
+  c.Nu = heat(c.Re, c.Pr, c.Ma, heat_sel);
+  R Tr = c.T/gas[4];
+  c.Cd = drag(c.Re, c.Ma, ggam, Tr, drag_sel);
+  return c;
+}
+
+// The rest of compute_source_ from the mass and heat transfer rates (Mod_Sources.f90:552-622):
+// mass, momentum and energy sources with radiation, the relaxation time, source_make. Returns tau
+// (INF when Cd == 0).
+template <int CL, typename R> __device__ __forceinline__ R cell_source_finish(const CellPhys<R>& c, const R* p,
+                                                                             const R* gas, const Mat& m, R mdot,
+                                                                             R Qconv, R* s) {
+  const R pi = (R)kPi;
+  R F[6];
+  F[1] = gas[1] - p[1]; F[2] = gas[2] - p[2]; F[3] = gas[3] - p[3];
+  F[0] = -mdot*c.n;
+  F[4] = Qconv*c.n;
+  F[4] = F[4] + (R)m.emiss*(R)kSigmaSB*(R)4*pi*c.Rp*c.Rp*c.n*(pw(gas[4], (R)4) - pw(c.T, (R)4));
+  R tau;
+  if (c.Cd == (R)0) tau = (R)INFINITY;
+  else tau = (R)8*c.rho_mat*c.Rp/((R)3*gas[0]*c.Cd*c.du + toll_d<R>());
+  F[5] = tau;
+  source_make<CL>(p, F, s, (R)m.cp, (R)m.lv);
+  return tau;
+}
+
+// The plain closure's mass and heat transfer rates (compute_source_'s evaporation part): heat
+// correlation, evaporation with its interface model, override or blowing.
+template <typename R> __device__ __forceinline__ void closure_rates(R rhog, R Tg, R gam, R gR, R gmu, R gk, R Ts, R Rp,
+                                                                   R Re, R Nu, const Mat& m, int blow, R& mdot, R& Qconv) {
+  const R pi = (R)kPi;
+  Qconv = (R)2*Nu*gk*pi*Rp*(Tg - Ts);
+  R Qevap; bool ovr;
+  evaporation<R>(rhog, Tg, gam, gR, gmu, gk, Ts, (R)2*Rp, Re, m, mdot, Qevap, ovr);
+  if (ovr) Qconv = Qevap;
+  else if (blow == 1) Qconv = Qconv*blowing<R>(gam, gR, gmu, gk, (R)m.rho, (R)2*Rp, (R)(4.0/3.0)*pi*(Rp*Rp*Rp)*(R)m.rho, mdot);
+}
+
 // compute_source_ + cell_surface on the ITC/clamp, non-burning, constant-property path.
 // gas = rho u v w T. Returns tau. INF when Cd == 0.
 template <int CL, typename R> __device__ R cell_source(const R* p, const R* gas, R gR, R ggam, R gk, R gmu,
                                                       const Mat& m, int drag_sel, int heat_sel, int blow, R* s) {
-  constexpr int nb = NC<CL>::v;
-  const R pi = (R)kPi;
-  R T = p[nb - 2], n = p[nb - 1];
-  R rho_mat = (R)m.rho;
-  R Rp = pw((R)0.75*p[0]/(n*pi*rho_mat), (R)(1.0/3.0));
-  R du = norm2_3(gas[1] - p[1], gas[2] - p[2], gas[3] - p[3]);
-  R Re = (R)2*gas[0]*Rp*du/gmu;
-  R Ma = du/pw(ggam*gR*gas[4], (R)0.5);
-  R Pr = ggam/(ggam - (R)1)*gR*gmu/gk;
-  R Nu = heat(Re, Pr, Ma, heat_sel);
-  R Ts = T;
-  R Tr = Ts/gas[4];
-  R Cd = drag(Re, Ma, ggam, Tr, drag_sel);
-  R F[6];
-  F[1] = gas[1] - p[1]; F[2] = gas[2] - p[2]; F[3] = gas[3] - p[3];
-  R Qconv = (R)2*Nu*gk*pi*Rp*(gas[4] - Ts);
-  R mdot, Qevap; bool ovr;
-  evaporation<R>(gas[0], gas[4], ggam, gR, gmu, gk, Ts, (R)2*Rp, Re, m, mdot, Qevap, ovr);
-  if (ovr) Qconv = Qevap;
-  else if (blow == 1) Qconv = Qconv*blowing<R>(ggam, gR, gmu, gk, rho_mat, (R)2*Rp, (R)(4.0/3.0)*pi*(Rp*Rp*Rp)*rho_mat, mdot);
-  F[0] = -mdot*n;
-  F[4] = Qconv*n;
-  F[4] = F[4] + (R)m.emiss*(R)kSigmaSB*(R)4*pi*Rp*Rp*n*(pw(gas[4], (R)4) - pw(Ts, (R)4));
-  R tau;
-  if (Cd == (R)0) tau = (R)INFINITY;
-  else tau = (R)8*rho_mat*Rp/((R)3*gas[0]*Cd*du + toll_d<R>());
-  F[5] = tau;
-  source_make<CL>(p, F, s, (R)m.cp, (R)m.lv);
-  return tau;
+  const CellPhys<R> c = cell_phys<CL, R>(p, gas, gR, ggam, gk, gmu, m, drag_sel, heat_sel);
+  R mdot, Qconv;
+  closure_rates<R>(gas[0], gas[4], ggam, gR, gmu, gk, c.T, c.Rp, c.Re, c.Nu, m, blow, mdot, Qconv);
+  return cell_source_finish<CL, R>(c, p, gas, m, mdot, Qconv, s);
 }
 
 }  // namespace ice

@@ -393,7 +393,10 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       double s[nc];
 #pragma unroll
       for (int v = 0; v < nc; ++v) s[v] = 0.0;
-      if (F.coupled) {                          // compute_source_ on the stage's state
+      if (F.coupled && F.src_ready) {           // the surrogate source kernel ran first
+#pragma unroll
+        for (int v = 0; v < nc; ++v) s[v] = F.S[(long long)v * G.NI + q];
+      } else if (F.coupled) {                   // compute_source_ on the stage's state
         R pr_[nc], gas[5], sr[nc];
 #pragma unroll
         for (int v = 0; v < nc; ++v) pr_[v] = (R)p[v];

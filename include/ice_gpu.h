@@ -142,6 +142,28 @@ typedef struct ice_gpu_step_out {
                                            the context's stream)                          */
 } ice_gpu_step_out;
 
+/* Training of the evaporation surrogate (ice_gpu_surrogate_train). */
+typedef struct ice_gpu_surrogate_opts {
+    int64_t  nsamples;                  /* training pairs drawn from the plain closure    */
+    int32_t  epochs;
+    int32_t  batch;
+    double   lr;                        /* Adam's initial learning rate (cosine decay)    */
+    double   jitter;                    /* spread of the sampled radius and speed (relative)
+                                           and temperatures (x 20 K) around visited cells */
+    uint64_t seed;
+    double   val_frac;                  /* held-out fraction of the pairs                 */
+} ice_gpu_surrogate_opts;
+
+typedef struct ice_gpu_surrogate_report {
+    double  train_loss;                 /* mean-square loss of the last 20 batches (standardised) */
+    double  val_loss;                   /* the same on the held-out pairs                 */
+    double  mdot_rel_median, mdot_rel_p99;   /* held-out relative error of the mass rate  */
+    double  q_rel_median, q_rel_p99;         /* and of the heat rate                      */
+    double  seconds;                    /* sampling and training                          */
+    int64_t nsamples, steps;
+    double  env_lo[7], env_hi[7];       /* the envelope of the seven inputs the network accepts */
+} ice_gpu_surrogate_report;
+
 typedef struct ice_gpu_ctx ice_gpu_ctx;
 
 /* Set-up (after setup_freeze, Wrap_Setup.f90:121). dims: 3 ints per block.
@@ -213,6 +235,31 @@ int ice_gpu_residual_norm(ice_gpu_ctx* ctx, double* total, double* fam);
 int ice_gpu_residual_sq_noalloc(const double* prim_new, const double* prim_old, int32_t nc,
                                 int32_t t_slot, const int32_t* dims, double* sums, void* stream,
                                 char* err, int32_t errlen);
+
+/* The evaporation surrogate of family p (FP32-flux form, coupled runs): draws o->nsamples inputs
+ * around the cells of the current state, evaluates the plain FP64 closure on them (evaporation with
+ * its interface model, the heat correlation, override or blowing: compute_source_,
+ * Mod_Sources.f90:520-551), trains a 7 -> 128 x 4 -> 2 SiLU network on them with the library's own
+ * FP32 forward, backward and Adam kernels, and switches the family's source to it: BF16 tensor-core
+ * inference, with the plain closure for every cell outside the training envelope or whose rates fail
+ * the closure's own equations by more than 1e-3. No counterpart in the reference (its closure is
+ * always evaluated); it replaces the iterative part of the evaporation source. */
+int ice_gpu_surrogate_train(ice_gpu_ctx* ctx, int32_t p, const ice_gpu_surrogate_opts* opts,
+                            ice_gpu_surrogate_report* report);
+
+/* Switches family p between the trained surrogate (on) and the plain closure (off). */
+int ice_gpu_surrogate_enable(ice_gpu_ctx* ctx, int32_t p, int32_t on);
+
+/* Cumulative counts of the surrogate source: counts[0] cells evaluated, counts[1] of them outside
+ * the envelope, counts[2] of them failing the closure check (both ran the plain closure). */
+int ice_gpu_surrogate_stats(const ice_gpu_ctx* ctx, int64_t* counts);
+
+/* Checks of the surrogate's kernels on host arrays (no context): the loss (mean-square over n x 2
+ * standardised targets t) and its gradient with respect to the FP32 parameters w of the training
+ * kernels, for n standardised inputs x (n x 7); and the BF16 tensor-core forward pass y (n x 2).
+ * No counterpart in the reference. */
+int ice_gpu_mlp_grad(const float* w, const float* x, const float* t, int32_t n, float* grad, float* loss);
+int ice_gpu_mlp_infer(const float* w, const float* x, int32_t n, float* y);
 
 /* A runtime re-read of input.ini (Wrap_Postprocess.f90:255 -> Read_Ini.f90:61): the
  * numerics may change between steps; nfam, closures and ndir may not. */
