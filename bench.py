@@ -1,7 +1,7 @@
 """Benchmark of the solve stage on B200: cell-updates/s of ICE's dispersed-phase time step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload multiblock48|cloud192|cloud96|jets1024|riemann2000]
+                    [--workload multiblock48|multiblock4|cloud192|cloud96|jets1024|riemann2000]
                     [--precision fp32flux|fp64] [--no-plain] [--timed-only] [--surrogate]
 
 One "step" is one full time step (every family, every RK stage) of the workload. The default
@@ -54,6 +54,8 @@ def peaks():
 def make_workload(name: str, precision: int, steps: int):
     if name == "multiblock48":
         return configs.multiblock_tree(steps=steps, precision=precision)
+    if name == "multiblock4":   # the first 4 blocks of the same tree (3.7 M cells), the profiling case
+        return configs.multiblock_tree(nblocks=4, steps=steps, precision=precision)
     if name == "cloud192":
         return configs.cloud_3d(n=192, steps=steps, precision=precision)
     if name == "cloud96":       # the same recipe at 96^3 (0.88 M cells), the profiling case
@@ -259,7 +261,7 @@ def allmax(dist, x: float) -> float:
 
 def run_surrogate(args, rank, world, dist):
     """The surrogate-evaporation workload (the 48-block, three-family geometry): every evaporating family
-    gets a network trained on 4,194,304 pairs from the plain closure over the envelope of the initial
+    gets a network trained on 4,194,304 pairs (by default) from the plain closure over the envelope of the initial
     state; the steps then run with it, beside the same steps with the plain FP32 closure. value: cell-
     updates/s with the surrogate; the line adds the fraction of cells the network served and each
     family's training report."""
@@ -275,7 +277,8 @@ def run_surrogate(args, rank, world, dist):
     for p, fam in enumerate(case.families):
         if fam.evap == "none":
             continue
-        o = abi.SurrogateOpts(nsamples=1 << 22, epochs=20, batch=8192, lr=2e-3, jitter=0.05, seed=17 + p, val_frac=0.02)
+        o = abi.SurrogateOpts(nsamples=args.surrogate_samples, epochs=args.surrogate_epochs, batch=8192, lr=2e-3,
+                              jitter=0.05, seed=17 + p, val_frac=0.02)
         rep = abi.SurrogateReport()
         rc = lib.surrogate_train(sur.ctx, p + 1, C.byref(o), C.byref(rep))
         if rc != 0:
@@ -437,6 +440,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 form beside the chosen one")
     ap.add_argument("--timed-only", action="store_true", help="only the timed steps (for profiler runs)")
     ap.add_argument("--surrogate", action="store_true", help="the surrogate-evaporation workload (networks trained first)")
+    ap.add_argument("--surrogate-samples", type=int, default=1 << 22, help="training pairs per evaporating family")
+    ap.add_argument("--surrogate-epochs", type=int, default=20)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
