@@ -1,7 +1,7 @@
 """Benchmark of the solve stage on B200: cell-updates/s of ICE's dispersed-phase time step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload multiblock48|multiblock4|cloud192|cloud96|jets1024|riemann2000]
+                    [--workload multiblock48|multiblock4|cloud192|cloud96|jets1024|taylorgreen192|riemann2000]
                     [--precision fp32flux|fp64] [--no-plain] [--timed-only] [--surrogate]
 
 One "step" is one full time step (every family, every RK stage) of the workload. The default
@@ -62,6 +62,8 @@ def make_workload(name: str, precision: int, steps: int):
         return configs.cloud_3d(n=96, steps=steps, length=0.0096, precision=precision)
     if name == "jets1024":
         return configs.jets_2d(n=1024, steps=steps, precision=precision)
+    if name == "taylorgreen192":   # built like the reference's published 192^3 IG benchmark
+        return configs.taylor_green_ig(n=192, steps=steps, precision=precision)
     if name == "riemann2000":
         return configs.riemann_1d(n=2000, steps=steps)
     raise SystemExit(f"unknown workload {name}")
@@ -78,6 +80,8 @@ def sample_workload(name: str):
         return configs.cloud_3d(n=48, steps=1, length=0.0048), "48^3 of the same recipe"
     if name == "jets1024":
         return configs.jets_2d(n=256, steps=1), "256^2 of the same recipe"
+    if name == "taylorgreen192":
+        return configs.taylor_green_ig(n=64, steps=1), "64^3 of the same recipe"
     return configs.riemann_1d(n=2000, steps=1), "the whole case"
 
 

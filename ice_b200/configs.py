@@ -190,6 +190,37 @@ def jets_2d(n=1024, steps=500, seed=2, length=0.1, precision=0):
     return case
 
 
+# --------------------------------------- the reference's published benchmark, restated
+def taylor_green_ig(n=192, steps=100, h=1e-3, precision=0):
+    """A case built like the reference's published performance benchmark (192^3 cube, one block, one IG
+    family, a frozen Taylor-Green gas, drag and heat, no evaporation; MUSCL van Leer, Rusanov, SSP-RK2,
+    CFL 0.5): cells of 1 mm; particles of 10 um and material density 1000 with bulk density
+    1e-3 (1 + 0.3 cos kx cos ky cos kz), velocity (10, 7, 4) m/s, dispersion 1 m/s, 300 K; gas 1.2 kg/m3,
+    u = sin kx cos ky cos kz, v = -cos kx sin ky cos kz, w = 0 (m/s), 300 K, k = 2 pi / L. Every face is
+    an outflow (400)."""
+    L = n * h
+    nodes = box_nodes(n, n, n, size=(L, L, L))
+    fam = Family("IG", riemann="Rusanov", rho_al=1000.0, cs_al=4180.0, lv_al=2.26e6)
+    num = Numerics(scheme="RK2", cfl=0.5, limiter="vanleer", coupled=True, drag="Schiller-Naumann",
+                   heat="Ranz-Marshall", itermax=steps, precision=precision)
+    rows = box_bc(1, (n, n, n), {1: 400, 2: 400, 3: 400, 4: 400, 5: 400, 6: 400})
+    case = Case("taylor_green_ig", [nodes], [fam], num, rows)
+    xc = (np.arange(n) + 0.5) * h
+    kk = 2.0 * PI / L
+    cz, cy, cx = np.meshgrid(np.cos(kk * xc), np.cos(kk * xc), np.cos(kk * xc), indexing="ij")
+    sz, sy, sx = np.meshgrid(np.sin(kk * xc), np.sin(kk * xc), np.sin(kk * xc), indexing="ij")
+    rho = 1e-3 * (1.0 + 0.3 * cx * cy * cz)
+    mp = particle_mass(10e-6, fam.rho_al)
+    st = empty_state((n, n, n), fam.nc)
+    I = st[2:-2, 2:-2, 2:-2]
+    I[..., 0] = rho; I[..., 1] = 10.0; I[..., 2] = 7.0; I[..., 3] = 4.0
+    I[..., 4] = rho * 1.0 / 3.0; I[..., 5] = 300.0; I[..., 6] = rho / mp
+    case.state = [[st]]
+    case.gas = [_gas_layout(case, 0, np.full((n, n, n), 1.2), sx * cy * cz, -cx * sy * cz, 0.0 * cx,
+                            np.full((n, n, n), 300.0))]
+    return case
+
+
 # ------------------------------------------------------------ config 3
 def droplet_material(**kw):
     d = dict(rho_al=1000.0, cs_al=4180.0, lv_al=2.26e6, emiss=0.9, evap="CEM", intf="LK", Mv=18.015,

@@ -47,7 +47,9 @@ void launch_family_t(const LaunchArgs& a) {
     k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
     tick(KC_GHOST);
   }
-  if (a.sd) {
+  // the Jameson sensor: the staged stage kernel and the boundary kernels evaluate it from the
+  // density they read; only the 1-D stage kernel reads it from a field
+  if (a.sd && a.ntile3 == 0) {
     k_beta<<<grid(a.G.NI, 256), 256, 0, s>>>(a.G, a.F);
     tick(KC_BETA);
   }

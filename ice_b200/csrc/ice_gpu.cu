@@ -10,7 +10,7 @@
 //   per family, per RK stage:
 //     k_ghost      both ghost layers from the record list, block
 //                  connections as on-device copies in one HBM pool    (Lib_Ghost.f90:29-387)
-//     k_beta       Jameson sensor (when on)                           (Mod_Fluxes.f90:366-389)
+//     k_beta       Jameson sensor (when on; 1-D runs only)            (Mod_Fluxes.f90:366-389)
 //     k_conn       connection-face fluxes by their owner records      (Mod_BC_Fluxes.f90:151-170)
 //     k_bound      boundary cells, records summed in face order        (Mod_BC_Fluxes.f90:105-144)
 //     k_stage      interior face fluxes of a tile in shared memory, gathered per cell in the
@@ -292,7 +292,7 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
   long long n = 2 + c->P.nfam;
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
-    long long per = (H.nrec > 0 ? 1 : 0) + (c->P.shock_detector ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
+    long long per = (H.nrec > 0 ? 1 : 0) + (c->P.shock_detector && !c->staged ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
                     (c->P.coupled && (!c->staged || sur_active(c, p)) ? 1 : 0);
     per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
     n += per * c->P.nrk;

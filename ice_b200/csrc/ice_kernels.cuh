@@ -71,6 +71,16 @@ __device__ __forceinline__ bool face_flux(const Geo& G, const FamDev& F, const D
   return bad;
 }
 
+// The Jameson weight of cell (i,j,k) of block B from the stage's density in global memory (the
+// boundary kernels; compute_beta, Mod_Fluxes.f90:366-389).
+template <typename R>
+__device__ __forceinline__ R beta_cell(const FamDev& F, const DBlock& B, int i, int j, int k) {
+  const double* P = F.Up;
+  return sd_rho<R>((R)P[gidx(B, i, j, k)], (R)P[gidx(B, i - 1, j, k)], (R)P[gidx(B, i + 1, j, k)],
+                   (R)P[gidx(B, i, j - 1, k)], (R)P[gidx(B, i, j + 1, k)],
+                   (R)P[gidx(B, i, j, k - 1)], (R)P[gidx(B, i, j, k + 1)]);
+}
+
 // record_flux (Mod_BC_Fluxes.f90:180-272): the flux through a record's face into its cell. R is the
 // reconstruction and Riemann type (double in the plain form, float in the FP32-flux form); LIM the
 // limiter the kernel is specialised for (the same formulas as the run-time switch in double).
@@ -84,7 +94,7 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
   int ig2 = i - 2 * g0, jg2 = j - 2 * g1, kg2 = k - 2 * g2;
   int ip = i + g0, jp = j + g1, kp = k + g2;
   int dir = (f + 1) / 2 - 1;
-  R bv = (R)(beta_face ? *beta_face : (F.beta ? F.beta[iidx(B, i, j, k)] : 1.0));
+  R bv = beta_face ? (R)*beta_face : (F.sd ? beta_cell<R>(F, B, i, j, k) : (R)1);
   R dl_g1 = (R)G.dl[(long long)dir * G.NR + ridx(B, ig, jg, kg)];
   R dl_m = (R)G.dl[(long long)dir * G.NR + ridx(B, i, j, k)];
   R dl_4 = (R)G.dl[(long long)dir * G.NR + ridx(B, ip, jp, kp)];
@@ -394,12 +404,12 @@ __global__ void __launch_bounds__(128, 4) k_conn(Geo G, FamDev F, const DRec* re
   if (n >= nown) return;
   constexpr int nc = NC<CL>::v;
   const DRec& r = recs[own[n]];
-  double bo = 1.0, bq = 1.0;
-  if (F.beta) {
-    bo = F.beta[iidx(G.blk[r.b], r.i, r.j, r.k)];
-    bq = F.beta[iidx(G.blk[r.pb], r.pi, r.pj, r.pk)];
+  R bo = (R)1, bq = (R)1;
+  if (F.sd) {
+    bo = beta_cell<R>(F, G.blk[r.b], r.i, r.j, r.k);
+    bq = beta_cell<R>(F, G.blk[r.pb], r.pi, r.pj, r.pk);
   }
-  double bf = mn(bo, bq);
+  const double bf = (double)mn(bo, bq);
   double fl[nc];
   if (record_flux<CL, RS, LIM, R>(G, F, r, fl, &bf)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_BAD_RECON);
 #pragma unroll
@@ -666,7 +676,7 @@ __global__ void k_beta(Geo G, FamDev F) {
   const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
   int i, j, k; decode(B, q, i, j, k);
   const double* P = F.Up;   // variable 0: density
-  F.betaw[q] = sd_rho(P[gidx(B, i, j, k)], P[gidx(B, i - 1, j, k)], P[gidx(B, i + 1, j, k)],
+  F.betaw[q] = sd_rho<double>(P[gidx(B, i, j, k)], P[gidx(B, i - 1, j, k)], P[gidx(B, i + 1, j, k)],
                       P[gidx(B, i, j - 1, k)], P[gidx(B, i, j + 1, k)],
                       P[gidx(B, i, j, k - 1)], P[gidx(B, i, j, k + 1)]);
 }

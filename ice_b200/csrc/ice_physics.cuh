@@ -495,16 +495,19 @@ template <int CL, int RS, typename R> __device__ __forceinline__ void riemann(co
 }
 
 // ------------------------------------------------------------------ sensor
-__device__ __forceinline__ double sd_rho(double r, double r1, double r2, double r3, double r4, double r5, double r6) {
-  double kp1 = fabs((r2 - 2.0*r + r1) / (r2 + 2.0*r + r1 + 1e-30));
-  double kp2 = fabs((r4 - 2.0*r + r3) / (r4 + 2.0*r + r3 + 1e-30));
-  double kp3 = fabs((r6 - 2.0*r + r5) / (r6 + 2.0*r + r5 + 1e-30));
-  double sw = mx(mx(kp1, kp2), kp3);
-  if (sw < 1.0/20.0) {
-    double phi = mx(sw*20.0, 0.0);
-    return 1.0 - ice_tanh(10.0*phi*phi*phi);
+// SD_rho (Lib_Shock_Detector.f90:17-42): the Jameson weight of a cell from its density and its six
+// neighbours' (r1, r2 along x, r3, r4 along y, r5, r6 along z).
+template <typename R>
+__device__ __forceinline__ R sd_rho(R r, R r1, R r2, R r3, R r4, R r5, R r6) {
+  R kp1 = fabs((r2 - (R)2*r + r1) / (r2 + (R)2*r + r1 + (R)1e-30));
+  R kp2 = fabs((r4 - (R)2*r + r3) / (r4 + (R)2*r + r3 + (R)1e-30));
+  R kp3 = fabs((r6 - (R)2*r + r5) / (r6 + (R)2*r + r5 + (R)1e-30));
+  R sw = mx(mx(kp1, kp2), kp3);
+  if (sw < (R)(1.0/20.0)) {
+    R phi = mx(sw*(R)20, (R)0);
+    return (R)1 - th((R)10*phi*phi*phi);
   }
-  return 0.0;
+  return (R)0;
 }
 
 // ------------------------------------------------------------------ drag

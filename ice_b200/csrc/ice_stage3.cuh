@@ -46,7 +46,9 @@ template <int CL, typename R> struct StageSmem {
   static constexpr size_t ring = st_align(stg + sizeof(double) * nc * P);  // R [3][nc][P]
   static constexpr size_t fx = st_align(ring + sizeof(R) * 3 * nc * P);    // R [nc][NT]
   static constexpr size_t fy = st_align(fx + sizeof(R) * nc * NT);         // R [nc][NT]
-  static constexpr size_t bar = st_align(fy + sizeof(R) * nc * NT);        // mbarrier
+  static constexpr int NB = (ST_TX + 1) * (Shape<CL>::TY + 1);              // sensor positions of a plane
+  static constexpr size_t bt = st_align(fy + sizeof(R) * nc * NT);         // R [2][NB]: beta of planes k, k+1
+  static constexpr size_t bar = st_align(bt + sizeof(R) * 2 * NB);         // mbarrier
   static constexpr size_t bytes = bar + 16 + 128;   // + the alignment of the base to 128 bytes
 };
 
@@ -118,17 +120,14 @@ template <typename S, int NP> struct SmemCell {        // c[v]: one cell of a st
 };
 
 // One interior face along d (0: x, 1: y) between the 0-based cells (i,j,k) and its upper neighbour,
-// its four-cell stencil from a staged plane (base = the position of cell c - 1): face_flux +
-// compute_flux_ (Mod_Fluxes.f90:599-685).
+// its four-cell stencil from a staged plane (base = the position of cell c - 1), bf the smaller of the
+// two cells' Jameson weights: face_flux + compute_flux_ (Mod_Fluxes.f90:599-685).
 template <int CL, int RS, int LIM, typename R>
 __device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, const DBlock& B, int d,
-                                                 int i, int j, int k, const R* P, int base, int st, R* flux) {
+                                                 int i, int j, int k, const R* P, int base, int st, R bf, R* flux) {
   constexpr int nc = NC<CL>::v;
   const int c = d == 0 ? i : j;
   const int n = d == 0 ? B.ni : B.nj;
-  const int o0 = d == 0, o1 = d == 1;
-  R bf = (R)1;
-  if (F.beta) bf = (R)mn(F.beta[iidx(B, i, j, k)], F.beta[iidx(B, i + o0, j + o1, k)]);
   const double* dl = G.dl + (long long)d * G.NR;
   const long long r0 = ridx(B, i, j, k);
   const long long rs = d == 0 ? 1LL : (long long)(B.ni + 2);
@@ -170,6 +169,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   R* ring = (R*)(smraw + L::ring);
   R* Fx = (R*)(smraw + L::fx);
   R* Fy = (R*)(smraw + L::fy);
+  R* BT = (R*)(smraw + L::bt);
   uint64_t* bar = (uint64_t*)(smraw + L::bar);
 
   const Tile t = tiles[blockIdx.x];
@@ -218,6 +218,31 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   auto stall = [&]() { if (tid == 0) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_TIMEOUT); };
   auto plane = [&](int slot) { return (const R*)(ring + slot * nc * ST_P); };
 
+  // The Jameson sensor from the staged densities (compute_beta, Mod_Fluxes.f90:366-389): the weight of
+  // the cell at column cx, row cy of the tile (0-based from the tile's first cell) on the plane of ring
+  // slot s0, with the planes below and above in slots sm and sp; in 2-D runs (no z march) the planes
+  // below and above are the ghost planes, read from global memory.
+  const int sh = t.i0 - xa;
+  auto rho_at = [&](int slot, int cx, int cy) { return plane(slot)[(cy + 2) * ST_BX + cx + 2 + sh]; };
+  auto beta_at = [&](int sm, int s0, int sp, int cx, int cy, int kc) -> R {
+    R zm, zp;
+    if (az) { zm = rho_at(sm, cx, cy); zp = rho_at(sp, cx, cy); }
+    else {
+      const long long gc = gidx(B, t.i0 + cx, t.j0 + cy, kc);
+      zm = (R)F.Up[gc - B.pxy]; zp = (R)F.Up[gc + B.pxy];
+    }
+    return sd_rho<R>(rho_at(s0, cx, cy), rho_at(s0, cx - 1, cy), rho_at(s0, cx + 1, cy),
+                     rho_at(s0, cx, cy - 1), rho_at(s0, cx, cy + 1), zm, zp);
+  };
+  // the weights of a whole plane's face cells (columns -1..ST_TX-1, rows -1..ST_TY-1) into BT[b]
+  constexpr int NBX = ST_TX + 1;
+  auto beta_plane = [&](int b, int sm, int s0, int sp, int kc) {
+    if (!F.sd) return;
+    for (int e = tid; e < L::NB; e += ST_NT) BT[b * L::NB + e] = beta_at(sm, s0, sp, e % NBX - 1, e / NBX - 1, kc);
+  };
+  auto beta_of = [&](int b, int cx, int cy) { return F.sd ? BT[b * L::NB + (cy + 1) * NBX + cx + 1] : (R)1; };
+  int bcur = 0;
+
   // z: slope of the thread's cell at plane c from three ring slots (c-1, c, c+1)
   R sz[nc], flo[nc], fhi[nc];
   R dlz = (R)0;
@@ -236,11 +261,9 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     cell_slope<CL, LIM, R>(F.limiter, q, lm, l0, lp, s, dlc, first);
   };
   // z face between c and c + 1 from the ring slots of the two cells and their slopes
-  auto zface = [&](int sl, int sr, int c, const R* sa, R da, bool fa, const R* sb, R db, bool fb, R* out) {
+  auto zface = [&](int sl, int sr, int c, const R* sa, R da, bool fa, const R* sb, R db, bool fb, R bf, R* out) {
     R pl[nc], pr[nc];
     const SmemCell<R, ST_P> ql{plane(sl), pos}, qr{plane(sr), pos};
-    R bf = (R)1;
-    if (F.beta) bf = (R)mn(F.beta[iidx(B, i, j, c)], F.beta[iidx(B, i, j, c + 1)]);
     bad |= states_from_slopes<CL, R>(ql, sa, da, fa, qr, sb, db, fb, bf, pl, pr);
     const long long fi = fidx(B, 2, i, j, c, c + 1);
     const long long NF = G.NF[2];
@@ -260,6 +283,8 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     issue(k0);
     if (!land(0)) { stall(); return; }
     cur = 0; nx1 = 1; nx2 = 2;
+    beta_plane(bcur, 0, 0, 0, k0);
+    __syncthreads();
   } else if (k0 >= 1) {
     issue(k0 - 2);
     if (!land(0)) { stall(); return; }
@@ -268,13 +293,19 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     issue(k0);
     if (!land(2)) { stall(); return; }
     R sm1[nc]; R dm1 = (R)0; bool fm1 = true;
-    if (owner) zslope(0, 1, 2, k0 - 1, sm1, dm1, fm1);
+    R bm1 = (R)1;
+    if (owner) {
+      zslope(0, 1, 2, k0 - 1, sm1, dm1, fm1);
+      if (F.sd) bm1 = beta_at(0, 1, 2, tx, ty, k0 - 1);
+    }
     issue(k0 + 1);
     __syncthreads();                            // slot 0 (plane k0-2) is read by every thread before reuse
     if (!land(0)) { stall(); return; }
+    beta_plane(bcur, 1, 2, 0, k0);
     if (owner) {
       zslope(1, 2, 0, k0, sz, dlz, fz);
-      zface(1, 2, k0 - 1, sm1, dm1, fm1, sz, dlz, fz, flo);
+      const R b0 = F.sd ? beta_at(1, 2, 0, tx, ty, k0) : (R)1;
+      zface(1, 2, k0 - 1, sm1, dm1, fm1, sz, dlz, fz, mn(bm1, b0), flo);
     }
     issue(k0 + 2);
     __syncthreads();
@@ -288,6 +319,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     issue(1);
     if (!land(2)) { stall(); return; }
     if (owner) zslope(0, 1, 2, 0, sz, dlz, fz);
+    beta_plane(bcur, 0, 1, 2, 0);
     issue(2);
     __syncthreads();
     if (!land(0)) { stall(); return; }
@@ -300,13 +332,15 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     const R* P = plane(cur);
     if (ax && col && i >= 1) {                  // x face below (i,j,k)
       R fl[nc];
-      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 0, i - 1, j, k, P, pos - 2, 1, fl);
+      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 0, i - 1, j, k, P, pos - 2, 1,
+                                              mn(beta_of(bcur, tx - 1, ty), beta_of(bcur, tx, ty)), fl);
 #pragma unroll
       for (int v = 0; v < nc; ++v) Fx[v * ST_NT + tid] = fl[v];
     }
     if (ay && col && j >= 1) {                  // y face below (i,j,k)
       R fl[nc];
-      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 1, i, j - 1, k, P, pos - 2 * ST_BX, ST_BX, fl);
+      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 1, i, j - 1, k, P, pos - 2 * ST_BX, ST_BX,
+                                              mn(beta_of(bcur, tx, ty - 1), beta_of(bcur, tx, ty)), fl);
 #pragma unroll
       for (int v = 0; v < nc; ++v) Fy[v * ST_NT + tid] = fl[v];
     }
@@ -314,8 +348,11 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     R szn[nc]; R dlzn = (R)0; bool fzn = true;
     if (az && owner && k <= B.nk - 2) {
       zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
-      zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, fhi);
+      const R b1 = F.sd ? beta_at(cur, nx1, nx2, tx, ty, k + 1) : (R)1;
+      zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), b1), fhi);
     }
+    // the next plane's weights (its planes below and above are in the ring now), read after a barrier
+    if (az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
     __syncthreads();
     if (owner) {
       const long long q = iidx(B, i, j, k);
@@ -443,6 +480,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     __syncthreads();                            // every read of Fx and Fy is done
     if (!land(cur)) { stall(); break; }         // plane k + 3 replaces plane k (read by nobody since)
     const int o = cur; cur = nx1; nx1 = nx2; nx2 = o;
+    bcur ^= 1;
 #pragma unroll
     for (int v = 0; v < nc; ++v) { flo[v] = fhi[v]; sz[v] = szn[v]; }
     dlz = dlzn; fz = fzn;
