@@ -47,7 +47,8 @@ def jets_capped(prec):
     lambda prec: configs.cloud_3d(n=32, steps=20, length=0.0032, precision=prec),
     lambda prec: configs.multiblock_tree(nblocks=6, seed=3, lo=8, hi=16, steps=20, precision=prec),
     jets_capped,
-], ids=["cloud3d", "multiblock", "jets2d"])
+    lambda prec: configs.taylor_green_ig(n=48, steps=20, precision=prec),
+], ids=["cloud3d", "multiblock", "jets2d", "taylorgreen"])
 def test_fp32_flux_form_within_1e4_l1(gpu, make):
     c32, c64 = make(abi.PREC_FP32FLUX), make(abi.PREC_FP64)
     s32, s64 = Solver(c32, gpu), Solver(c64, gpu)

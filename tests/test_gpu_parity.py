@@ -143,6 +143,20 @@ def test_jets_2d_coupled(gpu, orc):
     run_pair(gpu, orc, lambda: configs.jets_2d(n=96, steps=40), 40)
 
 
+def test_jets_2d_with_sensor(gpu, orc):
+    # the Jameson sensor in a 2-D run: the stage kernel reads the ghost planes above and below
+    def make():
+        c = configs.jets_2d(n=64, steps=60)
+        c.numerics.shock_detector = True
+        return c
+    run_pair(gpu, orc, make, 60)
+
+
+def test_taylor_green_ig(gpu, orc):
+    # the shape of the reference's published 192^3 benchmark (IG, frozen Taylor-Green gas, SSP-RK2), 32^3
+    run_pair(gpu, orc, lambda: configs.taylor_green_ig(n=32, steps=40), 40)
+
+
 def test_cloud_3d_evaporating_ag(gpu, orc):
     # config 3 shape (AG, Jameson sensor, drag, heat, radiation, evaporation LK + blowing), 24^3
     run_pair(gpu, orc, lambda: configs.cloud_3d(n=24, steps=12, length=0.0024), 12)
