@@ -330,14 +330,16 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     const bool more = k + 1 < k1;
     if (more) issue(k + 3);                     // lands at the end of this plane, into the slot of k
     const R* P = plane(cur);
-    if (ax && col && i >= 1) {                  // x face below (i,j,k)
+    // a face is computed by the thread of the cell above it when an owned cell reads it: the x faces
+    // of the last row and the y faces of the last column belong to the neighbouring tiles
+    if (ax && col && i >= 1 && (!ay || ty < ST_TY - 1)) {   // x face below (i,j,k)
       R fl[nc];
       bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 0, i - 1, j, k, P, pos - 2, 1,
                                               mn(beta_of(bcur, tx - 1, ty), beta_of(bcur, tx, ty)), fl);
 #pragma unroll
       for (int v = 0; v < nc; ++v) Fx[v * ST_NT + tid] = fl[v];
     }
-    if (ay && col && j >= 1) {                  // y face below (i,j,k)
+    if (ay && col && j >= 1 && (!ax || tx < ST_TX - 1)) {   // y face below (i,j,k)
       R fl[nc];
       bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 1, i, j - 1, k, P, pos - 2 * ST_BX, ST_BX,
                                               mn(beta_of(bcur, tx, ty - 1), beta_of(bcur, tx, ty)), fl);
@@ -477,8 +479,23 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       }
     }
     if (!more) break;
-    __syncthreads();                            // every read of Fx and Fy is done
-    if (!land(cur)) { stall(); break; }         // plane k + 3 replaces plane k (read by nobody since)
+    // plane k + 3 replaces plane k in the ring: nothing reads plane k after the barrier above, so
+    // each thread converts its share as soon as its own update is done; one barrier then both
+    // publishes the slot and agrees on a wait that gave up (the next plane's faces overwrite Fx and
+    // Fy only after it, when every owner has gathered its fluxes).
+    {
+      const bool ok = mbar_wait(bar, parity);
+      if (ok) {
+        R* dst = ring + cur * nc * ST_P;
+        for (int e = tid; e < nc * ST_P; e += ST_NT) dst[e] = (R)stg[e];
+      }
+      if (__syncthreads_or(!ok)) {
+        if (!ok) mbar_wait(bar, parity);
+        stall();
+        break;
+      }
+      parity ^= 1u;
+    }
     const int o = cur; cur = nx1; nx1 = nx2; nx2 = o;
     bcur ^= 1;
 #pragma unroll
