@@ -225,6 +225,12 @@ class Case:
     geoms: list = field(default_factory=list)
     rec_int: np.ndarray = None
     rec_real: np.ndarray = None
+    # chimera (102) rows of bc_rows: row number -> (donors of ghost layer 1, donors of layer 2), each a
+    # list of (b, i, j, k, weight) as the case's boundary file lists them (IO_BC.f90:209-236)
+    chimera: dict = field(default_factory=dict)
+    chim_n: np.ndarray = None
+    chim_donor: np.ndarray = None
+    chim_weight: np.ndarray = None
 
     @property
     def dims(self):
@@ -286,6 +292,18 @@ class Case:
                     ri[idx, 7:12] = pay[:5]
                 elif 401 <= code <= 403:
                     rr[idx, :len(pay)] = pay
+        if self.chimera:
+            cn = np.zeros((nrow * ng, 2), dtype=np.int32)
+            don, wts = [], []
+            for n in range(nrow):
+                l1, l2 = self.chimera.get(n, ((), ()))
+                for p in range(ng):
+                    cn[n * ng + p] = (len(l1), len(l2))
+                    for (b, i, j, k, w) in list(l1) + list(l2):
+                        don.append((b, i, j, k)); wts.append(w)
+            self.chim_n = cn
+            self.chim_donor = np.array(don, dtype=np.int32).reshape(-1, 4)
+            self.chim_weight = np.array(wts, dtype=np.float64)
         dims = np.array(self.dims, dtype=np.int32).reshape(-1)
         err = C.create_string_buffer(512)
         rc = lib.pair_connections(len(self.nodes), abi.ptr(dims, C.c_int32), ng, ri.shape[0],

@@ -142,6 +142,43 @@ def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
     return case
 
 
+def doisneau_chimera(data, closure="IG", steps=5000):
+    """The overlapping-grid variant of the crossing-jets case in the reference's suite (its
+    Doisneau IG-chimera case): block 1, 50 x 100 cells on [0,0.5] x [-0.5,0.5], and block 2,
+    45 x 73 cells on [0.4,1] x [-0.5,0.5], overlap by 0.1 and meet at chimera faces (102) whose
+    ghost cells blend donor cells of the other block; inlets, symmetry faces, numerics and
+    material of the crossing-jets case. `data` holds the case's tables (a mapping of arrays as
+    tests/golden/make_golden.py writes them from the case's mesh and boundary files): x<b>, y<b>,
+    z<b> the node coordinates of block b, bc the rows b i j k f code, inlet the six inlet reals of
+    each row, nchi the donors per ghost layer of each row, donor (b i j k) and weight."""
+    nodes = []
+    for b in (1, 2):
+        X, Y, Z = np.meshgrid(data[f"x{b}"], data[f"y{b}"], data[f"z{b}"], indexing="ij")
+        nodes.append(np.stack([X, Y, Z], axis=-1))
+    fam = Family(closure, rho_al=2000.0, cs_al=1500.0)
+    num = Numerics(scheme="RK2", time_accurate=False, cfl=0.8, limiter="vanleer", itermax=steps)
+    rows, chim, off = [], {}, 0
+    donor, weight = data["donor"], data["weight"]
+    for n, (r, pay, nc) in enumerate(zip(data["bc"], data["inlet"], data["nchi"])):
+        b, i, j, k, f, code = (int(x) for x in r)
+        payload = tuple(float(x) for x in pay) + (0.0, 0.0) if 401 <= code <= 403 else ()
+        rows.append((b, i, j, k, f, code, payload))
+        n1, n2 = int(nc[0]), int(nc[1])
+        if code == 102:
+            d = [tuple(int(x) for x in donor[s]) + (float(weight[s]),) for s in range(off, off + n1 + n2)]
+            chim[n] = (d[:n1], d[n1:])
+        off += n1 + n2
+    case = Case(f"doisneau_chimera_{closure}", nodes, [fam], num, rows)
+    case.chimera = chim
+    states = []
+    for nd in nodes:
+        st = empty_state(tuple(s - 1 for s in nd.shape[:3]), fam.nc)
+        st[2:-2, 2:-2, 2:-2, :] = 1e-20
+        states.append([st])
+    case.state = states
+    return case
+
+
 # ------------------------------------------------------------ config 2
 def jets_2d(n=1024, steps=500, seed=2, length=0.1, precision=0):
     """2-D single block n x n, MK and IG families advanced together (one run, two families),

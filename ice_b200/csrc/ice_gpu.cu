@@ -29,6 +29,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cstdarg>
+#include <cmath>
 #include <vector>
 #include <string>
 #include <algorithm>
@@ -82,6 +83,10 @@ struct FamHost {
   bool sur_on = false;
   int nrec = 0, nbc = 0, nown = 0, ncf = 0;
   std::vector<int> h_first, h_list, h_own;   // 0-based record numbers of the whole table
+  std::vector<int> h_grp;                    // the family's records: their numbers in the table
+  std::vector<DRec> h_recs;                  // the device records, kept to attach chimera donors
+  DevBuf<int4> cdon;                         // chimera donors (0-based block, i, j, k) and weights
+  DevBuf<double> cw;
 };
 
 
@@ -98,6 +103,8 @@ struct ice_gpu_ctx {
   bool have_gas = false;
   std::vector<bool> have_block;
   bool have_records = false;
+  int nchim = 0;          // 102 records of the table
+  bool have_chimera = true;   // their donors are set (ice_gpu_set_chimera)
   FamHost fam[kMaxF];
   std::vector<HRec> recs;
   DevBuf<Tile> tiles;
@@ -207,6 +214,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   F.bmap = H.bmap.p;
   F.Rb = H.Rb.p; F.Rbw = H.Rb.p;
   F.connF = H.connF.p;
+  F.cdon = H.cdon.p; F.cw = H.cw.p;
   F.resid = H.resid.p;
   static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
   F.rk = RKC[c->P.nrk - 1][srk - 1];
@@ -669,7 +677,8 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
         return fail(c, ICE_GPU_EINVAL, "record %d: cell %d %d %d is off its face %d", n + 1, r.i, r.j, r.k, r.f);
     }
     int t = r.type;
-    bool known = t == 0 || t == 101 || t == 201 || t == 200 || t == 300 || t == 301 || t == 400 || (t >= 401 && t <= 403);
+    bool known = t == 0 || t == 101 || t == 201 || t == 102 || t == 200 || t == 300 || t == 301 || t == 400 ||
+                 (t >= 401 && t <= 403);
     if (!known) return fail(c, ICE_GPU_EINVAL, "record %d: boundary code %d is not supported on the device", n + 1, t);
     if (t == 101 || t == 201) {
       if (r.bs < 1 || r.bs > c->nb) return fail(c, ICE_GPU_EINVAL, "record %d: source block %d", n + 1, r.bs);
@@ -710,10 +719,13 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
       d.temperature = r.temperature; d.radius = r.radius; d.gfixed = r.gfixed;
       d.ca = cos(r.alpha); d.sa = sin(r.alpha); d.cb = cos(r.beta); d.sb = sin(r.beta);
       d.vol_p = 4.0/3.0*kPi*pow(r.radius, 3.0);
+      d.cd0 = d.cn1 = d.cn2 = 0;
     }
     H.nrec = (int)grp.size();
     CK(H.recs.alloc(dr.size()));
     if (!dr.empty()) CK(cudaMemcpy(H.recs.p, dr.data(), dr.size() * sizeof(DRec), cudaMemcpyHostToDevice));
+    H.h_grp = grp;
+    H.h_recs = dr;
     // boundary cells: block by block in cell order, the records of a cell by face (stable)
     H.h_first.clear(); H.h_list.clear();
     std::vector<int> bmap(c->NI, -1);
@@ -765,7 +777,67 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
     if (!down.empty()) CK(cudaMemcpy(H.own.p, down.data(), down.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(H.connF.alloc((size_t)std::max(ncf, 1) * H.nc));
   }
+  c->nchim = 0;
+  for (const HRec& r : c->recs) c->nchim += r.type == 102;
+  c->have_chimera = c->nchim == 0;
   c->have_records = true;
+  free_graphs(c);
+  return 0;
+}
+
+// The donors of the table's chimera records (ICE_bc_type%ni, donorID, volume_fraction,
+// base/Advanced_Types_m.f90:29-31, as read_bc reads them, io/IO_BC.f90:209-236), attached to the
+// family record lists that ice_gpu_set_records built.
+int ice_gpu_set_chimera(ice_gpu_ctx* c, int32_t nrec, const int32_t* nchi, const int32_t* donor, const double* weight) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (!c->have_records) return fail(c, ICE_GPU_ENOTREADY, "set_chimera: set the boundary table first");
+  if (nrec != (int32_t)c->recs.size() || (nrec > 0 && !nchi))
+    return fail(c, ICE_GPU_EINVAL, "set_chimera: %d records given, the table has %d", nrec, (int)c->recs.size());
+  std::vector<long long> off(nrec + 1, 0);
+  for (int n = 0; n < nrec; ++n) {
+    const int n1 = nchi[2 * n], n2 = nchi[2 * n + 1];
+    if (n1 < 0 || n2 < 0) return fail(c, ICE_GPU_EINVAL, "record %d: negative donor count", n + 1);
+    if (c->recs[n].type != 102 && (n1 || n2))
+      return fail(c, ICE_GPU_EINVAL, "record %d: donors given to a record of code %d", n + 1, c->recs[n].type);
+    if (c->recs[n].type == 102 && (n1 < 1 || n2 < 1))
+      return fail(c, ICE_GPU_EINVAL, "record %d: a chimera record needs donors for both ghost layers", n + 1);
+    off[n + 1] = off[n] + n1 + n2;
+  }
+  if (off[nrec] > 0 && (!donor || !weight)) return fail(c, ICE_GPU_EINVAL, "set_chimera: null donor arrays");
+  if (off[nrec] > (1LL << 30)) return fail(c, ICE_GPU_EINVAL, "set_chimera: %lld donors", off[nrec]);
+  for (long long s = 0; s < off[nrec]; ++s) {
+    const int32_t* d = donor + 4 * s;
+    if (d[0] < 1 || d[0] > c->nb) return fail(c, ICE_GPU_EINVAL, "donor %lld: block %d", s + 1, d[0]);
+    const int* dm = &c->dims[3 * (d[0] - 1)];
+    if (d[1] < 1 || d[1] > dm[0] || d[2] < 1 || d[2] > dm[1] || d[3] < 1 || d[3] > dm[2])
+      return fail(c, ICE_GPU_EINVAL, "donor %lld: cell %d %d %d is not an interior cell of block %d", s + 1, d[1], d[2],
+                  d[3], d[0]);
+    if (!std::isfinite(weight[s])) return fail(c, ICE_GPU_EINVAL, "donor %lld: weight is not finite", s + 1);
+  }
+  for (int p = 0; p < c->P.nfam; ++p) {
+    FamHost& H = c->fam[p];
+    std::vector<int4> dn;
+    std::vector<double> dw;
+    for (size_t q = 0; q < H.h_grp.size(); ++q) {
+      const int n = H.h_grp[q];
+      DRec& d = H.h_recs[q];
+      d.cd0 = (int)dn.size(); d.cn1 = nchi[2 * n]; d.cn2 = nchi[2 * n + 1];
+      for (long long s = off[n]; s < off[n + 1]; ++s) {
+        const int32_t* x = donor + 4 * s;
+        dn.push_back(make_int4(x[0] - 1, x[1] - 1, x[2] - 1, x[3] - 1));
+        dw.push_back(weight[s]);
+      }
+    }
+    if (!H.h_recs.empty())
+      CK(cudaMemcpy(H.recs.p, H.h_recs.data(), H.h_recs.size() * sizeof(DRec), cudaMemcpyHostToDevice));
+    CK(H.cdon.alloc(std::max<size_t>(dn.size(), 1)));
+    CK(H.cw.alloc(std::max<size_t>(dw.size(), 1)));
+    if (!dn.empty()) {
+      CK(cudaMemcpy(H.cdon.p, dn.data(), dn.size() * sizeof(int4), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(H.cw.p, dw.data(), dw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  }
+  c->have_chimera = true;
   free_graphs(c);
   return 0;
 }
@@ -784,6 +856,8 @@ int ice_gpu_index_maps(const ice_gpu_ctx* c, int32_t p1, int32_t* nbcell, int32_
 static int check_ready(ice_gpu_ctx* c) {
   for (int b = 0; b < c->nb; ++b) if (!c->have_block[b]) return fail(c, ICE_GPU_ENOTREADY, "block %d has no metrics", b + 1);
   if (!c->have_records) return fail(c, ICE_GPU_ENOTREADY, "no boundary table");
+  if (!c->have_chimera)
+    return fail(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (ice_gpu_set_chimera)", c->nchim);
   if (c->P.coupled && !c->have_gas) return fail(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas");
   return 0;
 }

@@ -223,7 +223,36 @@ __device__ __forceinline__ void rec_normal(const Geo& G, const DBlock& B, const 
   if (area) *area = G.face[d][3 * NF + fi];
 }
 
-// ghost_record (Lib_Ghost.f90:76-267), every record type but 102
+// ghost_chimera (Lib_Ghost.f90:439-466): ghost cell gg (layer 1 or 2) of a chimera record from its
+// donors, the weighted sum of their conservative states in donor order, back to primitive with the
+// closure's floors. The donors are interior cells, which no ghost fill writes.
+template <int CL>
+__device__ __forceinline__ void chimera_ghost(const Geo& G, const FamDev& F, const DRec& r, int layer, long long gg) {
+  constexpr int nc = NC<CL>::v;
+  const double* P = F.Ug;
+  const long long NG = G.NG;
+  const int d0 = r.cd0 + (layer == 1 ? 0 : r.cn1), d1 = d0 + (layer == 1 ? r.cn1 : r.cn2);
+  double cs[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) cs[v] = 0.0;
+  for (int d = d0; d < d1; ++d) {
+    const int4 dn = F.cdon[d];
+    const long long gd = gidx(G.blk[dn.x], dn.y, dn.z, dn.w);
+    const double w = F.cw[d];
+    double pd[nc], cd[nc];
+#pragma unroll
+    for (int v = 0; v < nc; ++v) pd[v] = P[v * NG + gd];
+    prim2cons<CL, double>(pd, cd, F.mat.cp);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) cs[v] = cs[v] + w*cd[v];
+  }
+  double pg[nc];
+  cons2prim<CL>(cs, pg, F.mat.cp);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) F.Ug[v * NG + gg] = pg[v];
+}
+
+// ghost_record (Lib_Ghost.f90:76-267)
 template <int CL>
 __device__ __forceinline__ void ghost1_rec(const Geo& G, const FamDev& F, const DRec& r) {
   constexpr int nc = NC<CL>::v;
@@ -327,6 +356,9 @@ __device__ __forceinline__ void ghost1_rec(const Geo& G, const FamDev& F, const 
       for (int v = 0; v < nc; ++v) P[v * NG + gg] = gv[v];
       break;
     }
+    case 102:
+      chimera_ghost<CL>(G, F, r, 1, gg);
+      break;
     default: break;
   }
 }
@@ -376,6 +408,9 @@ __device__ __forceinline__ void ghost2_rec(const Geo& G, const FamDev& F, const 
       for (int v = 0; v < nc; ++v) P[v * NG + gg2] = gv[v];
       break;
     }
+    case 102:
+      chimera_ghost<CL>(G, F, r, 2, gg2);
+      break;
     default: {
 #pragma unroll
       for (int v = 0; v < nc; ++v) P[v * NG + gg2] = 3.0*P[v * NG + gg1] - 3.0*P[v * NG + gm] + P[v * NG + gp];

@@ -41,6 +41,9 @@ struct DRec {                // one boundary record, 0-based cells
   // host-computed once per record (the platform libm of the driver's host, as the
   // reference's ghost_record evaluates them): cos/sin of the inlet angles and 4/3 pi r^3
   double ca, sa, cb, sb, vol_p;
+  // chimera (102): donors cd0 .. cd0 + cn1 - 1 of ghost layer 1, then cn2 of layer 2, in the family's
+  // donor arrays (FamDev::cdon, cw)
+  int cd0, cn1, cn2;
 };
 
 struct Status {
@@ -93,6 +96,8 @@ struct FamDev {              // what the kernels of one family read
   const double* Rb;          // [nbcell][nc]
   double* Rbw;
   double* connF;             // [ncf][nc]
+  const int4* cdon;          // chimera donors: 0-based block, i, j, k
+  const double* cw;          // chimera donor weights
   double* resid;             // IRS: [v][NI]
   double rk;
   int write_tau;

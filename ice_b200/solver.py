@@ -37,6 +37,10 @@ class Solver:
                                            abi.ptr(g.vol), abi.ptr(g.dl), abi.ptr(g.M)), "set_block")
         self._check(self.lib.set_records(ctx, case.rec_int.shape[0], abi.ptr(case.rec_int, C.c_int32),
                                          abi.ptr(case.rec_real)), "set_records")
+        if case.chim_n is not None:
+            self._check(self.lib.set_chimera(ctx, case.chim_n.shape[0], abi.ptr(case.chim_n, C.c_int32),
+                                             abi.ptr(case.chim_donor, C.c_int32), abi.ptr(case.chim_weight)),
+                        "set_chimera")
         for b, gas in enumerate(case.gas):
             self._check(self.lib.set_gas(ctx, b + 1, abi.ptr(gas["prim5"]), abi.ptr(gas["R"]), abi.ptr(gas["gam"]),
                                          abi.ptr(gas["k"]), abi.ptr(gas["mu"])), "set_gas")

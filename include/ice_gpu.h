@@ -189,6 +189,17 @@ int ice_gpu_set_block(ice_gpu_ctx* ctx, int32_t b, const double* face1, const do
  * replaces: build_local_bc_index (parallel/Mod_GhostExchange.f90:103-172). */
 int ice_gpu_set_records(ice_gpu_ctx* ctx, int32_t nrec, const int32_t* rec, const double* inlet);
 
+/* The donors of the table's chimera records (code 102), after ice_gpu_set_records: for each
+ * record of the table in table order, nchi[2n] and nchi[2n+1] donors of ghost layers 1 and 2
+ * (0 and 0 unless the record is 102; at least one each if it is), then every donor in the
+ * same order, donor[4s..4s+3] = block, i, j, k (1-based, an interior cell) and weight[s].
+ * Each ghost cell is the weighted sum of its donors' conservative states (ghost_chimera,
+ * numerics/space/Lib_Ghost.f90:439-466); a step refuses to run while 102 records lack donors.
+ * replaces: the chimera payload of read_bc (io/IO_BC.f90:209-236) stored in ICE_bc_type%ni,
+ * donorID, volume_fraction (base/Advanced_Types_m.f90:29-31). */
+int ice_gpu_set_chimera(ice_gpu_ctx* ctx, int32_t nrec, const int32_t* nchi, const int32_t* donor,
+                        const double* weight);
+
 /* Frozen gas of block b: prim5 (5,ni,nj,nk) = rho u v w T, then R, gamma, k, mu (ni,nj,nk).
  * replaces: setup_gas (driver/Mod_Phase.f90:11-63). */
 int ice_gpu_set_gas(ice_gpu_ctx* ctx, int32_t b, const double* prim5, const double* R,

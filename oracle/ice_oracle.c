@@ -49,6 +49,7 @@ typedef struct {
     int b, i, j, k, f, type, p, bs, is, js, ks, fs, partner, owner, cf;
     double massflux, velocity, alpha, beta, temperature, radius, gfixed;
     int normal_dir;
+    long d0; int n1, n2;  /* chimera: donors d0 .. d0+n1-1 of ghost layer 1, then n2 of layer 2 */
 } orec;
 
 typedef struct orc_ctx {
@@ -57,6 +58,9 @@ typedef struct orc_ctx {
     oblk* blk;
     int nrec;
     orec* bc;
+    int nchim, have_chim; /* chimera records and whether their donors are set */
+    int* cdon;            /* chimera donors: block, i, j, k (1-based) */
+    double* cw;           /* their weights */
     int* grp_first;       /* nfam+1, 0-based into grp */
     int* grp;             /* records by family, table order */
     int bn[MAXF]; int* bfirst[MAXF]; int* brec[MAXF];   /* boundary cells (0-based record ids) */
@@ -151,7 +155,7 @@ int orc_destroy(orc_ctx* c) {
             free(F->dt); free(F->beta); free(F->tau); free(F->inj);
         }
     }
-    free(c->blk); free(c->bc); free(c->grp_first); free(c->grp);
+    free(c->blk); free(c->bc); free(c->grp_first); free(c->grp); free(c->cdon); free(c->cw);
     for (int p = 0; p < MAXF; ++p) { free(c->bfirst[p]); free(c->brec[p]); free(c->connF[p]); free(c->own[p]); }
     free(c->fbuf);
     free(c);
@@ -330,6 +334,9 @@ int orc_set_records(orc_ctx* c, int nrec, const int* ri, const double* rr) {
         if (r->b < 1 || r->b > c->nb || r->p < 1 || r->p > nf || r->f < 1 || r->f > 6)
             return seterr(c, ICE_GPU_EINVAL, "record %d: bad block, family or face", n + 1);
     }
+    c->nchim = 0;
+    for (int n = 0; n < nrec; ++n) { c->nchim += c->bc[n].type == 102; c->bc[n].d0 = 0; c->bc[n].n1 = c->bc[n].n2 = 0; }
+    c->have_chim = c->nchim == 0;
     /* records grouped by family, table order */
     free(c->grp_first); free(c->grp);
     c->grp_first = (int*)calloc(nf + 1, sizeof(int));
@@ -407,7 +414,64 @@ int orc_index_maps(const orc_ctx* c, int p1, int* nbcell, int* first, int* nrecs
     return 0;
 }
 
+/* The donors of the chimera records (ICE_bc_type%ni, donorID, volume_fraction;
+ * Advanced_Types_m.f90:29-31, read by IO_BC.f90:209-236), in table order. */
+int orc_set_chimera(orc_ctx* c, int nrec, const int* nchi, const int* donor, const double* weight) {
+    if (!c) return ICE_GPU_EINVAL;
+    if (nrec != c->nrec || (nrec > 0 && !nchi))
+        return seterr(c, ICE_GPU_EINVAL, "set_chimera: %d records given, the table has %d", nrec, c->nrec);
+    long tot = 0;
+    for (int n = 0; n < nrec; ++n) {
+        int n1 = nchi[2*n], n2 = nchi[2*n + 1];
+        if (n1 < 0 || n2 < 0) return seterr(c, ICE_GPU_EINVAL, "record %d: negative donor count", n + 1);
+        if (c->bc[n].type != 102 && (n1 || n2))
+            return seterr(c, ICE_GPU_EINVAL, "record %d: donors given to a record of code %d", n + 1, c->bc[n].type);
+        if (c->bc[n].type == 102 && (n1 < 1 || n2 < 1))
+            return seterr(c, ICE_GPU_EINVAL, "record %d: a chimera record needs donors for both ghost layers", n + 1);
+        tot += n1 + n2;
+    }
+    if (tot > 0 && (!donor || !weight)) return seterr(c, ICE_GPU_EINVAL, "set_chimera: null donor arrays");
+    for (long s = 0; s < tot; ++s) {
+        const int* d = donor + 4*s;
+        if (d[0] < 1 || d[0] > c->nb) return seterr(c, ICE_GPU_EINVAL, "donor %ld: block %d", s + 1, d[0]);
+        const oblk* B = &c->blk[d[0] - 1];
+        if (d[1] < 1 || d[1] > B->ni || d[2] < 1 || d[2] > B->nj || d[3] < 1 || d[3] > B->nk)
+            return seterr(c, ICE_GPU_EINVAL, "donor %ld: cell %d %d %d is not an interior cell of block %d",
+                          s + 1, d[1], d[2], d[3], d[0]);
+        if (!isfinite(weight[s])) return seterr(c, ICE_GPU_EINVAL, "donor %ld: weight is not finite", s + 1);
+    }
+    free(c->cdon); free(c->cw);
+    c->cdon = (int*)malloc(sizeof(int)*4*(tot > 0 ? tot : 1));
+    c->cw = (double*)malloc(sizeof(double)*(tot > 0 ? tot : 1));
+    if (tot > 0) { memcpy(c->cdon, donor, sizeof(int)*4*tot); memcpy(c->cw, weight, sizeof(double)*tot); }
+    long off = 0;
+    for (int n = 0; n < nrec; ++n) {
+        c->bc[n].d0 = off; c->bc[n].n1 = nchi[2*n]; c->bc[n].n2 = nchi[2*n + 1];
+        off += nchi[2*n] + nchi[2*n + 1];
+    }
+    c->have_chim = 1;
+    return 0;
+}
+
 /* ---------------------------------------------------------------- ghosts */
+/* ghost_chimera (Lib_Ghost.f90:439-466): ghost cell g of layer `layer` is the weighted sum of its
+ * donors' conservative states, in donor order, back to primitive (cons_2_prim with its floors). */
+static void ghost_chimera(orc_ctx* c, const orec* r, int layer, double* g) {
+    int pm = r->p - 1, nc = nc_of(c, pm), cl = c->P.fam[pm].closure;
+    const ice_gpu_family* m = &c->P.fam[pm];
+    long a = r->d0 + (layer == 1 ? 0 : r->n1), z = a + (layer == 1 ? r->n1 : r->n2);
+    double cs[NCM], cd[NCM];
+    for (int v = 0; v < nc; ++v) cs[v] = 0.0;
+    for (long s = a; s < z; ++s) {
+        const int* d = c->cdon + 4*s;
+        oblk* D = &c->blk[d[0] - 1];
+        const double* pd = D->fam[pm].prim + nc*CI(D, d[1], d[2], d[3]);
+        o_prim2cons(cl, pd, cd, m);
+        for (int v = 0; v < nc; ++v) cs[v] = cs[v] + c->cw[s]*cd[v];
+    }
+    o_cons2prim(cl, cs, g, m);
+}
+
 /* The face normal of a record's own face: dir(d)%f(ic,...) with ic = im - mod(fm,2) (Lib_Ghost.f90:114-123). */
 static const double* rec_face(const oblk* B, const orec* r) {
     int f = r->f;
@@ -441,7 +505,7 @@ static void injected_velocity(double speed, const orec* r, const double* inward,
     }
 }
 
-/* ghost_record (Lib_Ghost.f90:76-267) for every record type but 102 */
+/* ghost_record (Lib_Ghost.f90:76-267) */
 static void ghost_record(orc_ctx* c, const orec* r) {
     int pm = r->p - 1, nc = nc_of(c, pm), cl = c->P.fam[pm].closure, nb = o_nbase(cl);
     oblk* B = &c->blk[r->b - 1];
@@ -472,6 +536,9 @@ static void ghost_record(orc_ctx* c, const orec* r) {
     }
     case 0: case 400:
         for (int v = 0; v < nc; ++v) g[v] = m[v];
+        break;
+    case 102:
+        ghost_chimera(c, r, 1, g);
         break;
     case 401: case 402: case 403: {
         const double* N = rec_face(B, r);
@@ -564,6 +631,9 @@ static void second_ghost_record(orc_ctx* c, const orec* r) {
         }
         break;
     }
+    case 102:
+        ghost_chimera(c, r, 2, g2);
+        break;
     default:
         for (int v = 0; v < nc; ++v) g2[v] = 3.0*g1[v] - 3.0*m[v] + mp[v];
         break;
@@ -977,6 +1047,8 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
 
 int orc_step(orc_ctx* c, int nsteps, ice_gpu_step_out* out) {
     int rc = 0;
+    if (c->nchim > 0 && !c->have_chim)
+        return seterr(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (set_chimera)", c->nchim);
     for (int s = 0; s < nsteps && !rc; ++s) rc = explicit_step(c, out);
     if (out) {
         out->dtglobal = c->dtglobal; out->time = c->time; out->iter = c->iter;

@@ -9,6 +9,13 @@ boundary table of the case (test/Doisneau/<closure>/INPUT/part-bc.txt) reduced t
 row per record: b i j k f code [alpha] -- so that the test can check the case it builds
 against the reference's inputs before comparing fields.
 
+chimera_IG.npz: the reference's overlapping-grid variant of the IG case (test/Doisneau/IG-chimera):
+the node coordinates of its two blocks (tensor-product meshes: x, y, z per block, MESH/mesh.tec), its
+boundary table (INPUT/part-bc.txt: b i j k f code per row, the six inlet reals of each 402 row, and
+the donors of each 102 row: counts per ghost layer, then b i j k and weight per donor) and the bulk
+density the reference's binary wrote after 5000 iterations (reference/part-field.tec), per block in
+(j, i) order.
+
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
 import re
@@ -51,6 +58,68 @@ def read_bc(path):
     return np.array(rows)
 
 
+def tec_zones(path):
+    """(I, J, K, values) of every zone of a Tecplot ASCII block-packed file."""
+    lines = Path(path).read_text().split("\n")
+    heads = [i for i, l in enumerate(lines) if re.match(r"\s*ZONE\b", l)]
+    out = []
+    for a, z in enumerate(heads):
+        end = heads[a + 1] if a + 1 < len(heads) else len(lines)
+        hdr, vals = lines[z], []
+        for l in lines[z + 1:end]:
+            if re.search(r"[A-DF-Za-df-z]", l):       # header continuation lines (I=, DATAPACKING=, ...)
+                hdr += " " + l
+                continue
+            vals += [float(t) for t in l.split()]
+        g = lambda k: int(re.search(r"\b%s\s*=\s*(\d+)" % k, hdr).group(1))
+        out.append((g("I"), g("J"), g("K"), np.array(vals)))
+    return out
+
+
+def read_chimera_bc(path):
+    """Rows b i j k f code; the six inlet reals of 402/401/403 rows; the donors of 102 rows."""
+    lines = [l for l in Path(path).read_text().split("\n") if l.strip()]
+    rows, pay, cn, don, wts = [], [], [], [], []
+    q = 0
+    while q < len(lines):
+        b, i, j, k, f, code = map(int, lines[q].split())
+        q += 1
+        p6 = [0.0] * 6
+        n12 = [0, 0]
+        if 401 <= code <= 403:
+            p6 = [float(t) for t in lines[q].split()[:6]]
+            q += 1
+        elif code in (101, 201):
+            q += 1
+        elif code == 102:
+            n12 = [int(t) for t in lines[q].split()[:2]]
+            q += 1
+            for _ in range(sum(n12)):
+                t = lines[q].split()
+                don.append([int(x) for x in t[:4]]); wts.append(float(t[4]))
+                q += 1
+        rows.append((b, i, j, k, f, code)); pay.append(p6); cn.append(n12)
+    return (np.array(rows, dtype=np.int32), np.array(pay), np.array(cn, dtype=np.int32),
+            np.array(don, dtype=np.int32).reshape(-1, 4), np.array(wts))
+
+
+def chimera(ref):
+    case = ref / "test" / "Doisneau" / "IG-chimera"
+    out = {}
+    for b, (I, J, K, v) in enumerate(tec_zones(case / "MESH" / "mesh.tec"), start=1):
+        N = I * J * K
+        x, y, z = (v[a * N:(a + 1) * N].reshape(K, J, I) for a in range(3))
+        assert np.all(x == x[:1, :1, :]) and np.all(y == y[:1, :, :1]) and np.all(z == z[:, :1, :1])
+        out[f"x{b}"], out[f"y{b}"], out[f"z{b}"] = x[0, 0, :], y[0, :, 0], z[:, 0, 0]
+    for b, (I, J, K, v) in enumerate(tec_zones(case / "reference" / "part-field.tec"), start=1):
+        Nn, Nc = I * J * K, (I - 1) * (J - 1) * max(K - 1, 1)
+        out[f"rho{b}"] = v[3 * Nn:3 * Nn + Nc].reshape(J - 1, I - 1)
+    rows, pay, cn, don, wts = read_chimera_bc(case / "INPUT" / "part-bc.txt")
+    out.update(bc=rows, inlet=pay, nchi=cn, donor=don, weight=wts)
+    np.savez_compressed(HERE / "chimera_IG.npz", **out)
+    print("chimera_IG", rows.shape, don.shape, out["rho1"].shape, out["rho2"].shape)
+
+
 def main(ref):
     ref = Path(ref)
     for cl in ("MK", "IG", "AG"):
@@ -59,6 +128,7 @@ def main(ref):
         bc = read_bc(case / "INPUT" / "part-bc.txt")
         np.savez_compressed(HERE / f"crossing_jets_{cl}.npz", field=field, bc=bc)
         print(cl, field.shape, bc.shape)
+    chimera(ref)
 
 
 if __name__ == "__main__":

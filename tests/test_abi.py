@@ -104,3 +104,35 @@ def test_create_refuses_saurel_for_gaussian_closures(gpu_lib):
     rc = gpu_lib.create(C.byref(P), 1, abi.ptr(dims, C.c_int32), C.byref(ctx))
     assert rc == abi.EINVAL
     assert "Saurel" in gpu_lib.error(None)
+
+
+def test_chimera_donors_are_checked(orc):
+    """ice_gpu_set_chimera refuses donors given to other records, a chimera record without donors
+    for a layer, and a donor outside its block's interior; a step refuses to run before the
+    donors are set (through the oracle, which shares the ABI)."""
+    from ice_b200.solver import Solver, SolveError
+    g = dict(np.load(ROOT / "tests" / "golden" / "chimera_IG.npz"))
+    case = configs.doisneau_chimera(g, steps=2)
+    chim = case.chimera
+    case.chimera = {}
+    s = Solver(case, orc)
+    with pytest.raises(SolveError, match="no donors"):
+        s.step(1)
+    case.chimera = chim
+    case.build_records(orc)
+    n = case.chim_n.copy()
+    first = int(np.flatnonzero(n[:, 0])[0])
+    other = int(np.flatnonzero(n[:, 0] == 0)[0])
+
+    def call(nchi, donor, weight):
+        return orc.set_chimera(s.ctx, nchi.shape[0], abi.ptr(nchi, C.c_int32), abi.ptr(donor, C.c_int32),
+                               abi.ptr(weight))
+
+    bad = n.copy(); bad[other] = (1, 1)
+    assert call(bad, case.chim_donor, case.chim_weight) == abi.EINVAL
+    bad = n.copy(); bad[first, 1] = 0
+    assert call(bad, case.chim_donor, case.chim_weight) == abi.EINVAL
+    d = case.chim_donor.copy(); d[0, 1] = 0
+    assert call(n, d, case.chim_weight) == abi.EINVAL
+    assert call(n, case.chim_donor, case.chim_weight) == abi.OK
+    assert s.step(2).status == 0

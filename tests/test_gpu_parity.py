@@ -96,6 +96,28 @@ def test_crossing_jets_matches_reference_output(gpu):
     assert l2 <= 1e-12
 
 
+def _chimera(steps):
+    from pathlib import Path
+    g = dict(np.load(Path(__file__).resolve().parent / "golden" / "chimera_IG.npz"))
+    return g, configs.doisneau_chimera(g, steps=steps)
+
+
+def test_chimera_bit_exact(gpu, orc):
+    # two overlapping blocks joined by chimera faces (102): ghost cells blended from donor cells
+    run_pair(gpu, orc, lambda: _chimera(400)[1], 400, exact=True)
+
+
+def test_chimera_matches_reference_output(gpu):
+    """The CUDA path against the density the reference's own binary wrote on its chimera case."""
+    g, case = _chimera(5000)
+    s = Solver(case, gpu)
+    s.step(5000)
+    for b in range(2):
+        p = s.download(b, 0)[2, 2:-2, 2:-2, 0]
+        l2 = float(np.sqrt(np.mean((p - g[f"rho{b + 1}"]) ** 2)))
+        assert l2 <= 1e-12, (b, l2)
+
+
 def _irs(case):
     case.numerics.irs = True
     case.numerics.irs_beta = 0.5

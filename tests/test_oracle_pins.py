@@ -4,6 +4,8 @@
   its crossing-jets validation cases (tests/golden/crossing_jets_*.npz, made by
   tests/golden/make_golden.py). The reference's gate is L2(rho) <= 1e-4; the oracle is held
   to 1e-12.
+- test/Doisneau/IG-chimera: the overlapping-grid variant (two blocks joined by chimera faces,
+  102), its density after 5000 iterations (tests/golden/chimera_IG.npz); same gates.
 - test/unit/test_muscl_bounds.f90 B1-B5: the bounds of the limited slopes.
 """
 import math
@@ -18,6 +20,25 @@ from ice_b200.solver import Solver
 GOLDEN = Path(__file__).resolve().parent / "golden"
 ZERO_AT_NEG = ["vanleer", "mc", "superbee", "koren", "umist", "osher", "sweby", "minmod"]
 ALL_LIM = ZERO_AT_NEG + ["vanalbada", "ospre"]
+
+
+@pytest.mark.slow
+def test_chimera_matches_reference_output(orc):
+    g = dict(np.load(GOLDEN / "chimera_IG.npz"))
+    case = configs.doisneau_chimera(g)
+    # every chimera row of the reference's table carries its donors, with weights summing to 1 per layer
+    assert len(case.chimera) == int(np.sum(g["bc"][:, 5] == 102)) > 0
+    for l1, l2 in case.chimera.values():
+        for layer in (l1, l2):
+            assert abs(sum(w for *_, w in layer) - 1.0) < 1e-6
+    s = Solver(case, orc)
+    out = s.step(5000)
+    assert out.status == 0 and out.iter == 5000
+    for b in range(2):
+        p = s.download(b, 0)[2, 2:-2, 2:-2, 0]       # (j, i)
+        l2 = math.sqrt(float(np.mean((p - g[f"rho{b + 1}"]) ** 2)))
+        assert l2 <= 1e-4                            # the reference's own gate
+        assert l2 <= 1e-12, (b, l2)
 
 
 @pytest.mark.slow
