@@ -88,9 +88,10 @@ def sample_workload(name: str):
 def algorithmic_bytes(case) -> float:
     """Bytes one launch of the stage kernel must move per cell, averaged over the families and the RK
     stages: read U_(k-1) and U_0 and write U_k (24 nc, FP64 state); per direction the face normal and
-    area (32) and the cell length (8); the volume (8); the boundary map (4); the sensor weight (8) when
-    the shock detector is on; in a coupled run the nine frozen-gas values the source reads (72) and
-    the relaxation time it writes on the last stage (8 / nrk); the local dt (8) in steady mode."""
+    area (32) and the cell length (8); the volume (8); the boundary map (4); in a coupled run the nine
+    frozen-gas values the source reads (72) and the relaxation time it writes on the last stage
+    (8 / nrk); the local dt (8) in steady mode; in 1-D runs the sensor weight (8) when the shock
+    detector is on (2-D and 3-D runs evaluate it from the staged density)."""
     ndir = case.ndir
     nrk = case.params().nrk
     per = []
@@ -98,12 +99,27 @@ def algorithmic_bytes(case) -> float:
         b = 24 * f.nc + 40 * ndir + 8 + 4
         if case.numerics.coupled:
             b += 72 + 8 / nrk
-        if case.numerics.shock_detector:
+        if case.numerics.shock_detector and ndir == 1:
             b += 8
         if not case.numerics.time_accurate:
             b += 8
         per.append(b)
     return float(np.mean(per))
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one stage-kernel launch, from an
+# ncu capture of the 4-block case of the 48-block tree in the chosen form (second RK stage of each
+# family, 3,714,802 cells). The 48-block case is the same recipe with the same tile shapes, so its
+# launches move the same bytes per cell: traffic per launch = these x its cells.
+DRAM_BYTES_PER_CELL = {"MK": 393.97, "IG": 458.15, "AG": 626.42}
+
+
+def dram_traffic(case, workload: str, precision: int):
+    """Measured DRAM bytes of one stage-kernel launch of the workload (mean over its families), where a
+    capture of the same recipe and form exists; None otherwise."""
+    if not workload.startswith("multiblock") or precision != abi.PREC_FP32FLUX:
+        return None
+    return float(np.mean([DRAM_BYTES_PER_CELL[f.closure] for f in case.families])) * case.ncells
 
 
 class Clocks:
@@ -383,9 +399,12 @@ def run_ours(args, rank, world, dist):
         bpc = algorithmic_bytes(case)
         achieved = bpc * cells / (stage_ms * 1e-3) / 1e9
         peak, peak_kind = peaks()
+        traffic = dram_traffic(case, args.workload, prec)
         extra = {
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "k_stage3", "bytes_per_cell": bpc,
+                         "traffic": traffic, "traffic_unit": "bytes per launch (ncu DRAM read + write)",
+                         "algorithmic_bytes_per_launch": bpc * cells,
+                         "kernel": "k_stage3", "bytes_per_cell": bpc,
                          "launch_ms": stage_ms,
                          "note": f"peak of {peak_kind}; achieved = algorithmic bytes per launch / mean CUDA-event "
                                  f"duration of the stage kernel's launches"},

@@ -41,7 +41,8 @@ module ice_gpu
     real(c_double)     :: device_ms
   end type ice_gpu_step_out_t
 
-  public :: ice_gpu_create, ice_gpu_set_block, ice_gpu_set_records, ice_gpu_set_gas, ice_gpu_upload_state, &
+  public :: ice_gpu_create, ice_gpu_set_block, ice_gpu_set_records, ice_gpu_set_chimera, ice_gpu_set_gas, &
+            ice_gpu_upload_state, &
             ice_gpu_download_state, ice_gpu_set_time, ice_gpu_step, ice_gpu_residual_norm, ice_gpu_update_params, &
             ice_gpu_last_error, ice_gpu_destroy, ice_gpu_pair_connections
 
@@ -67,6 +68,15 @@ module ice_gpu
       integer(c_int32_t), value      :: nrec
       integer(c_int32_t), intent(in) :: rec(*)
       real(c_double), intent(in)     :: inlet(*)
+    end function
+
+    integer(c_int) function ice_gpu_set_chimera(ctx, nrec, nchi, donor, weight) bind(C, name='ice_gpu_set_chimera')
+      import :: c_int, c_int32_t, c_double, c_ptr
+      type(c_ptr), value             :: ctx
+      integer(c_int32_t), value      :: nrec
+      integer(c_int32_t), intent(in) :: nchi(*)
+      integer(c_int32_t), intent(in) :: donor(*)
+      real(c_double), intent(in)     :: weight(*)
     end function
 
     integer(c_int) function ice_gpu_set_gas(ctx, b, prim5, R, gam, k, mu) bind(C, name='ice_gpu_set_gas')
