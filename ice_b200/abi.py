@@ -104,6 +104,7 @@ _SIGNATURES = [
     ("index_maps", C.c_int, [_vp, C.c_int32, _ip, _ip, _ip, _ip, _ip, _ip]),
 ]
 GPU_ONLY = [
+    ("step_host", C.c_int, [_vp, C.c_int32, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(StepOut)]),
     ("set_profiling", C.c_int, [_vp, C.c_int32]),
     ("kernel_times", C.c_int, [_vp, _dp, C.c_int32, C.POINTER(C.c_int64)]),
     ("residual_sq_noalloc", C.c_int, [_vp, _vp, C.c_int32, C.c_int32, _ip, _dp, _vp, C.c_char_p, C.c_int32]),

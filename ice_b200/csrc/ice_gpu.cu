@@ -34,6 +34,8 @@
 #include <string>
 #include <algorithm>
 #include <memory>
+#include <queue>
+#include <functional>
 #include "ice_kernels.cuh"
 #include "ice_stage3.cuh"
 #include "ice_mlp.cuh"
@@ -117,6 +119,13 @@ struct ice_gpu_ctx {
   DevBuf<Status> st;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  // ice_gpu_step_host: the step cut into its dt part and one graph per family (per buffer phase), two
+  // copy streams, the caller's arrays staged in one device buffer, one event per family
+  cudaGraphExec_t graph_pre[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t graph_fam[3][kMaxF] = {};
+  cudaStream_t s_up = nullptr, s_down = nullptr;
+  cudaEvent_t ev_up = nullptr, ev_fam[kMaxF] = {};
+  DevBuf<double> xall;
   int phase = 0;          // buffer holding the current state
   int prev_phase = -1;    // buffer holding the state before the last step
   bool profiling = false;
@@ -176,6 +185,8 @@ static int nbase_of(int cl) { return cl == ICE_CLOSURE_MK ? 6 : cl == ICE_CLOSUR
 
 static void free_graphs(ice_gpu_ctx* c) {
   for (auto& g : c->graph) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& g : c->graph_pre) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& row : c->graph_fam) for (auto& g : row) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 // The surrogate source runs for family p: on, trained, a coupled run in the FP32-flux form.
@@ -276,14 +287,23 @@ static int next_phase(const ice_gpu_ctx* c, int phase) {
   return c->P.nrk == 2 ? (phase + 2) % 3 : (phase + 1) % 3;
 }
 
-// One Explicit_Step on stream s starting from buffer `phase`.
-static void enqueue_step(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*tick)(void*, int, cudaStream_t)) {
+// One Explicit_Step on stream s starting from buffer `phase`: the step's dt over every family, then
+// each family's RK stages (the families are independent of one another within a step).
+static void enqueue_step_dt(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*tick)(void*, int, cudaStream_t)) {
   k_begin<<<1, 1, 0, s>>>(c->st.p);
   for (int p = 0; p < c->P.nfam; ++p) launch_dt(c, p, phase, s);
   k_time<<<1, 1, 0, s>>>(c->st.p, c->P.time_accurate);
   if (tick) tick(c, KC_DT, s);
-  for (int p = 0; p < c->P.nfam; ++p)
-    for (int srk = 1; srk <= c->P.nrk; ++srk) launch_family(c, p, srk, phase, s, tick);
+}
+
+static void enqueue_step_family(ice_gpu_ctx* c, int p, int phase, cudaStream_t s,
+                                void (*tick)(void*, int, cudaStream_t)) {
+  for (int srk = 1; srk <= c->P.nrk; ++srk) launch_family(c, p, srk, phase, s, tick);
+}
+
+static void enqueue_step(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*tick)(void*, int, cudaStream_t)) {
+  enqueue_step_dt(c, phase, s, tick);
+  for (int p = 0; p < c->P.nfam; ++p) enqueue_step_family(c, p, phase, s, tick);
 }
 
 static void prof_tick(void* vc, int cls, cudaStream_t s) {
@@ -321,6 +341,39 @@ static void tile_shape(int ndir, int& TX, int& TY, int& KZ) {
   }
 }
 
+// The chunk height of the staged kernel's tiles for one closure: of a few candidates up to ST_KZ
+// planes, the one whose tiles, handed longest first to the least-loaded of the GPU's resident CTA
+// slots (as the block scheduler hands them out), finish soonest; a tile costs its planes plus the
+// three its prologue loads. Small grids get shorter chunks and more tiles, so that the last wave is
+// not left half empty; large ones keep ST_KZ (a change must gain more than 1 %).
+static int choose_kz(const ice_gpu_ctx* c, int closure, int slots) {
+  static const int cand[] = {ST_KZ, 28, 24, 20, 16, 12, 8};
+  int best = ST_KZ;
+  double best_t = 0.0;
+  for (int kz : cand) {
+    std::vector<int> cost;
+    for (int b = 0; b < c->nb; ++b) {
+      int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
+      int sx = ni >= 2 ? ST_TX - 1 : 1, sy = nj >= 2 ? st_ty(closure) - 1 : 1;
+      long long ncol = (long long)((ni + sx - 1) / sx) * ((nj + sy - 1) / sy);
+      int nch = (nk + kz - 1) / kz, base = nk / nch, extra = nk % nch;
+      for (int ch = 0; ch < nch; ++ch)
+        for (long long q = 0; q < ncol; ++q) cost.push_back(base + (ch < extra ? 1 : 0) + 3);
+    }
+    std::sort(cost.begin(), cost.end(), std::greater<int>());
+    std::priority_queue<long long, std::vector<long long>, std::greater<long long>> load;
+    for (int q = 0; q < slots; ++q) load.push(0);
+    long long span = 0;
+    for (int x : cost) {
+      long long l = load.top() + x;
+      load.pop(); load.push(l);
+      span = std::max(span, l);
+    }
+    if (kz == ST_KZ || (double)span < 0.99 * best_t) { best = kz; best_t = (double)span; }
+  }
+  return best;
+}
+
 static int build_tiles(ice_gpu_ctx* c) {
   tile_shape(c->P.ndir, c->TX, c->TY, c->KZ);
   std::vector<Tile> t;
@@ -337,15 +390,23 @@ static int build_tiles(ice_gpu_ctx* c) {
     CK(cudaMemcpy(c->tiles.p, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
   } else {
     // the staged kernel: column tiles of (ST_TX - 1) x (TY - 1) cells (TY of the family's closure),
-    // each block's height cut into equal chunks of at most ST_KZ planes; the longest chunks first
+    // each block's height cut into equal chunks of at most kz planes (choose_kz); the longest first
     c->staged = true;
+    int nsm = 148;
+    {
+      int dev = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int slots = nsm * (c->P.precision == ICE_PREC_FP32FLUX ? 2 : 1);   // the kernel's launch bounds
     for (int p = 0; p < c->P.nfam; ++p) {
       FamHost& H = c->fam[p];
       t.clear();
+      const int kz = choose_kz(c, H.closure, slots);
       for (int b = 0; b < c->nb; ++b) {
         int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
         int sx = ni >= 2 ? ST_TX - 1 : 1, sy = nj >= 2 ? st_ty(H.closure) - 1 : 1;
-        int nch = (nk + ST_KZ - 1) / ST_KZ, base = nk / nch, extra = nk % nch;
+        int nch = (nk + kz - 1) / kz, base = nk / nch, extra = nk % nch;
         for (int ch = 0, k = 0; ch < nch; ++ch) {
           int h = base + (ch < extra ? 1 : 0);
           for (int j = 0; j < nj; j += sy)
@@ -510,6 +571,10 @@ int ice_gpu_destroy(ice_gpu_ctx* c) {
   free_graphs(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->s_up) { cudaStreamSynchronize(c->s_up); cudaStreamDestroy(c->s_up); }
+  if (c->s_down) { cudaStreamSynchronize(c->s_down); cudaStreamDestroy(c->s_down); }
+  if (c->ev_up) cudaEventDestroy(c->ev_up);
+  for (auto& e : c->ev_fam) if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -862,6 +927,8 @@ static int check_ready(ice_gpu_ctx* c) {
   return 0;
 }
 
+static int finish_step(ice_gpu_ctx* c, ice_gpu_step_out* out, float dms);
+
 int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
   if (!c) return ICE_GPU_EINVAL;
   if (int rc = check_ready(c)) return rc;
@@ -899,6 +966,11 @@ int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
   float dms = 0.f;
   CK(cudaEventElapsedTime(&dms, t0, t1));
   cudaEventDestroy(t0); cudaEventDestroy(t1);
+  return finish_step(c, out, dms);
+}
+
+// The step's report from the device status (after the stream has drained).
+static int finish_step(ice_gpu_ctx* c, ice_gpu_step_out* out, float dms) {
   CK(cudaGetLastError());
   Status h;
   CK(cudaMemcpy(&h, c->st.p, sizeof h, cudaMemcpyDeviceToHost));
@@ -917,6 +989,121 @@ int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
               "invalid state after the update (NaN or infinity)" : "unphysical state at first order on a face");
   }
   return rc;
+}
+
+// ice_gpu_step with the state on the host: upload every block and family, nsteps steps, download.
+// The uploads run on their own stream into one staging buffer (converted to the pools as each
+// block lands); the step waits for them (its dt is a minimum over every family); the last step runs
+// one graph per family, converts each family's new state as soon as its own stages end, and its
+// download runs on a third stream under the next family's stages. The largest families step first,
+// so that the download left after the last stage is the smallest.
+int ice_gpu_step_host(ice_gpu_ctx* c, int32_t nsteps, const double* const* prim_in, double* const* prim_out,
+                      ice_gpu_step_out* out) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (int rc = check_ready(c)) return rc;
+  if (nsteps < 1) return fail(c, ICE_GPU_EINVAL, "step_host: nsteps %d", nsteps);
+  if (!prim_in || !prim_out) return fail(c, ICE_GPU_EINVAL, "step_host: null array list");
+  const int nf = c->P.nfam;
+  for (int q = 0; q < c->nb * nf; ++q)
+    if (!prim_in[q] || !prim_out[q]) return fail(c, ICE_GPU_EINVAL, "step_host: null array for block %d family %d",
+                                                 q / nf + 1, q % nf + 1);
+  if (c->profiling) {                 // per-class timing: the plain calls, one after another
+    for (int b = 0; b < c->nb; ++b)
+      for (int p = 0; p < nf; ++p)
+        if (int rc = ice_gpu_upload_state(c, b + 1, p + 1, prim_in[b * nf + p], nullptr)) return rc;
+    if (int rc = ice_gpu_step(c, nsteps, out)) return rc;
+    for (int b = 0; b < c->nb; ++b)
+      for (int p = 0; p < nf; ++p)
+        if (int rc = ice_gpu_download_state(c, b + 1, p + 1, prim_out[b * nf + p])) return rc;
+    return 0;
+  }
+  // staging offsets: block-major, family within
+  std::vector<long long> off((size_t)c->nb * nf + 1, 0);
+  for (int b = 0; b < c->nb; ++b) {
+    const DBlock& B = c->hblk[b];
+    const long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
+    for (int p = 0; p < nf; ++p) off[(size_t)b * nf + p + 1] = off[(size_t)b * nf + p] + ng * c->fam[p].nc;
+  }
+  if (c->xall.n < (size_t)off.back()) CK(c->xall.alloc((size_t)off.back()));
+  if (!c->s_up) CK(cudaStreamCreateWithFlags(&c->s_up, cudaStreamNonBlocking));
+  if (!c->s_down) CK(cudaStreamCreateWithFlags(&c->s_down, cudaStreamNonBlocking));
+  if (!c->ev_up) CK(cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming));
+  for (int p = 0; p < nf; ++p) if (!c->ev_fam[p]) CK(cudaEventCreateWithFlags(&c->ev_fam[p], cudaEventDisableTiming));
+  cudaStream_t s = c->stream;
+  CK(cudaStreamSynchronize(s));
+  // families by size, largest first (their order within a step does not change any result)
+  std::vector<int> order(nf);
+  for (int p = 0; p < nf; ++p) order[p] = p;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return c->fam[a].nc > c->fam[b].nc; });
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  CK(cudaEventCreate(&t0)); CK(cudaEventCreate(&t1));
+  CK(cudaEventRecord(t0, c->s_up));
+  const int ph0 = c->phase;
+  for (int p : order)
+    for (int b = 0; b < c->nb; ++b) {
+      const DBlock& B = c->hblk[b];
+      const FamHost& H = c->fam[p];
+      const long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
+      double* x = c->xall.p + off[(size_t)b * nf + p];
+      CK(cudaMemcpyAsync(x, prim_in[b * nf + p], (size_t)ng * H.nc * sizeof(double), cudaMemcpyHostToDevice, c->s_up));
+      k_aos2soa<<<grid_of(ng), 256, 0, c->s_up>>>(x, H.S[ph0].p + B.goff, c->NG, ng, H.nc, B.ni + 4, B.nj + 4, B.px);
+      CK(cudaGetLastError());
+    }
+  CK(cudaEventRecord(c->ev_up, c->s_up));
+  CK(cudaStreamWaitEvent(s, c->ev_up, 0));
+  for (int n = 0; n < nsteps; ++n) {
+    const int ph = c->phase;
+    if (!c->graph_pre[ph]) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      enqueue_step_dt(c, ph, s, nullptr);
+      CK(cudaStreamEndCapture(s, &g));
+      CK(cudaGraphInstantiate(&c->graph_pre[ph], g, 0));
+      cudaGraphDestroy(g);
+    }
+    CK(cudaGraphLaunch(c->graph_pre[ph], s));
+    const int phn = next_phase(c, ph);
+    for (int p : order) {
+      if (!c->graph_fam[ph][p]) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue_step_family(c, p, ph, s, nullptr);
+        CK(cudaStreamEndCapture(s, &g));
+        CK(cudaGraphInstantiate(&c->graph_fam[ph][p], g, 0));
+        cudaGraphDestroy(g);
+      }
+      CK(cudaGraphLaunch(c->graph_fam[ph][p], s));
+      if (n + 1 < nsteps) continue;
+      // the family's new state is final: converted to the caller's layout in order on the step's stream
+      // (a conversion kernel beside the stage kernels would wait for SM room), then downloaded on the
+      // copy stream beside the next family's stages
+      const FamHost& H = c->fam[p];
+      for (int b = 0; b < c->nb; ++b) {
+        const DBlock& B = c->hblk[b];
+        const long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
+        double* x = c->xall.p + off[(size_t)b * nf + p];
+        k_soa2aos<<<grid_of(ng), 256, 0, s>>>(H.S[phn].p + B.goff, x, c->NG, ng, H.nc, B.ni + 4, B.nj + 4, B.px);
+        CK(cudaGetLastError());
+      }
+      CK(cudaEventRecord(c->ev_fam[p], s));
+      CK(cudaStreamWaitEvent(c->s_down, c->ev_fam[p], 0));
+      for (int b = 0; b < c->nb; ++b) {
+        const DBlock& B = c->hblk[b];
+        const long long ng = (long long)(B.ni + 4) * (B.nj + 4) * (B.nk + 4);
+        CK(cudaMemcpyAsync(prim_out[b * nf + p], c->xall.p + off[(size_t)b * nf + p],
+                           (size_t)ng * H.nc * sizeof(double), cudaMemcpyDeviceToHost, c->s_down));
+      }
+    }
+    c->prev_phase = ph;
+    c->phase = phn;
+  }
+  CK(cudaEventRecord(t1, c->s_down));
+  CK(cudaStreamSynchronize(c->s_down));
+  CK(cudaStreamSynchronize(s));
+  float dms = 0.f;
+  CK(cudaEventElapsedTime(&dms, t0, t1));
+  cudaEventDestroy(t0); cudaEventDestroy(t1);
+  return finish_step(c, out, dms);
 }
 
 int ice_gpu_residual_norm(ice_gpu_ctx* c, double* total, double* fam) {

@@ -73,6 +73,24 @@ class Solver:
             raise SolveError(f"step failed ({rc}, status {self.last.status}): {self.lib.error(self.ctx)}")
         return self.last
 
+    def step_host(self, states_in, states_out, nsteps: int = 1, check: bool = True) -> abi.StepOut:
+        """ice_gpu_step_host: the state in and out of host arrays, per block and family in the layout
+        of upload/download (C-contiguous float64; page-locked for full-speed copies). states_out may
+        be states_in."""
+        nf = len(self.case.families)
+        flat_in = [a for per in states_in for a in per]
+        flat_out = [a for per in states_out for a in per]
+        assert len(flat_in) == len(flat_out) == len(self.case.nodes) * nf
+        for a in flat_in + flat_out:
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        P = C.POINTER(C.c_double)
+        pin = (P * len(flat_in))(*[abi.ptr(a) for a in flat_in])
+        pout = (P * len(flat_out))(*[abi.ptr(a) for a in flat_out])
+        rc = self.lib.step_host(self.ctx, nsteps, pin, pout, C.byref(self.last))
+        if check and rc != 0:
+            raise SolveError(f"step_host failed ({rc}, status {self.last.status}): {self.lib.error(self.ctx)}")
+        return self.last
+
     def set_time(self, time: float, it: int, it_from_call: int = 0):
         self._check(self.lib.set_time(self.ctx, time, it, it_from_call), "set_time")
 

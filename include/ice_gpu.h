@@ -223,6 +223,17 @@ int ice_gpu_set_time(ice_gpu_ctx* ctx, double time, int32_t iter, int32_t iter_f
  * step ended on a state the reference stops on (out->status says which). */
 int ice_gpu_step(ice_gpu_ctx* ctx, int32_t nsteps, ice_gpu_step_out* out);
 
+/* nsteps time steps for a driver that keeps the state on the host. prim_in[(b-1)*nfam + (p-1)]
+ * holds family p of block b in the layout of ice_gpu_upload_state, and prim_out the same for the
+ * state after the steps (prim_out may equal prim_in). The result is that of upload_state for every
+ * block and family, then ice_gpu_step(nsteps), then download_state for every block and family. Here
+ * the uploads, the steps and each family's download overlap, so the call takes less time than those
+ * calls one after another. Page-locked host arrays let the copies run at full speed.
+ * replaces: call Explicit_Step(grid) (driver/Wrap_Solve.f90:26) with the state kept in the
+ * driver's arrays. */
+int ice_gpu_step_host(ice_gpu_ctx* ctx, int32_t nsteps, const double* const* prim_in,
+                      double* const* prim_out, ice_gpu_step_out* out);
+
 /* The residual norm of the last step: total[5], and fam[5*nfam] per family (may be NULL).
  * replaces: residual_norm (diagnostic/Mod_Diagnostic.f90:22-83). */
 int ice_gpu_residual_norm(ice_gpu_ctx* ctx, double* total, double* fam);
