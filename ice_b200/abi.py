@@ -91,6 +91,7 @@ _SIGNATURES = [
     ("set_block", C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp]),
     ("set_records", C.c_int, [_vp, C.c_int32, _ip, _dp]),
     ("set_chimera", C.c_int, [_vp, C.c_int32, _ip, _ip, _dp]),
+    ("set_imports", C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),
     ("set_gas", C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp, _dp]),
     ("upload_state", C.c_int, [_vp, C.c_int32, C.c_int32, _dp, _u8p]),
     ("download_state", C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),

@@ -103,6 +103,29 @@ def riemann_1d(n=2000, steps=1000):
     return case
 
 
+def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
+    """The setting of the reference's unit test of the steps of empty cells a source fills
+    (test/unit/test_empty_dt.f90): one block of 4 x 1 x 1 cells of 1 mm (the last 0.1 mm wide when
+    narrow_last), an MK family, CFL 0.4, dt-max 1e-4 s; the first n_occupied cells at density 1 and
+    100 m/s (300 K, 1e9 particles), the others at ICE's empty state (1e-25 in every slot); transmissive
+    ends. The coupler's imports are set separately (ice_gpu_set_imports)."""
+    dx = 1e-3
+    x = np.array([0.0, 1.0, 2.0, 3.0, 3.1 if narrow_last else 4.0]) * dx
+    X, Y, Z = np.meshgrid(x, np.array([0.0, dx]), np.array([0.0, dx]), indexing="ij")
+    nodes = np.stack([X, Y, Z], axis=-1)
+    fam = Family("MK", rho_al=1000.0, cs_al=1000.0)
+    num = Numerics(scheme="euler", time_accurate=time_accurate, cfl=0.4, dt_max=1e-4, limiter="minmod",
+                   itermax=steps)
+    rows = box_bc(1, (4, 1, 1), {1: 400, 2: 400, 3: 0, 4: 0, 5: 0, 6: 0})
+    case = Case("empty_tube", [nodes], [fam], num, rows)
+    st = empty_state((4, 1, 1), 6)
+    I = st[2:3, 2:3, 2:-2]
+    I[...] = 1e-25
+    I[0, 0, :n_occupied] = [1.0, 100.0, 0.0, 0.0, 300.0, 1e9]
+    case.state = [[st]]
+    return case
+
+
 # --------------------------------------------------- crossing jets (validation)
 def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
     """The crossing-jets validation case of the reference's suite (its Doisneau cases):

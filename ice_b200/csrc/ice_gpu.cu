@@ -89,6 +89,9 @@ struct FamHost {
   std::vector<DRec> h_recs;                  // the device records, kept to attach chimera donors
   DevBuf<int4> cdon;                         // chimera donors (0-based block, i, j, k) and weights
   DevBuf<double> cw;
+  DevBuf<double> imp;                        // the coupler's imports [v][NI] (ice_gpu_set_imports)
+  DevBuf<EmptyScan> escan;                   // bound_empty_dt's reductions
+  bool have_imp = false;
 };
 
 
@@ -226,6 +229,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   F.Rb = H.Rb.p; F.Rbw = H.Rb.p;
   F.connF = H.connF.p;
   F.cdon = H.cdon.p; F.cw = H.cw.p;
+  F.imports = H.have_imp ? H.imp.p : nullptr;
   F.resid = H.resid.p;
   static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
   F.rk = RKC[c->P.nrk - 1][srk - 1];
@@ -281,6 +285,24 @@ static void launch_dt(ice_gpu_ctx* c, int p, int phase, cudaStream_t s) {
     case ICE_CLOSURE_IG: k_dt<IG><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
     default: k_dt<AG><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
   }
+  // a family the coupler feeds or drains: bound_empty_dt and bound_removal_dt (Mod_Explicit.f90:57-60)
+  if (!c->fam[p].have_imp) return;
+  EmptyScan* e = c->fam[p].escan.p;
+  k_empty_init<<<1, 1, 0, s>>>(e);
+  switch (c->fam[p].closure) {
+    case ICE_CLOSURE_MK:
+      k_empty_scan<MK><<<g, 256, 0, s>>>(G, F, dto, c->P.cfl, c->P.ndir, e);
+      k_empty_apply<MK><<<g, 256, 0, s>>>(G, F, dto, c->P.cfl, c->P.ndir, e, c->st.p);
+      break;
+    case ICE_CLOSURE_IG:
+      k_empty_scan<IG><<<g, 256, 0, s>>>(G, F, dto, c->P.cfl, c->P.ndir, e);
+      k_empty_apply<IG><<<g, 256, 0, s>>>(G, F, dto, c->P.cfl, c->P.ndir, e, c->st.p);
+      break;
+    default:
+      k_empty_scan<AG><<<g, 256, 0, s>>>(G, F, dto, c->P.cfl, c->P.ndir, e);
+      k_empty_apply<AG><<<g, 256, 0, s>>>(G, F, dto, c->P.cfl, c->P.ndir, e, c->st.p);
+      break;
+  }
 }
 
 static int next_phase(const ice_gpu_ctx* c, int phase) {
@@ -318,6 +340,7 @@ static void prof_tick(void* vc, int cls, cudaStream_t s) {
 
 static long long launches_per_step(const ice_gpu_ctx* c) {
   long long n = 2 + c->P.nfam;
+  for (int p = 0; p < c->P.nfam; ++p) n += c->fam[p].have_imp ? 3 : 0;
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
     long long per = (H.nrec > 0 ? 1 : 0) + (c->P.shock_detector && !c->staged ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
@@ -904,6 +927,36 @@ int ice_gpu_set_chimera(ice_gpu_ctx* c, int32_t nrec, const int32_t* nchi, const
   }
   c->have_chimera = true;
   free_graphs(c);
+  return 0;
+}
+
+// The coupler's imports into family p of block b (ICE_cond_phase_type%imports, which the coupler's
+// add_birth_rate, add_absorption_rate and add_removal_rate accumulate: coupling/Mod_Exchange.f90:270-390),
+// (ncond, ni, nj, nk) in the driver's layout; NULL sets the block's to zero. The first call for a family
+// allocates them (zero elsewhere), and from then on the family's steps add them to the residual and
+// bound its steps as bound_empty_dt and bound_removal_dt do.
+int ice_gpu_set_imports(ice_gpu_ctx* c, int32_t b1, int32_t p1, const double* imports) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam) return fail(c, ICE_GPU_EINVAL, "set_imports: bad block/family");
+  FamHost& H = c->fam[p1 - 1];
+  const DBlock& B = c->hblk[b1 - 1];
+  const long long n = (long long)B.ni * B.nj * B.nk;
+  if (imports)
+    for (long long q = 0; q < n * H.nc; ++q)
+      if (!std::isfinite(imports[q])) return fail(c, ICE_GPU_EINVAL, "set_imports: a rate is not finite");
+  CK(cudaStreamSynchronize(c->stream));
+  if (!H.have_imp) {
+    CK(H.imp.alloc((size_t)c->NI * H.nc));
+    CK(cudaMemset(H.imp.p, 0, (size_t)c->NI * H.nc * sizeof(double)));
+    CK(H.escan.alloc(1));
+    H.have_imp = true;
+    free_graphs(c);
+  }
+  std::vector<double> col((size_t)n);
+  for (int v = 0; v < H.nc; ++v) {
+    for (long long q = 0; q < n; ++q) col[(size_t)q] = imports ? imports[q * H.nc + v] : 0.0;
+    CK(cudaMemcpy(H.imp.p + (long long)v * c->NI + B.ioff, col.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+  }
   return 0;
 }
 

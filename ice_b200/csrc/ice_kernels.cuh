@@ -199,6 +199,101 @@ __global__ void __launch_bounds__(256) k_dt(Geo G, FamDev F, Status* st, double 
   }
 }
 
+// The rate of compute_dt_ (Mod_dt.f90:256-275): sum over the resolved directions of (|u . versor| +
+// the closure's signal speed) times the modulus of the metric row, for the state p of cell q.
+template <int CL>
+__device__ __forceinline__ double dt_rate(const Geo& G, long long q, const double* p, int ndir) {
+  double rate = 0.0;
+  for (int d = 0; d < ndir; ++d) {
+    double t0 = G.M[(long long)d * G.NI + q], t1 = G.M[(long long)(3 + d) * G.NI + q], t2 = G.M[(long long)(6 + d) * G.NI + q];
+    double gn = norm2_3(t0, t1, t2);
+    double vs[3] = {t0 / gn, t1 / gn, t2 / gn};
+    rate = rate + (fabs(p[1]*vs[0] + p[2]*vs[1] + p[3]*vs[2]) + wavespeed<CL>(p, vs)) * gn;
+  }
+  return rate;
+}
+
+__global__ void k_empty_init(EmptyScan* e) {
+  e->floor_bits = (unsigned long long)__double_as_longlong(1.79769313486231570e+308);
+  e->src_bits = e->floor_bits;
+  e->umax_bits[0] = e->umax_bits[1] = e->umax_bits[2] = 0ULL;
+  e->filled = 0u;
+}
+
+// bound_empty_dt's first pass (Mod_dt.f90:134-196) over one family's cells, with the coupler's
+// imports as the only source: an occupied cell (density above rho_empty) gives its step and speeds;
+// an empty cell with a positive mass rate gives the speeds of what it receives (the rate's momentum
+// over its mass) and the step of compute_dt_ at that speed, times cfl.
+template <int CL>
+__global__ void __launch_bounds__(256) k_empty_scan(Geo G, FamDev F, const double* dt_cell, double cfl, int ndir,
+                                                    EmptyScan* e) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.NI) return;
+  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  int i, j, k; decode(B, q, i, j, k);
+  constexpr int nc = NC<CL>::v;
+  const long long g = gidx(B, i, j, k);
+  double p[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
+  double s[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) s[v] = F.imports[(long long)v * G.NI + q];
+  if (s[0] > 0.0) atomicOr(&e->filled, 1u);
+  if (p[0] > kRhoEmpty) {
+    if (dt_cell) atomicMin(&e->floor_bits, (unsigned long long)__double_as_longlong(dt_cell[q]));
+    for (int a = 0; a < 3; ++a) atomicMax(&e->umax_bits[a], (unsigned long long)__double_as_longlong(fabs(p[1 + a])));
+    return;
+  }
+  if (!(s[0] > 0.0)) return;
+  p[1] = s[1]/s[0]; p[2] = s[2]/s[0]; p[3] = s[3]/s[0];
+  for (int a = 0; a < 3; ++a) atomicMax(&e->umax_bits[a], (unsigned long long)__double_as_longlong(fabs(p[1 + a])));
+  double dts = (double)1e+5f;
+  const double rate = dt_rate<CL>(G, q, p, ndir);
+  if (rate > 0.0) dts = mn(dts, 1.0/rate);
+  atomicMin(&e->src_bits, (unsigned long long)__double_as_longlong(dts*cfl));
+}
+
+// bound_empty_dt's second pass (Mod_dt.f90:197-214) and bound_removal_dt (Mod_dt.f90:220-242). Time-
+// accurate: the global step lowered to the sources' step (when a source fills anything) and to each
+// cell's removal step (its density over the rate the coupler takes out). Steady: each empty cell's
+// step lowered to the smaller of the occupied cells' smallest step and the sources', and to cfl over
+// its rate at the largest speeds; each cell's to its removal step. Only minima: the order of the two
+// bounds does not change a bit.
+template <int CL>
+__global__ void __launch_bounds__(256) k_empty_apply(Geo G, FamDev F, double* dt_cell, double cfl, int ndir,
+                                                     const EmptyScan* e, Status* st) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.NI) return;
+  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  int i, j, k; decode(B, q, i, j, k);
+  const double rho = F.Up[gidx(B, i, j, k)];
+  const bool filled = e->filled != 0u;
+  const double src_dt = __longlong_as_double((long long)e->src_bits);
+  if (!dt_cell) {                                    // time-accurate
+    if (q == 0 && filled) atomicMin(&st->dtbits, e->src_bits);
+  } else if (filled && !(rho > kRhoEmpty)) {
+    const double floor_dt = mn(__longlong_as_double((long long)e->floor_bits), src_dt);
+    double umax[3];
+    for (int a = 0; a < 3; ++a) umax[a] = __longlong_as_double((long long)e->umax_bits[a]);
+    double rate = 0.0;
+    for (int d = 0; d < ndir; ++d) {
+      double sum = umax[0]*fabs(G.M[(long long)d * G.NI + q]);
+      sum = sum + umax[1]*fabs(G.M[(long long)(3 + d) * G.NI + q]);
+      sum = sum + umax[2]*fabs(G.M[(long long)(6 + d) * G.NI + q]);
+      rate = rate + sum;
+    }
+    double dts = floor_dt;
+    if (rate > 0.0) dts = mn(dts, cfl/rate);
+    dt_cell[q] = mn(dt_cell[q], dts);
+  }
+  const double out = -F.imports[q];
+  if (!(out > 0.0)) return;
+  const double dts = rho/out;
+  if (!dt_cell) atomicMin(&st->dtbits, (unsigned long long)__double_as_longlong(dts));
+  else dt_cell[q] = mn(dt_cell[q], dts);
+}
+
 // ------------------------------------------------------------------ ghosts
 __device__ __forceinline__ int ghost_rule(const DRec& r, double veln) {
   int rule = 0;  // copy
@@ -640,6 +735,10 @@ k_stage(Geo G, FamDev F, const Tile* tiles, int TX, int TY, int KZ, int write_r,
       const double vol = G.vol[q];
 #pragma unroll
       for (int v = 0; v < nc; ++v) r[v] = (r[v]/vol + s[v]) * dt;
+      if (F.imports) {                          // add_births (Lib_Residual.f90:164-210): the coupler's rates
+#pragma unroll
+        for (int v = 0; v < nc; ++v) r[v] = r[v] + F.imports[(long long)v * G.NI + q] * dt;
+      }
 #pragma unroll
       for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) r[v] = 0.0;
       if (write_r) {

@@ -98,10 +98,19 @@ struct FamDev {              // what the kernels of one family read
   double* connF;             // [ncf][nc]
   const int4* cdon;          // chimera donors: 0-based block, i, j, k
   const double* cw;          // chimera donor weights
+  const double* imports;     // [v][NI]: the coupler's rates into the cells, or null
   double* resid;             // IRS: [v][NI]
   double rk;
   int write_tau;
   int src_ready;             // S holds this stage's source already (the surrogate source kernel ran)
+};
+
+// bound_empty_dt's reductions over one family's cells, as the bits of non-negative doubles (which
+// order as their bits): the smallest step of an occupied cell, the smallest step of a source, the
+// largest speed per axis, and whether a source fills anything.
+struct EmptyScan {
+  unsigned long long floor_bits, src_bits, umax_bits[3];
+  unsigned int filled, pad;
 };
 
 struct Tile { int b, i0, j0, k0, nkz; };

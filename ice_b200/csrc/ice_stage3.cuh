@@ -458,6 +458,10 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
 #pragma unroll
         for (int v = 0; v < nc; ++v) rd[v] = ((double)r[v]*ivol + s[v]) * dt;
       }
+      if (F.imports) {                          // add_births (Lib_Residual.f90:164-210): the coupler's rates
+#pragma unroll
+        for (int v = 0; v < nc; ++v) rd[v] = rd[v] + F.imports[(long long)v * G.NI + q] * dt;
+      }
 #pragma unroll
       for (int v = 0; v < nc; ++v) if (F.frozen_mask & (1u << v)) rd[v] = 0.0;
       if (write_r) {

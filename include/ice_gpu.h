@@ -205,6 +205,15 @@ int ice_gpu_set_chimera(ice_gpu_ctx* ctx, int32_t nrec, const int32_t* nchi, con
 int ice_gpu_set_gas(ice_gpu_ctx* ctx, int32_t b, const double* prim5, const double* R,
                     const double* gam, const double* k, const double* mu);
 
+/* The coupler's imports into family p (1-based) of block b: imports (ncond, ni, nj, nk), the rates
+ * that the coupler's add_birth_rate, add_absorption_rate and add_removal_rate accumulate in
+ * ICE_cond_phase_type%imports (coupling/Mod_Exchange.f90:270-390); NULL sets the block's rates to
+ * zero. From the first call on, every step of the family adds imports * dt to the residual
+ * (add_births) and bounds its steps as bound_empty_dt and bound_removal_dt do.
+ * replaces: add_births (numerics/time/explicit/Lib_Residual.f90:164-210), bound_empty_dt and
+ * bound_removal_dt (numerics/time/Mod_dt.f90:134-242) for a coupled family. */
+int ice_gpu_set_imports(ice_gpu_ctx* ctx, int32_t b, int32_t p, const double* imports);
+
 /* State of family p (1-based) in block b: prim (ncond, 1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc),
  * gc = 2; inj the injected-ghost flags on the same cells (NULL: all false).
  * replaces: setup_cond's result (driver/Mod_Phase.f90:66-124). */

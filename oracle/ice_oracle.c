@@ -35,6 +35,7 @@
 
 typedef struct {
     double *prim, *prim_old, *residual, *source, *dt, *tau, *beta;
+    double *imports;      /* the coupler's rates (nc per interior cell), or NULL */
     unsigned char *inj;
 } ofam;
 
@@ -59,6 +60,7 @@ typedef struct orc_ctx {
     int nrec;
     orec* bc;
     int nchim, have_chim; /* chimera records and whether their donors are set */
+    int have_imp[MAXF];   /* the family has the coupler's imports (set_imports) */
     int* cdon;            /* chimera donors: block, i, j, k (1-based) */
     double* cw;           /* their weights */
     int* grp_first;       /* nfam+1, 0-based into grp */
@@ -152,7 +154,7 @@ int orc_destroy(orc_ctx* c) {
         for (int p = 0; p < c->P.nfam; ++p) {
             ofam* F = &B->fam[p];
             free(F->prim); free(F->prim_old); free(F->residual); free(F->source);
-            free(F->dt); free(F->beta); free(F->tau); free(F->inj);
+            free(F->dt); free(F->beta); free(F->tau); free(F->inj); free(F->imports);
         }
     }
     free(c->blk); free(c->bc); free(c->grp_first); free(c->grp); free(c->cdon); free(c->cw);
@@ -958,6 +960,124 @@ static void compute_dt(orc_ctx* c, int p) {
     c->dtglobal = o_min2(c->dtglobal, dtmin);
 }
 
+/* The coupler's imports into family p1 of block b1 (ICE_cond_phase_type%imports, accumulated by
+ * Mod_Exchange.f90:270-390), (nc, ni, nj, nk); NULL zeroes the block's. The first call allocates the
+ * family's arrays (zero in every block). */
+int orc_set_imports(orc_ctx* c, int b1, int p1, const double* imports) {
+    if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam) return seterr(c, ICE_GPU_EINVAL, "set_imports: bad block/family");
+    int p = p1 - 1, nc = nc_of(c, p);
+    oblk* Bq = &c->blk[b1 - 1];
+    if (imports)
+        for (long q = 0; q < ncells(Bq)*nc; ++q)
+            if (!isfinite(imports[q])) return seterr(c, ICE_GPU_EINVAL, "set_imports: a rate is not finite");
+    if (!c->have_imp[p]) {
+        for (int b = 0; b < c->nb; ++b) c->blk[b].fam[p].imports = (double*)calloc((size_t)nc*ncells(&c->blk[b]), sizeof(double));
+        c->have_imp[p] = 1;
+    }
+    double* d = Bq->fam[p].imports;
+    for (long q = 0; q < ncells(Bq)*nc; ++q) d[q] = imports ? imports[q] : 0.0;
+    return 0;
+}
+
+/* bound_empty_dt (Mod_dt.f90:134-214) with the coupler's imports as the source (no births of the
+ * family's own, no burning family): an empty cell that a source fills steps no further than what
+ * fills it. */
+static void bound_empty_dt(orc_ctx* c, int p) {
+    if (!c->have_imp[p]) return;
+    int nc = nc_of(c, p), cl = c->P.fam[p].closure, ndir = c->P.ndir;
+    double cfl = c->P.cfl;
+    int filled = 0;
+    double floor_dt = DBL_MAX, src_dt = DBL_MAX, umax[3] = {0.0, 0.0, 0.0};
+    double ps[NCM];
+    for (int b = 0; b < c->nb; ++b) {
+        oblk* B = &c->blk[b];
+        ofam* F = &B->fam[p];
+        for (int k = 1; k <= B->nk; ++k) for (int j = 1; j <= B->nj; ++j) for (int i = 1; i <= B->ni; ++i) {
+            long q = II(B, i, j, k);
+            const double* pr = F->prim + nc*CI(B, i, j, k);
+            const double* s = F->imports + nc*q;
+            if (s[0] > 0.0) filled = 1;
+            if (pr[0] > O_RHO_EMPTY) {
+                floor_dt = o_min2(floor_dt, F->dt[q]);
+                for (int a = 0; a < 3; ++a) umax[a] = o_max2(umax[a], fabs(pr[1 + a]));
+                continue;
+            }
+            if (!(s[0] > 0.0)) continue;
+            for (int v = 0; v < nc; ++v) ps[v] = pr[v];
+            for (int a = 0; a < 3; ++a) ps[1 + a] = s[1 + a]/s[0];
+            for (int a = 0; a < 3; ++a) umax[a] = o_max2(umax[a], fabs(ps[1 + a]));
+            double dts = (double)1e+5f, rate = 0.0;
+            const double* T = B->M + 9*RI(B, i, j, k);
+            for (int d = 0; d < ndir; ++d) {
+                double gn = o_norm2(T[d], T[3 + d], T[6 + d]);
+                double vs[3] = {T[d]/gn, T[3 + d]/gn, T[6 + d]/gn};
+                rate = rate + (fabs(ps[1]*vs[0] + ps[2]*vs[1] + ps[3]*vs[2]) + o_wavespeed(cl, ps, vs)) * gn;
+            }
+            if (rate > 0.0) dts = o_min2(dts, 1.0/rate);
+            src_dt = o_min2(src_dt, dts*cfl);
+        }
+    }
+    if (!filled) return;
+    if (c->P.time_accurate) { c->dtglobal = o_min2(c->dtglobal, src_dt); return; }
+    floor_dt = o_min2(floor_dt, src_dt);
+    for (int b = 0; b < c->nb; ++b) {
+        oblk* B = &c->blk[b];
+        ofam* F = &B->fam[p];
+        for (int k = 1; k <= B->nk; ++k) for (int j = 1; j <= B->nj; ++j) for (int i = 1; i <= B->ni; ++i) {
+            const double* pr = F->prim + nc*CI(B, i, j, k);
+            if (pr[0] > O_RHO_EMPTY) continue;
+            const double* T = B->M + 9*RI(B, i, j, k);
+            double rate = 0.0;
+            for (int d = 0; d < ndir; ++d) {
+                double sum = umax[0]*fabs(T[d]);
+                sum = sum + umax[1]*fabs(T[3 + d]);
+                sum = sum + umax[2]*fabs(T[6 + d]);
+                rate = rate + sum;
+            }
+            double dts = floor_dt;
+            if (rate > 0.0) dts = o_min2(dts, cfl/rate);
+            long q = II(B, i, j, k);
+            F->dt[q] = o_min2(F->dt[q], dts);
+        }
+    }
+}
+
+/* bound_removal_dt (Mod_dt.f90:220-242): a cell the coupler takes mass out of steps no further
+ * than empties it. */
+static void bound_removal_dt(orc_ctx* c, int p) {
+    if (!c->have_imp[p]) return;
+    int nc = nc_of(c, p);
+    for (int b = 0; b < c->nb; ++b) {
+        oblk* B = &c->blk[b];
+        ofam* F = &B->fam[p];
+        for (int k = 1; k <= B->nk; ++k) for (int j = 1; j <= B->nj; ++j) for (int i = 1; i <= B->ni; ++i) {
+            long q = II(B, i, j, k);
+            double out = -F->imports[nc*q];
+            if (!(out > 0.0)) continue;
+            double dts = F->prim[nc*CI(B, i, j, k)]/out;
+            if (c->P.time_accurate) c->dtglobal = o_min2(c->dtglobal, dts);
+            else F->dt[q] = o_min2(F->dt[q], dts);
+        }
+    }
+}
+
+/* add_births (Lib_Residual.f90:164-210) with the coupler's imports: residual + imports * dt, then the
+ * frozen slots to zero. */
+static void add_births(orc_ctx* c, int p) {
+    if (!c->have_imp[p]) return;
+    int nc = nc_of(c, p);
+    const ice_gpu_family* mat = &c->P.fam[p];
+    for (int b = 0; b < c->nb; ++b) {
+        oblk* B = &c->blk[b];
+        ofam* F = &B->fam[p];
+        for (long q = 0; q < ncells(B); ++q) {
+            double* r = F->residual + nc*q;
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + F->imports[nc*q + v]*F->dt[q];
+            for (int f = 0; f < mat->nfrozen; ++f) r[mat->frozen[f] - 1] = 0.0;
+        }
+    }
+}
+
 /* --------------------------------------------------------------- norm */
 static void residual_norm(orc_ctx* c) {
     int nf = c->P.nfam;
@@ -1003,7 +1123,7 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
     int nf = c->P.nfam;
     c->iter += 1; c->iter_from_call += 1;
     c->dtglobal = (double)1e+5f;
-    for (int p = 0; p < nf; ++p) compute_dt(c, p);
+    for (int p = 0; p < nf; ++p) { compute_dt(c, p); bound_empty_dt(c, p); bound_removal_dt(c, p); }
     if (c->P.time_accurate) {
         c->time = c->time + c->dtglobal;
         for (int b = 0; b < c->nb; ++b) for (int p = 0; p < nf; ++p) {
@@ -1026,6 +1146,7 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
             if (compute_bound(c, p)) { c->status |= ICE_GPU_ST_BAD_RECON; return ICE_GPU_ESTATE; }
             if (compute_flux(c, p)) { c->status |= ICE_GPU_ST_BAD_RECON; return ICE_GPU_ESTATE; }
             compute_residual(c, p);
+            add_births(c, p);
             if (c->P.irs) residual_smoothing(c, p);
             if (state_update(c, p, srk)) { c->status |= ICE_GPU_ST_NAN_STATE; return ICE_GPU_ESTATE; }
         }

@@ -118,6 +118,75 @@ def test_chimera_matches_reference_output(gpu):
         assert l2 <= 1e-12, (b, l2)
 
 
+def _with_imports(case, seed, scale):
+    """The coupler's imports for every block and family: births into a quarter of the cells (mass at
+    up to `scale` per second with a momentum of 0-30 m/s), removal from another quarter (up to a
+    tenth of the local density per second)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b, (ni, nj, nk) in enumerate(case.dims):
+        per = []
+        for p, fam in enumerate(case.families):
+            rho = case.state[b][p][2:-2, 2:-2, 2:-2, 0]
+            imp = np.zeros((nk, nj, ni, fam.nc))
+            u = rng.random((nk, nj, ni))
+            born = u < 0.25
+            gone = u > 0.75
+            m = scale * rng.random((nk, nj, ni))
+            imp[..., 0] = np.where(born, m, 0.0) - np.where(gone, 0.1 * np.nan_to_num(rho) * rng.random((nk, nj, ni)), 0.0)
+            for a in range(3):
+                imp[..., 1 + a] = np.where(born, m * 30.0 * (rng.random((nk, nj, ni)) - 0.5), 0.0)
+            per.append(np.ascontiguousarray(imp))
+        out.append(per)
+    return out
+
+
+def _set_imports(lib, solver, imports):
+    for b, per in enumerate(imports):
+        for p, imp in enumerate(per):
+            assert lib.set_imports(solver.ctx, b + 1, p + 1, abi.ptr(imp)) == 0
+
+
+@pytest.mark.parametrize("args", [(2, None, False, False), (2, 3, False, False), (0, 3, False, False),
+                                  (2, 1, False, False), (2, 1, False, True), (0, 3, True, False)],
+                         ids=["E1", "E2", "E4", "E5", "E6", "E7"])
+def test_empty_tube_imports_bit_exact(gpu, orc, args):
+    # the unit test's tube of empty cells that the coupler's imports fill: its steps and states
+    n_occ, cell, ta, narrow = args
+    res = []
+    for lib in (gpu, orc):
+        case = configs.empty_tube(n_occ, ta, narrow, steps=3)
+        s = Solver(case, lib)
+        if cell is not None:
+            imp = np.zeros((1, 1, 4, 6))
+            imp[0, 0, cell - 1] = [2e2, 2e2 * 800.0, 0.0, 0.0, 0.0, 0.0]
+            assert lib.set_imports(s.ctx, 1, 1, abi.ptr(imp)) == 0
+        out = s.step(3)
+        res.append((out.status, out.dtglobal, out.time, s.download(0, 0)[2, 2, 2:-2]))
+    (st_g, dt_g, t_g, p_g), (st_o, dt_o, t_o, p_o) = res
+    assert st_g == st_o == 0 and dt_g == dt_o and t_g == t_o
+    assert np.array_equal(p_g, p_o)
+
+
+@pytest.mark.parametrize("steady", [False, True], ids=["time_accurate", "steady"])
+def test_multiblock_imports(gpu, orc, steady):
+    # the coupler's births and removals in every family of a multi-block case
+    def make():
+        c = configs.multiblock_tree(nblocks=5, seed=4, lo=5, hi=10, steps=6)
+        c.numerics.time_accurate = not steady
+        return c
+    cg, co = make(), make()
+    imports = _with_imports(cg, 11, 50.0)
+    sg, so = Solver(cg, gpu), Solver(co, orc)
+    _set_imports(gpu, sg, imports)
+    _set_imports(orc, so, imports)
+    og, oo = sg.step(6), so.step(6)
+    assert og.status == 0 and oo.status == 0
+    assert abs(og.dtglobal - oo.dtglobal) <= TOL * abs(oo.dtglobal)
+    err = compare(sg, so, cg)
+    assert err <= TOL, err
+
+
 def _irs(case):
     case.numerics.irs = True
     case.numerics.irs_beta = 0.5

@@ -7,6 +7,8 @@
 - test/Doisneau/IG-chimera: the overlapping-grid variant (two blocks joined by chimera faces,
   102), its density after 5000 iterations (tests/golden/chimera_IG.npz); same gates.
 - test/unit/test_muscl_bounds.f90 B1-B5: the bounds of the limited slopes.
+- test/unit/test_empty_dt.f90 E1-E7: the steps of empty cells that the coupler's imports fill
+  (bound_empty_dt), through a whole step (compute_dt gives the starting steps the unit test sets).
 """
 import math
 from pathlib import Path
@@ -171,3 +173,53 @@ def test_riemann_1d_runs_and_conserves_mass(orc):
     dx = 1.0 / 200
     gained = (float(p[:, 0].sum()) - m0) * dx
     assert abs(gained - 1.5 * out.time) <= 1e-10 * 1.5 * out.time
+
+
+def _empty_tube_step(orc, n_occupied, source_cell=None, time_accurate=False, narrow_last=False):
+    """One step of the unit test's 4-cell tube; returns the step's output and each cell's step."""
+    case = configs.empty_tube(n_occupied, time_accurate, narrow_last)
+    s = Solver(case, orc)
+    if source_cell is not None:
+        imp = np.zeros((1, 1, 4, 6))
+        imp[0, 0, source_cell - 1] = [2e2, 2e2 * 800.0, 0.0, 0.0, 0.0, 0.0]   # births at 800 m/s
+        assert orc.set_imports(s.ctx, 1, 1, abi.ptr(imp)) == 0
+    out = s.step(1)
+    dt = np.zeros(4)
+    orc.download_aux(s.ctx, 1, 1, abi.ptr(dt), None, None)
+    return out, dt
+
+
+def test_empty_dt_unit_cases(orc):
+    cfl, dx, dtmax = 0.4, 1e-3, 1e-4
+    occ, src = cfl * dx / 100.0, cfl * dx / 800.0
+    near = lambda a, b: bool(np.all(np.abs(np.asarray(a) - b) <= 4 * np.finfo(float).eps * abs(b)))
+    # E1: no source; the steps compute_dt gives: cfl dx/|u| occupied, the dt-max ceiling empty
+    _, dt0 = _empty_tube_step(orc, 2)
+    assert near(dt0[:2], occ) and np.all(dt0[2:] == dtmax)
+    # E2/E3: imports at 800 m/s into empty cell 3: occupied cells keep their steps, empty ones cfl dx/800
+    _, dt = _empty_tube_step(orc, 2, source_cell=3)
+    assert np.array_equal(dt[:2], dt0[:2]) and near(dt[2:], src)
+    # E4: no occupied cell: every cell at the source's step
+    _, dt = _empty_tube_step(orc, 0, source_cell=3)
+    assert near(dt, src)
+    # E5: a source in occupied cell 1 only: the empty cells at the occupied cells' step
+    _, dt = _empty_tube_step(orc, 2, source_cell=1)
+    assert np.array_equal(dt[:2], dt0[:2]) and near(dt[2:], occ)
+    # E6: the same, empty cell 4 ten times narrower: it steps at its own width at the occupied speed.
+    # The unit test sets that cell's metric to 10/dx exactly; here it comes from the nodes 3.0 and
+    # 3.1 mm, whose difference is 1e-4 only to a few ulp, so the bound is 64 ulp there
+    _, dt = _empty_tube_step(orc, 2, source_cell=1, narrow_last=True)
+    assert np.array_equal(dt[:2], dt0[:2]) and near(dt[2:3], occ)
+    assert abs(dt[3] - occ / 10.0) <= 64 * np.finfo(float).eps * occ / 10.0
+    # E7: time-accurate, imports into empty cell 3, no occupied cell: the global step at the source's
+    out, _ = _empty_tube_step(orc, 0, source_cell=3, time_accurate=True)
+    assert near([out.dtglobal], src)
+
+
+def test_imports_are_checked(orc):
+    case = configs.empty_tube(2)
+    s = Solver(case, orc)
+    imp = np.zeros((1, 1, 4, 6))
+    assert orc.set_imports(s.ctx, 2, 1, abi.ptr(imp)) == abi.EINVAL
+    imp[0, 0, 1, 0] = np.nan
+    assert orc.set_imports(s.ctx, 1, 1, abi.ptr(imp)) == abi.EINVAL
