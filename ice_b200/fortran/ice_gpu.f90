@@ -42,7 +42,7 @@ module ice_gpu
   end type ice_gpu_step_out_t
 
   public :: ice_gpu_create, ice_gpu_set_block, ice_gpu_set_records, ice_gpu_set_chimera, ice_gpu_set_gas, &
-            ice_gpu_upload_state, &
+            ice_gpu_set_imports, ice_gpu_step_host, ice_gpu_upload_state, &
             ice_gpu_download_state, ice_gpu_set_time, ice_gpu_step, ice_gpu_residual_norm, ice_gpu_update_params, &
             ice_gpu_last_error, ice_gpu_destroy, ice_gpu_pair_connections
 
@@ -68,6 +68,22 @@ module ice_gpu
       integer(c_int32_t), value      :: nrec
       integer(c_int32_t), intent(in) :: rec(*)
       real(c_double), intent(in)     :: inlet(*)
+    end function
+
+    integer(c_int) function ice_gpu_set_imports(ctx, b, p, imports) bind(C, name='ice_gpu_set_imports')
+      import :: c_int, c_int32_t, c_double, c_ptr
+      type(c_ptr), value         :: ctx
+      integer(c_int32_t), value  :: b, p
+      real(c_double), intent(in) :: imports(*)
+    end function
+
+    integer(c_int) function ice_gpu_step_host(ctx, nsteps, prim_in, prim_out, out) bind(C, name='ice_gpu_step_host')
+      import :: c_int, c_int32_t, c_ptr, ice_gpu_step_out_t
+      type(c_ptr), value              :: ctx
+      integer(c_int32_t), value       :: nsteps
+      type(c_ptr), intent(in)         :: prim_in(*)
+      type(c_ptr), intent(in)         :: prim_out(*)
+      type(ice_gpu_step_out_t), intent(out) :: out
     end function
 
     integer(c_int) function ice_gpu_set_chimera(ctx, nrec, nchi, donor, weight) bind(C, name='ice_gpu_set_chimera')
