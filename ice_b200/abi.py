@@ -92,6 +92,8 @@ _SIGNATURES = [
     ("set_records", C.c_int, [_vp, C.c_int32, _ip, _dp]),
     ("set_chimera", C.c_int, [_vp, C.c_int32, _ip, _ip, _dp]),
     ("set_imports", C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),
+    ("set_exchange", C.c_int, [_vp, C.c_int32]),
+    ("exchange_rate", C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),
     ("set_gas", C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp, _dp]),
     ("upload_state", C.c_int, [_vp, C.c_int32, C.c_int32, _dp, _u8p]),
     ("download_state", C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),

@@ -92,6 +92,7 @@ struct FamHost {
   DevBuf<double> imp;                        // the coupler's imports [v][NI] (ice_gpu_set_imports)
   DevBuf<EmptyScan> escan;                   // bound_empty_dt's reductions
   bool have_imp = false;
+  DevBuf<double> xstep;                      // the step's weighted source, slots 1-4 and energy [5][NI]
 };
 
 
@@ -108,6 +109,7 @@ struct ice_gpu_ctx {
   bool have_gas = false;
   std::vector<bool> have_block;
   bool have_records = false;
+  bool exchange = false;  // two-way coupling: the step's weighted source is kept for the gas
   int nchim = 0;          // 102 records of the table
   bool have_chimera = true;   // their donors are set (ice_gpu_set_chimera)
   FamHost fam[kMaxF];
@@ -230,6 +232,8 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   F.connF = H.connF.p;
   F.cdon = H.cdon.p; F.cw = H.cw.p;
   F.imports = H.have_imp ? H.imp.p : nullptr;
+  F.xstep = (c->exchange && c->P.coupled) ? H.xstep.p : nullptr;
+  F.xfirst = srk == 1;
   F.resid = H.resid.p;
   static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
   F.rk = RKC[c->P.nrk - 1][srk - 1];
@@ -956,6 +960,42 @@ int ice_gpu_set_imports(ice_gpu_ctx* c, int32_t b1, int32_t p1, const double* im
   for (int v = 0; v < H.nc; ++v) {
     for (long long q = 0; q < n; ++q) col[(size_t)q] = imports ? imports[q * H.nc + v] : 0.0;
     CK(cudaMemcpy(H.imp.p + (long long)v * c->NI + B.ioff, col.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+// Two-way coupling (twcoupled): every stage adds its source to the step's running sum
+// (add_stage_source, Mod_Explicit.f90:257-280), which the gas reads after the step as exchange_rate.
+int ice_gpu_set_exchange(ice_gpu_ctx* c, int32_t on) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (on && !c->P.coupled) return fail(c, ICE_GPU_EINVAL, "set_exchange: the run is not coupled to a gas");
+  CK(cudaStreamSynchronize(c->stream));
+  if (on && !c->exchange)
+    for (int p = 0; p < c->P.nfam; ++p) {
+      FamHost& H = c->fam[p];
+      CK(H.xstep.alloc((size_t)5 * c->NI));
+      CK(cudaMemset(H.xstep.p, 0, (size_t)5 * c->NI * sizeof(double)));
+    }
+  c->exchange = on != 0;
+  free_graphs(c);
+  return 0;
+}
+
+// exchange_rate (coupling/Mod_Exchange.f90:60-78) of every cell of family p in block b over the last step,
+// (5, ni, nj, nk): the mass, momentum and energy the gas receives per unit volume and time, the
+// negated step source of the family (no burning family: nothing generated, no heat of reaction).
+int ice_gpu_exchange_rate(ice_gpu_ctx* c, int32_t b1, int32_t p1, double* x) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam || !x) return fail(c, ICE_GPU_EINVAL, "exchange_rate: bad arguments");
+  if (!c->exchange) return fail(c, ICE_GPU_ENOTREADY, "exchange_rate: exchange is off (ice_gpu_set_exchange)");
+  const DBlock& B = c->hblk[b1 - 1];
+  const long long n = (long long)B.ni * B.nj * B.nk;
+  std::vector<double> col((size_t)n);
+  CK(cudaStreamSynchronize(c->stream));
+  for (int m = 0; m < 5; ++m) {
+    CK(cudaMemcpy(col.data(), c->fam[p1 - 1].xstep.p + (long long)m * c->NI + B.ioff, (size_t)n * sizeof(double),
+                  cudaMemcpyDeviceToHost));
+    for (long long q = 0; q < n; ++q) x[q * 5 + m] = -col[(size_t)q];
   }
   return 0;
 }

@@ -731,6 +731,7 @@ k_stage(Geo G, FamDev F, const Tile* tiles, int TX, int TY, int KZ, int write_r,
       double s[nc];
 #pragma unroll
       for (int v = 0; v < nc; ++v) s[v] = F.coupled ? F.S[(long long)v * G.NI + q] : 0.0;
+      if (F.xstep) accumulate_source<CL>(F.xstep, G.NI, q, s, F.xfirst, F.rk);
       const double dt = F.dt ? F.dt[q] : *F.dtg;
       const double vol = G.vol[q];
 #pragma unroll

@@ -99,6 +99,8 @@ struct FamDev {              // what the kernels of one family read
   const int4* cdon;          // chimera donors: 0-based block, i, j, k
   const double* cw;          // chimera donor weights
   const double* imports;     // [v][NI]: the coupler's rates into the cells, or null
+  double* xstep;             // [5][NI]: the step's weighted source in slots 1-4 and the energy slot, or null
+  int xfirst;                // this stage starts the running sum (stage 1)
   double* resid;             // IRS: [v][NI]
   double rk;
   int write_tau;

@@ -494,6 +494,23 @@ template <int CL, int RS, typename R> __device__ __forceinline__ void riemann(co
   else rusanov<CL>(p1, p4, n, f, cp);
 }
 
+// ------------------------------------------------------------------ exchange
+// add_stage_source (Mod_Explicit.f90:257-280) for one cell: the source of slots 1-4 and of the energy slot
+// (ie) added to the step's running sum with RK_accumulate's weights (Lib_RK.f90:28-44): stage 1 starts
+// it, stage k > 1 makes it (sum + source) * c_k, so that after the last stage it holds what the update
+// integrated over the step.
+template <int CL>
+__device__ __forceinline__ void accumulate_source(double* xstep, long long NI, long long q, const double* s, int first,
+                                                  double ck) {
+  constexpr int ie = NC<CL>::v == 12 ? 10 : NC<CL>::v == 7 ? 5 : 4;
+  const double sv[5] = {s[0], s[1], s[2], s[3], s[ie]};
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    double* a = xstep + (long long)m * NI + q;
+    *a = first ? sv[m] : (*a + sv[m]) * ck;
+  }
+}
+
 // ------------------------------------------------------------------ sensor
 // SD_rho (Lib_Shock_Detector.f90:17-42): the Jameson weight of a cell from its density and its six
 // neighbours' (r1, r2 along x, r3, r4 along y, r5, r6 along z).

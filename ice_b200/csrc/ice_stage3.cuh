@@ -447,6 +447,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
         for (int v = 0; v < nc; ++v) s[v] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)sr[v];
         if (F.write_tau) F.tau[q] = (double)tau;
       }
+      if (F.xstep) accumulate_source<CL>(F.xstep, G.NI, q, s, F.xfirst, F.rk);
       const double dt = F.dt ? F.dt[q] : *F.dtg;
       const double vol = G.vol[q];
       double rd[nc];

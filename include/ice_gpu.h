@@ -214,6 +214,18 @@ int ice_gpu_set_gas(ice_gpu_ctx* ctx, int32_t b, const double* prim5, const doub
  * bound_removal_dt (numerics/time/Mod_dt.f90:134-242) for a coupled family. */
 int ice_gpu_set_imports(ice_gpu_ctx* ctx, int32_t b, int32_t p, const double* imports);
 
+/* Two-way coupling on (on != 0) or off: every stage then adds its source to the step's running sum,
+ * weighted as the update weighs the stages, for ice_gpu_exchange_rate.
+ * replaces: add_stage_source and hand_step_source (numerics/time/explicit/Mod_Explicit.f90:257-300)
+ * of a twcoupled run. */
+int ice_gpu_set_exchange(ice_gpu_ctx* ctx, int32_t on);
+
+/* What family p (1-based) gave the gas from every cell of block b over the last step, per unit volume
+ * and time: x (5, ni, nj, nk) = mass, momentum (3), energy (no burning family: nothing is generated
+ * and there is no heat of reaction).
+ * replaces: exchange_rate (coupling/Mod_Exchange.f90:60-78). */
+int ice_gpu_exchange_rate(ice_gpu_ctx* ctx, int32_t b, int32_t p, double* x);
+
 /* State of family p (1-based) in block b: prim (ncond, 1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc),
  * gc = 2; inj the injected-ghost flags on the same cells (NULL: all false).
  * replaces: setup_cond's result (driver/Mod_Phase.f90:66-124). */

@@ -36,6 +36,7 @@
 typedef struct {
     double *prim, *prim_old, *residual, *source, *dt, *tau, *beta;
     double *imports;      /* the coupler's rates (nc per interior cell), or NULL */
+    double *source_step;  /* two-way coupling: the step's weighted source (nc per interior cell) */
     unsigned char *inj;
 } ofam;
 
@@ -61,6 +62,7 @@ typedef struct orc_ctx {
     orec* bc;
     int nchim, have_chim; /* chimera records and whether their donors are set */
     int have_imp[MAXF];   /* the family has the coupler's imports (set_imports) */
+    int exchange;         /* two-way coupling: the step's source is kept (set_exchange) */
     int* cdon;            /* chimera donors: block, i, j, k (1-based) */
     double* cw;           /* their weights */
     int* grp_first;       /* nfam+1, 0-based into grp */
@@ -154,7 +156,7 @@ int orc_destroy(orc_ctx* c) {
         for (int p = 0; p < c->P.nfam; ++p) {
             ofam* F = &B->fam[p];
             free(F->prim); free(F->prim_old); free(F->residual); free(F->source);
-            free(F->dt); free(F->beta); free(F->tau); free(F->inj); free(F->imports);
+            free(F->dt); free(F->beta); free(F->tau); free(F->inj); free(F->imports); free(F->source_step);
         }
     }
     free(c->blk); free(c->bc); free(c->grp_first); free(c->grp); free(c->cdon); free(c->cw);
@@ -1078,6 +1080,48 @@ static void add_births(orc_ctx* c, int p) {
     }
 }
 
+/* Two-way coupling on or off (twcoupled): the step's weighted source of every family is kept. */
+int orc_set_exchange(orc_ctx* c, int on) {
+    if (on && !c->P.coupled) return seterr(c, ICE_GPU_EINVAL, "set_exchange: the run is not coupled to a gas");
+    if (on && !c->exchange)
+        for (int b = 0; b < c->nb; ++b) for (int p = 0; p < c->P.nfam; ++p) {
+            oblk* B = &c->blk[b];
+            free(B->fam[p].source_step);
+            B->fam[p].source_step = (double*)calloc((size_t)nc_of(c, p)*ncells(B), sizeof(double));
+        }
+    c->exchange = on != 0;
+    return 0;
+}
+
+/* add_stage_source (Mod_Explicit.f90:257-280) with RK_accumulate (Lib_RK.f90:28-44): stage 1 starts the
+ * running sum, stage k > 1 makes it (sum + source) * c_k. After the last stage it is the step's source
+ * (hand_step_source, Mod_Explicit.f90:284-300). With one stage it is that stage's source. */
+static void add_stage_source(orc_ctx* c, int p, int srk) {
+    static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
+    int nc = nc_of(c, p);
+    double ck = RKC[c->P.nrk - 1][srk - 1];
+    for (int b = 0; b < c->nb; ++b) {
+        oblk* B = &c->blk[b];
+        ofam* F = &B->fam[p];
+        for (long q = 0; q < (long)nc*ncells(B); ++q)
+            F->source_step[q] = srk == 1 ? F->source[q] : (F->source_step[q] + F->source[q]) * ck;
+    }
+}
+
+/* exchange_rate (Mod_Exchange.f90:60-78) of family p1 in block b1 over the last step: (5, ni, nj, nk) of
+ * mass, momentum and energy the gas receives, the negated step source (no burning family). */
+int orc_exchange_rate(orc_ctx* c, int b1, int p1, double* x) {
+    if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam || !x) return seterr(c, ICE_GPU_EINVAL, "exchange_rate: bad arguments");
+    if (!c->exchange) return seterr(c, ICE_GPU_ENOTREADY, "exchange_rate: exchange is off (set_exchange)");
+    int p = p1 - 1, nc = nc_of(c, p), ie = o_nbase(c->P.fam[p].closure) - 2;
+    oblk* B = &c->blk[b1 - 1];
+    for (long q = 0; q < ncells(B); ++q) {
+        const double* a = B->fam[p].source_step + (long)nc*q;
+        x[5*q] = -a[0]; x[5*q + 1] = -a[1]; x[5*q + 2] = -a[2]; x[5*q + 3] = -a[3]; x[5*q + 4] = -a[ie];
+    }
+    return 0;
+}
+
 /* --------------------------------------------------------------- norm */
 static void residual_norm(orc_ctx* c) {
     int nf = c->P.nfam;
@@ -1141,6 +1185,7 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
         for (int srk = 1; srk <= c->P.nrk; ++srk) {
             for (int b = 0; b < c->nb; ++b) memset(c->blk[b].fam[p].residual, 0, sizeof(double)*nc_of(c, p)*ncells(&c->blk[b]));
             if (c->P.coupled) compute_source(c, p);
+            if (c->P.coupled && c->exchange) add_stage_source(c, p, srk);
             compute_ghost(c, p);
             compute_beta(c, p);
             if (compute_bound(c, p)) { c->status |= ICE_GPU_ST_BAD_RECON; return ICE_GPU_ESTATE; }

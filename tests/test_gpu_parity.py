@@ -187,6 +187,28 @@ def test_multiblock_imports(gpu, orc, steady):
     assert err <= TOL, err
 
 
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32FLUX], ids=["fp64", "fp32flux"])
+def test_exchange_rates(gpu, orc, prec):
+    # two-way coupling: the rates the gas receives from every family over a step (3 RK stages). The
+    # plain form against the oracle to 1e-12 of each component's largest value; the chosen form to 1e-4
+    make = lambda: configs.multiblock_tree(nblocks=5, seed=4, lo=5, hi=10, steps=4, precision=prec)
+    cg, co = make(), make()
+    cg.numerics.precision = prec
+    co.numerics.precision = abi.PREC_FP64
+    sg, so = Solver(cg, gpu), Solver(co, orc)
+    assert gpu.set_exchange(sg.ctx, 1) == 0 and orc.set_exchange(so.ctx, 1) == 0
+    assert sg.step(4).status == 0 and so.step(4).status == 0
+    tol = TOL if prec == abi.PREC_FP64 else 1e-4
+    for b, (ni, nj, nk) in enumerate(cg.dims):
+        for p in range(len(cg.families)):
+            xg, xo = np.zeros((nk, nj, ni, 5)), np.zeros((nk, nj, ni, 5))
+            assert gpu.exchange_rate(sg.ctx, b + 1, p + 1, abi.ptr(xg)) == 0
+            assert orc.exchange_rate(so.ctx, b + 1, p + 1, abi.ptr(xo)) == 0
+            for m in range(5):
+                scale = max(float(np.max(np.abs(xo[..., m]))), 1e-300)
+                assert float(np.max(np.abs(xg[..., m] - xo[..., m]))) <= tol * scale, (b, p, m)
+
+
 def _irs(case):
     case.numerics.irs = True
     case.numerics.irs_beta = 0.5
