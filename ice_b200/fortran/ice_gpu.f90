@@ -42,7 +42,8 @@ module ice_gpu
   end type ice_gpu_step_out_t
 
   public :: ice_gpu_create, ice_gpu_set_block, ice_gpu_set_records, ice_gpu_set_chimera, ice_gpu_set_gas, &
-            ice_gpu_set_imports, ice_gpu_step_host, ice_gpu_upload_state, &
+            ice_gpu_set_imports, ice_gpu_set_exchange, ice_gpu_exchange_rate, ice_gpu_step_host, &
+            ice_gpu_upload_state, &
             ice_gpu_download_state, ice_gpu_set_time, ice_gpu_step, ice_gpu_residual_norm, ice_gpu_update_params, &
             ice_gpu_last_error, ice_gpu_destroy, ice_gpu_pair_connections
 
@@ -75,6 +76,19 @@ module ice_gpu
       type(c_ptr), value         :: ctx
       integer(c_int32_t), value  :: b, p
       real(c_double), intent(in) :: imports(*)
+    end function
+
+    integer(c_int) function ice_gpu_set_exchange(ctx, on) bind(C, name='ice_gpu_set_exchange')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value        :: ctx
+      integer(c_int32_t), value :: on
+    end function
+
+    integer(c_int) function ice_gpu_exchange_rate(ctx, b, p, x) bind(C, name='ice_gpu_exchange_rate')
+      import :: c_int, c_int32_t, c_double, c_ptr
+      type(c_ptr), value          :: ctx
+      integer(c_int32_t), value   :: b, p
+      real(c_double), intent(out) :: x(*)
     end function
 
     integer(c_int) function ice_gpu_step_host(ctx, nsteps, prim_in, prim_out, out) bind(C, name='ice_gpu_step_host')
