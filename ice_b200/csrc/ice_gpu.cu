@@ -106,6 +106,9 @@ struct ice_gpu_ctx {
   long long NG = 0, NI = 0, NR = 0, NF[3] = {0, 0, 0};
   DevBuf<DBlock> blk;
   DevBuf<double> face[3], vol, dl, M, gas;
+  DevBuf<float4> facef[3];  // the FP32-flux form's geometry (Geo::ff, dlf), rounded from the FP64 arrays
+  DevBuf<float> dlf;
+  bool geo32_ok = false;
   bool have_gas = false;
   std::vector<bool> have_block;
   bool have_records = false;
@@ -248,7 +251,41 @@ static Geo make_geo(ice_gpu_ctx* c) {
   G.NG = c->NG; G.NI = c->NI; G.NR = c->NR;
   for (int d = 0; d < 3; ++d) { G.NF[d] = c->NF[d]; G.face[d] = c->face[d].p; }
   G.vol = c->vol.p; G.dl = c->dl.p; G.M = c->M.p; G.gas = c->gas.p;
+  for (int d = 0; d < 3; ++d) G.ff[d] = c->facef[d].p;
+  G.dlf = c->dlf.p;
   return G;
+}
+
+__global__ void k_face32(const double* f, long long NF, float4* out) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < NF; q += (long long)gridDim.x * blockDim.x)
+    out[q] = make_float4((float)f[q], (float)f[NF + q], (float)f[2 * NF + q], (float)f[3 * NF + q]);
+}
+
+__global__ void k_dl32(const double* dl, long long n, float* out) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    out[q] = (float)dl[q];
+}
+
+// The FP32-flux form's geometry: the face normals and areas packed per face and the cell lengths in
+// single precision, rounded as the kernels rounded each value on reading (allocated once, so that
+// captured graphs keep their pointers; converted again after any ice_gpu_set_block).
+static int build_geo32(ice_gpu_ctx* c) {
+  if (c->P.precision != ICE_PREC_FP32FLUX || c->geo32_ok) return 0;
+  bool fresh = false;
+  for (int d = 0; d < 3; ++d) {
+    if (!c->facef[d].p && c->NF[d] > 0) { CK(c->facef[d].alloc((size_t)c->NF[d])); fresh = true; }
+    if (c->NF[d] > 0) {
+      k_face32<<<grid_of(c->NF[d]), 256, 0, c->stream>>>(c->face[d].p, c->NF[d], c->facef[d].p);
+      CK(cudaGetLastError());
+    }
+  }
+  if (!c->dlf.p) { CK(c->dlf.alloc((size_t)3 * c->NR)); fresh = true; }
+  k_dl32<<<grid_of(3 * c->NR), 256, 0, c->stream>>>(c->dl.p, 3 * c->NR, c->dlf.p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  if (fresh) free_graphs(c);          // graphs captured before the buffers existed hold null pointers
+  c->geo32_ok = true;
+  return 0;
 }
 
 // ---------------------------------------------------------------- kernel dispatch
@@ -648,6 +685,7 @@ int ice_gpu_set_block(ice_gpu_ctx* c, int32_t b1, const double* f1, const double
     CK(cudaMemcpy(c->M.p + (long long)comp * c->NI + B.ioff, tmp.data(), ncell * sizeof(double), cudaMemcpyHostToDevice));
   }
   c->have_block[b1 - 1] = true;
+  c->geo32_ok = false;
   return 0;
 }
 
@@ -1025,6 +1063,7 @@ static int finish_step(ice_gpu_ctx* c, ice_gpu_step_out* out, float dms);
 int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
   if (!c) return ICE_GPU_EINVAL;
   if (int rc = check_ready(c)) return rc;
+  if (int rc = build_geo32(c)) return rc;
   if (nsteps < 0) return fail(c, ICE_GPU_EINVAL, "step: nsteps %d", nsteps);
   cudaStream_t s = c->stream;
   if (c->profiling) {
@@ -1094,6 +1133,7 @@ int ice_gpu_step_host(ice_gpu_ctx* c, int32_t nsteps, const double* const* prim_
                       ice_gpu_step_out* out) {
   if (!c) return ICE_GPU_EINVAL;
   if (int rc = check_ready(c)) return rc;
+  if (int rc = build_geo32(c)) return rc;
   if (nsteps < 1) return fail(c, ICE_GPU_EINVAL, "step_host: nsteps %d", nsteps);
   if (!prim_in || !prim_out) return fail(c, ICE_GPU_EINVAL, "step_host: null array list");
   const int nf = c->P.nfam;

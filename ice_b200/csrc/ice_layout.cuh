@@ -29,6 +29,10 @@ struct Geo {                 // geometry shared by the families
   const double* dl;          // 3 SoA components of NR
   const double* M;           // 9 SoA components of NI (column-major c(3,3))
   const double* gas;         // 9 SoA components of NI: rho u v w T R gam k mu
+  // the FP32-flux form's copies of the face geometry (nx, ny, nz, A of a face in one 16-byte word) and
+  // of the cell lengths, rounded once from the FP64 arrays above (null in the plain form)
+  const float4* ff[3];
+  const float* dlf;
 };
 
 struct DRec {                // one boundary record, 0-based cells

@@ -109,6 +109,20 @@ __device__ __forceinline__ bool states_from_slopes(const QL& ql, const R* sl, R 
   return false;
 }
 
+// Normal and area of face fi along d: the FP64 arrays in the plain form, the packed single-precision
+// copy (one 16-byte load, the same roundings) in the FP32-flux form.
+template <typename R>
+__device__ __forceinline__ void face_geometry(const Geo& G, int d, long long fi, R* nrm, R& area) {
+  if constexpr (sizeof(R) == 4) {
+    const float4 f = G.ff[d][fi];
+    nrm[0] = f.x; nrm[1] = f.y; nrm[2] = f.z; area = f.w;
+  } else {
+    const long long NF = G.NF[d];
+    const double* fc = G.face[d];
+    nrm[0] = fc[fi]; nrm[1] = fc[NF + fi]; nrm[2] = fc[2 * NF + fi]; area = fc[3 * NF + fi];
+  }
+}
+
 template <typename S, int NP> struct SmemStencil {     // q(s, v): stencil cell s of a staged plane
   const S* P; int base, st;
   __device__ __forceinline__ S operator()(int s, int v) const { return P[v * NP + base + s * st]; }
@@ -128,10 +142,16 @@ __device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, 
   constexpr int nc = NC<CL>::v;
   const int c = d == 0 ? i : j;
   const int n = d == 0 ? B.ni : B.nj;
-  const double* dl = G.dl + (long long)d * G.NR;
   const long long r0 = ridx(B, i, j, k);
   const long long rs = d == 0 ? 1LL : (long long)(B.ni + 2);
-  R l0 = (R)dl[r0 - rs], l1 = (R)dl[r0], l2 = (R)dl[r0 + rs], l3 = (R)dl[r0 + 2 * rs];
+  R l0, l1, l2, l3;
+  if constexpr (sizeof(R) == 4) {
+    const float* dl = G.dlf + (long long)d * G.NR;
+    l0 = dl[r0 - rs]; l1 = dl[r0]; l2 = dl[r0 + rs]; l3 = dl[r0 + 2 * rs];
+  } else {
+    const double* dl = G.dl + (long long)d * G.NR;
+    l0 = dl[r0 - rs]; l1 = dl[r0]; l2 = dl[r0 + rs]; l3 = dl[r0 + 2 * rs];
+  }
   if (c == 0 || c == n - 2) {
     const long long gs = gstride(B, d);
     const long long g0 = gidx(B, i, j, k) - gs;
@@ -144,10 +164,8 @@ __device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, 
   SmemStencil<R, Shape<CL>::P> q{P, base, st};
   const bool bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
   const long long fi = fidx(B, d, i, j, k, c + 1);
-  const long long NF = G.NF[d];
-  const double* fc = G.face[d];
-  R nrm[3] = {(R)fc[fi], (R)fc[NF + fi], (R)fc[2 * NF + fi]};
-  R area = (R)fc[3 * NF + fi];
+  R nrm[3], area;
+  face_geometry<R>(G, d, fi, nrm, area);
   riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
   for (int v = 0; v < nc; ++v) flux[v] = fl[v] * area;
@@ -249,10 +267,16 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   bool fz = true;
   bool bad = false;
   auto zslope = [&](int sm, int s0, int sp, int c, R* s, R& dlc, bool& first) {
-    const double* dl = G.dl + 2 * G.NR;
     const long long r0 = ridx(B, i, j, c);
     const long long rs = (long long)(B.ni + 2) * (B.nj + 2);
-    R lm = (R)dl[r0 - rs], l0 = (R)dl[r0], lp = (R)dl[r0 + rs];
+    R lm, l0, lp;
+    if constexpr (sizeof(R) == 4) {
+      const float* dl = G.dlf + 2 * G.NR;
+      lm = dl[r0 - rs]; l0 = dl[r0]; lp = dl[r0 + rs];
+    } else {
+      const double* dl = G.dl + 2 * G.NR;
+      lm = dl[r0 - rs]; l0 = dl[r0]; lp = dl[r0 + rs];
+    }
     const long long g = gidx(B, i, j, c);
     if (c == 0 && F.inj[g - B.pxy]) lm = (R)0;
     if (c == B.nk - 1 && F.inj[g + B.pxy]) lp = (R)0;
@@ -266,10 +290,8 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     const SmemCell<R, ST_P> ql{plane(sl), pos}, qr{plane(sr), pos};
     bad |= states_from_slopes<CL, R>(ql, sa, da, fa, qr, sb, db, fb, bf, pl, pr);
     const long long fi = fidx(B, 2, i, j, c, c + 1);
-    const long long NF = G.NF[2];
-    const double* fc = G.face[2];
-    R nrm[3] = {(R)fc[fi], (R)fc[NF + fi], (R)fc[2 * NF + fi]};
-    R area = (R)fc[3 * NF + fi];
+    R nrm[3], area;
+    face_geometry<R>(G, 2, fi, nrm, area);
     R fl[nc];
     riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
