@@ -267,12 +267,20 @@ def e2e_run(lib, case, steps):
 
 
 def allmax(dist, x: float) -> float:
+    """The largest x over the ranks (a device tensor over NCCL, a host tensor over gloo)."""
     if not dist:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(dist, cells: int, steps: int, world: int, ms: float) -> float:
+    """Cell-updates/s of the whole job: every rank steps its own replica of `cells` cells, and the job
+    takes as long as its slowest rank."""
+    return cells * steps * world / (allmax(dist, ms) * 1e-3)
 
 
 def run_surrogate(args, rank, world, dist):
@@ -310,7 +318,7 @@ def run_surrogate(args, rank, world, dist):
     c1 = (C.c_int64 * 3)()
     lib.surrogate_stats(sur.ctx, c1)
     ms = allmax(dist, out.device_ms)
-    value = cells * args.steps * world / (ms * 1e-3)
+    value = whole_job_rate(dist, cells, args.steps, world, out.device_ms)
     st_sur = sur.download_all()
     sur.close()
     plain = Solver(case, lib)
@@ -353,7 +361,7 @@ def run_ours(args, rank, world, dist):
     if out.status != 0:
         raise SystemExit(f"step status {out.status}")
     ms = allmax(dist, out.device_ms)
-    value = cells * args.steps * world / (ms * 1e-3)
+    value = whole_job_rate(dist, cells, args.steps, world, out.device_ms)
     if args.timed_only:         # the timed region alone (profiler runs)
         chosen.close()
         if rank == 0:
