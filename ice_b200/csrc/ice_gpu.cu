@@ -5,7 +5,7 @@
 // numerics/time/explicit/Mod_Explicit.f90:11-245). Every array is resident in HBM; a step is a
 // CUDA graph of:
 //   k_begin        iteration counters, dt reset                      (Mod_Explicit.f90:40-44)
-//   k_dt           per-cell CFL dt + global min (FP64, warp shuffles) (Mod_dt.f90:11-112,256-275)
+//   k_dt_all       per-cell CFL dt of every family + global min (FP64)  (Mod_dt.f90:11-112,256-275)
 //   k_time         dtglobal, time += dt                               (Mod_Explicit.f90:67-73)
 //   per family, per RK stage:
 //     k_ghost      both ghost layers from the record list, block
@@ -316,18 +316,14 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   else launch_family_ag(a);
 }
 
-static void launch_dt(ice_gpu_ctx* c, int p, int phase, cudaStream_t s) {
+// A family the coupler feeds or drains: bound_empty_dt and bound_removal_dt (Mod_Explicit.f90:57-60),
+// after every family's compute_dt (k_dt_all).
+static void launch_dt_bounds(ice_gpu_ctx* c, int p, int phase, cudaStream_t s) {
+  if (!c->fam[p].have_imp) return;
   Geo G = make_geo(c);
   FamDev F = make_famdev(c, p, 1, phase);
   double* dto = c->P.time_accurate ? nullptr : c->fam[p].dt.p;
   unsigned g = GRID(c->NI, 256);
-  switch (c->fam[p].closure) {
-    case ICE_CLOSURE_MK: k_dt<MK><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
-    case ICE_CLOSURE_IG: k_dt<IG><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
-    default: k_dt<AG><<<g, 256, 0, s>>>(G, F, c->st.p, c->P.cfl, c->P.cfl_ramp_iter, c->P.dt_max, c->P.tau_factor, c->P.ndir, dto); break;
-  }
-  // a family the coupler feeds or drains: bound_empty_dt and bound_removal_dt (Mod_Explicit.f90:57-60)
-  if (!c->fam[p].have_imp) return;
   EmptyScan* e = c->fam[p].escan.p;
   k_empty_init<<<1, 1, 0, s>>>(e);
   switch (c->fam[p].closure) {
@@ -354,7 +350,19 @@ static int next_phase(const ice_gpu_ctx* c, int phase) {
 // each family's RK stages (the families are independent of one another within a step).
 static void enqueue_step_dt(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*tick)(void*, int, cudaStream_t)) {
   k_begin<<<1, 1, 0, s>>>(c->st.p);
-  for (int p = 0; p < c->P.nfam; ++p) launch_dt(c, p, phase, s);
+  {
+    DtArgs a;
+    memset(&a, 0, sizeof a);
+    a.nf = c->P.nfam; a.ramp = c->P.cfl_ramp_iter; a.ndir = c->P.ndir;
+    a.cfl = c->P.cfl; a.dt_max = c->P.dt_max; a.tau_factor = c->P.tau_factor;
+    for (int p = 0; p < c->P.nfam; ++p) {
+      FamDev F = make_famdev(c, p, 1, phase);
+      a.f[p].Up = F.Up; a.f[p].tau = F.tau; a.f[p].coupled = F.coupled; a.f[p].closure = c->fam[p].closure;
+      a.f[p].dt_out = c->P.time_accurate ? nullptr : c->fam[p].dt.p;
+    }
+    k_dt_all<<<GRID(c->NI, 256), 256, 0, s>>>(make_geo(c), a, c->st.p);
+  }
+  for (int p = 0; p < c->P.nfam; ++p) launch_dt_bounds(c, p, phase, s);
   k_time<<<1, 1, 0, s>>>(c->st.p, c->P.time_accurate);
   if (tick) tick(c, KC_DT, s);
 }
@@ -380,7 +388,7 @@ static void prof_tick(void* vc, int cls, cudaStream_t s) {
 }
 
 static long long launches_per_step(const ice_gpu_ctx* c) {
-  long long n = 2 + c->P.nfam;
+  long long n = 3;
   for (int p = 0; p < c->P.nfam; ++p) n += c->fam[p].have_imp ? 3 : 0;
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
@@ -575,6 +583,8 @@ int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims
   for (int b = 0; b < nblocks; ++b) {
     int ni = dims[3 * b], nj = dims[3 * b + 1], nk = dims[3 * b + 2];
     if (ni < 1 || nj < 1 || nk < 1) return fail(nullptr, ICE_GPU_EINVAL, "block %d: dims %d %d %d", b + 1, ni, nj, nk);
+    if ((long long)ni * nj * nk >= (1LL << 31))
+      return fail(nullptr, ICE_GPU_EINVAL, "block %d: %lld cells, at most 2^31 - 1 per block", b + 1, (long long)ni * nj * nk);
     DBlock B;
     B.ni = ni; B.nj = nj; B.nk = nk;
     B.px = (ni + 4 + 1) & ~1;

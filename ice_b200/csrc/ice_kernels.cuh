@@ -71,6 +71,27 @@ __device__ __forceinline__ bool face_flux(const Geo& G, const FamDev& F, const D
   return bad;
 }
 
+// Normal and area of face fi along d: the FP64 arrays in the plain form, the packed single-precision
+// copy (one 16-byte load, the same roundings) in the FP32-flux form.
+template <typename R>
+__device__ __forceinline__ void face_geometry(const Geo& G, int d, long long fi, R* nrm, R& area) {
+  if constexpr (sizeof(R) == 4) {
+    const float4 f = G.ff[d][fi];
+    nrm[0] = f.x; nrm[1] = f.y; nrm[2] = f.z; area = f.w;
+  } else {
+    const long long NF = G.NF[d];
+    const double* fc = G.face[d];
+    nrm[0] = fc[fi]; nrm[1] = fc[NF + fi]; nrm[2] = fc[2 * NF + fi]; area = fc[3 * NF + fi];
+  }
+}
+
+// The length along d of the cell at ring index r, in the precision of R (the same rounding either way).
+template <typename R>
+__device__ __forceinline__ R cell_length(const Geo& G, int d, long long r) {
+  if constexpr (sizeof(R) == 4) return G.dlf[(long long)d * G.NR + r];
+  else return G.dl[(long long)d * G.NR + r];
+}
+
 // The Jameson weight of cell (i,j,k) of block B from the stage's density in global memory (the
 // boundary kernels; compute_beta, Mod_Fluxes.f90:366-389).
 template <typename R>
@@ -95,18 +116,17 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
   int ip = i + g0, jp = j + g1, kp = k + g2;
   int dir = (f + 1) / 2 - 1;
   R bv = beta_face ? (R)*beta_face : (F.sd ? beta_cell<R>(F, B, i, j, k) : (R)1);
-  R dl_g1 = (R)G.dl[(long long)dir * G.NR + ridx(B, ig, jg, kg)];
-  R dl_m = (R)G.dl[(long long)dir * G.NR + ridx(B, i, j, k)];
-  R dl_4 = (R)G.dl[(long long)dir * G.NR + ridx(B, ip, jp, kp)];
+  R dl_g1 = cell_length<R>(G, dir, ridx(B, ig, jg, kg));
+  R dl_m = cell_length<R>(G, dir, ridx(B, i, j, k));
+  R dl_4 = cell_length<R>(G, dir, ridx(B, ip, jp, kp));
   R dl0, dl1, dl2, dll, dlr;
   R pl[nc], pr[nc], fl[nc];
   bool bad;
   const double* P = F.Up;
-  long long NF = G.NF[dir];
   if (f % 2 == 1) {
     long long fi = fidx(B, dir, i, j, k, (dir == 0 ? i : dir == 1 ? j : k));   // the face below the cell
-    R nrm[3] = {(R)G.face[dir][fi], (R)G.face[dir][NF + fi], (R)G.face[dir][2 * NF + fi]};
-    R area = (R)G.face[dir][3 * NF + fi];
+    R nrm[3], area;
+    face_geometry<R>(G, dir, fi, nrm, area);
     dl0 = dl_g1; dl1 = (R)0.5*(dl_g1 + dl_m); dl2 = (R)0.5*(dl_m + dl_4);
     dll = (R)0.5*dl_g1; dlr = (R)0.5*dl_m;
     if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = (R)0.5*dl_m; dll = (R)0; }
@@ -119,8 +139,8 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
     for (int v = 0; v < nc; ++v) flux[v] = (double)(fl[v] * area);
   } else {
     long long fi = fidx(B, dir, i, j, k, (dir == 0 ? i : dir == 1 ? j : k) + 1);  // the face above the cell
-    R nrm[3] = {(R)G.face[dir][fi], (R)G.face[dir][NF + fi], (R)G.face[dir][2 * NF + fi]};
-    R area = (R)G.face[dir][3 * NF + fi];
+    R nrm[3], area;
+    face_geometry<R>(G, dir, fi, nrm, area);
     dl0 = (R)0.5*(dl_4 + dl_m); dl1 = (R)0.5*(dl_m + dl_g1); dl2 = dl_g1;
     dll = (R)0.5*dl_m; dlr = (R)0.5*dl_g1;
     if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = (R)0.5*dl_m; dlr = (R)0; }
@@ -153,38 +173,68 @@ __device__ __forceinline__ void decode(const DBlock& B, long long q, int& i, int
   k = (int)(l / B.nj);
 }
 
-// compute_dt / compute_dt_ (Mod_dt.f90:11-112, 256-275), every block of one family.
+// compute_dt for every family in one pass (Mod_dt.f90:11-112, 256-275; Mod_Explicit.f90:46-61): each
+// cell's metric rows are read once for all families; the cell's indices come from its block by 32-bit
+// arithmetic (ice_gpu_create refuses a block of 2^31 cells or more). Per family the operations of
+// compute_dt_ in its order; the global step is the smallest over every family and cell (an exact
+// minimum, so the order of the families does not matter).
+struct DtFam {
+  const double* Up;
+  const double* tau;
+  double* dt_out;   // the per-cell step (steady runs), or null
+  int closure, coupled;
+};
+struct DtArgs {
+  DtFam f[ICE_GPU_MAX_FAMILIES];
+  int nf, ramp, ndir;
+  double cfl, dt_max, tau_factor;
+};
+
 template <int CL>
-__global__ void __launch_bounds__(256) k_dt(Geo G, FamDev F, Status* st, double cfl, int ramp, double dt_max,
-                                            double tau_factor, int ndir, double* dt_out) {
+__device__ __forceinline__ double family_dt(const Geo& G, const DtFam& f, const DtArgs& a, long long q, long long g,
+                                            const double (*vs)[3], const double* gn, int it) {
+  constexpr int nc = NC<CL>::v;
+  double p[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) p[v] = f.Up[(long long)v * G.NG + g];
+  double rate = 0.0;
+  for (int d = 0; d < a.ndir; ++d)
+    rate = rate + (fabs(p[1]*vs[d][0] + p[2]*vs[d][1] + p[3]*vs[d][2]) + wavespeed<CL>(p, vs[d])) * gn[d];
+  double dt = (double)1e+5f;
+  if (rate > 0.0) dt = mn(dt, 1.0/rate);
+  dt = dt * a.cfl;
+  if (it <= a.ramp) dt = dt * (double)it / (double)a.ramp;
+  dt = mn(dt, a.dt_max);
+  if (f.coupled && a.tau_factor > 0.0) {
+    double tau = f.tau[q];
+    if (p[0] > kRhoEmpty && !not_finite(tau) && tau > 0.0) dt = mn(dt, a.tau_factor*tau);
+  }
+  if (f.dt_out) f.dt_out[q] = dt;
+  return dt;
+}
+
+__global__ void __launch_bounds__(256) k_dt_all(Geo G, DtArgs a, Status* st) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double dt = INFINITY;
   if (q < G.NI) {
     const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
-    int i, j, k; decode(B, q, i, j, k);
-    constexpr int nc = NC<CL>::v;
-    double p[nc];
-    long long g = gidx(B, i, j, k);
-#pragma unroll
-    for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
-    double rate = 0.0;
-    dt = (double)1e+5f;
-    for (int d = 0; d < ndir; ++d) {
+    const unsigned l = (unsigned)(q - B.ioff), ni = (unsigned)B.ni, nj = (unsigned)B.nj;
+    const unsigned i = l % ni, jk = l / ni, j = jk % nj, k = jk / nj;
+    const long long g = gidx(B, (int)i, (int)j, (int)k);
+    double vs[3][3], gn[3];
+    for (int d = 0; d < a.ndir; ++d) {
       double t0 = G.M[(long long)d * G.NI + q], t1 = G.M[(long long)(3 + d) * G.NI + q], t2 = G.M[(long long)(6 + d) * G.NI + q];
-      double gn = norm2_3(t0, t1, t2);
-      double vs[3] = {t0 / gn, t1 / gn, t2 / gn};
-      rate = rate + (fabs(p[1]*vs[0] + p[2]*vs[1] + p[3]*vs[2]) + wavespeed<CL>(p, vs)) * gn;
+      gn[d] = norm2_3(t0, t1, t2);
+      vs[d][0] = t0 / gn[d]; vs[d][1] = t1 / gn[d]; vs[d][2] = t2 / gn[d];
     }
-    if (rate > 0.0) dt = mn(dt, 1.0/rate);
-    dt = dt * cfl;
-    int it = st->iter;
-    if (it <= ramp) dt = dt * (double)it / (double)ramp;
-    dt = mn(dt, dt_max);
-    if (F.coupled && tau_factor > 0.0) {
-      double tau = F.tau[q];
-      if (p[0] > kRhoEmpty && !not_finite(tau) && tau > 0.0) dt = mn(dt, tau_factor*tau);
+    const int it = st->iter;
+    for (int p = 0; p < a.nf; ++p) {
+      const DtFam& f = a.f[p];
+      double d = f.closure == ICE_CLOSURE_MK ? family_dt<MK>(G, f, a, q, g, vs, gn, it)
+               : f.closure == ICE_CLOSURE_IG ? family_dt<IG>(G, f, a, q, g, vs, gn, it)
+                                             : family_dt<AG>(G, f, a, q, g, vs, gn, it);
+      dt = mn(dt, d);
     }
-    if (dt_out) dt_out[q] = dt;
   }
   // warp and block min; a positive double orders as its bits
   unsigned long long bits = (unsigned long long)__double_as_longlong(dt);

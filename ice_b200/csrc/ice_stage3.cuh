@@ -109,20 +109,6 @@ __device__ __forceinline__ bool states_from_slopes(const QL& ql, const R* sl, R 
   return false;
 }
 
-// Normal and area of face fi along d: the FP64 arrays in the plain form, the packed single-precision
-// copy (one 16-byte load, the same roundings) in the FP32-flux form.
-template <typename R>
-__device__ __forceinline__ void face_geometry(const Geo& G, int d, long long fi, R* nrm, R& area) {
-  if constexpr (sizeof(R) == 4) {
-    const float4 f = G.ff[d][fi];
-    nrm[0] = f.x; nrm[1] = f.y; nrm[2] = f.z; area = f.w;
-  } else {
-    const long long NF = G.NF[d];
-    const double* fc = G.face[d];
-    nrm[0] = fc[fi]; nrm[1] = fc[NF + fi]; nrm[2] = fc[2 * NF + fi]; area = fc[3 * NF + fi];
-  }
-}
-
 template <typename S, int NP> struct SmemStencil {     // q(s, v): stencil cell s of a staged plane
   const S* P; int base, st;
   __device__ __forceinline__ S operator()(int s, int v) const { return P[v * NP + base + s * st]; }
