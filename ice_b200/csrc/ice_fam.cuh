@@ -44,7 +44,7 @@ void launch_family_t(const LaunchArgs& a) {
     tick(KC_SOURCE);
   }
   if (a.nrec > 0) {
-    k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.recs, a.nrec);
+    k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.grecs, a.nrec);
     tick(KC_GHOST);
   }
   // the Jameson sensor: the staged stage kernel and the boundary kernels evaluate it from the

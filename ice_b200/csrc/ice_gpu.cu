@@ -73,6 +73,7 @@ struct FamHost {
   DevBuf<int> bmap;
   DevBuf<double> Rb, connF, resid, resid2, resid3, src;
   DevBuf<DRec> recs;
+  DevBuf<DRec> grecs;                        // the same records ordered for the ghost kernel (upload_recs)
   DevBuf<int> bfirst, blist, own;
   DevBuf<CUtensorMap> maps[3];               // per state buffer, per block: the staged kernel's TMA maps
   DevBuf<Tile> tiles3;                       // the staged kernel's tiles (the tile shape is the closure's)
@@ -297,7 +298,7 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   LaunchArgs a;
   a.G = make_geo(c);
   a.F = make_famdev(c, p, srk, phase);
-  a.recs = H.recs.p; a.nrec = H.nrec;
+  a.recs = H.recs.p; a.nrec = H.nrec; a.grecs = H.grecs.p;
   a.own = H.own.p; a.nown = H.nown;
   a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc;
   a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.KZ = c->KZ;
@@ -791,6 +792,32 @@ int ice_gpu_update_params(ice_gpu_ctx* c, const ice_gpu_params* P) {
   return 0;
 }
 
+// The family's device records (table order, which the boundary and connection kernels index), and a
+// copy for the ghost kernel ordered by block, face and cell with the first index fastest, so that the
+// threads of a warp fill neighbouring ghost cells of one face (a record's ghosts are its own, and what
+// it reads no other record writes: the order of the fills does not change a value).
+static int upload_recs(ice_gpu_ctx* c, FamHost& H) {
+  const std::vector<DRec>& dr = H.h_recs;
+  CK(H.recs.alloc(dr.size()));
+  CK(H.grecs.alloc(dr.size()));
+  if (dr.empty()) return 0;
+  CK(cudaMemcpy(H.recs.p, dr.data(), dr.size() * sizeof(DRec), cudaMemcpyHostToDevice));
+  std::vector<int> ord(dr.size());
+  for (size_t q = 0; q < ord.size(); ++q) ord[q] = (int)q;
+  std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+    const DRec& a = dr[x]; const DRec& b = dr[y];
+    if (a.b != b.b) return a.b < b.b;
+    if (a.f != b.f) return a.f < b.f;
+    if (a.k != b.k) return a.k < b.k;
+    if (a.j != b.j) return a.j < b.j;
+    return a.i < b.i;
+  });
+  std::vector<DRec> g(dr.size());
+  for (size_t q = 0; q < ord.size(); ++q) g[q] = dr[ord[q]];
+  CK(cudaMemcpy(H.grecs.p, g.data(), g.size() * sizeof(DRec), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 // build_local_bc_index + collect_boundary_cells + collect_owner_records
 // (parallel/Mod_GhostExchange.f90:103-360) for a device that owns every block.
 int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const double* rr) {
@@ -862,10 +889,9 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
       d.cd0 = d.cn1 = d.cn2 = 0;
     }
     H.nrec = (int)grp.size();
-    CK(H.recs.alloc(dr.size()));
-    if (!dr.empty()) CK(cudaMemcpy(H.recs.p, dr.data(), dr.size() * sizeof(DRec), cudaMemcpyHostToDevice));
     H.h_grp = grp;
     H.h_recs = dr;
+    if (int rc = upload_recs(c, H)) return rc;
     // boundary cells: block by block in cell order, the records of a cell by face (stable)
     H.h_first.clear(); H.h_list.clear();
     std::vector<int> bmap(c->NI, -1);
@@ -968,8 +994,7 @@ int ice_gpu_set_chimera(ice_gpu_ctx* c, int32_t nrec, const int32_t* nchi, const
         dw.push_back(weight[s]);
       }
     }
-    if (!H.h_recs.empty())
-      CK(cudaMemcpy(H.recs.p, H.h_recs.data(), H.h_recs.size() * sizeof(DRec), cudaMemcpyHostToDevice));
+    if (int rc = upload_recs(c, H)) return rc;
     CK(H.cdon.alloc(std::max<size_t>(dn.size(), 1)));
     CK(H.cw.alloc(std::max<size_t>(dw.size(), 1)));
     if (!dn.empty()) {

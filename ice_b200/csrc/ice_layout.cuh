@@ -128,6 +128,7 @@ struct LaunchArgs {
   Geo G;
   FamDev F;
   const DRec* recs; int nrec;
+  const DRec* grecs;                                 // the records in the ghost kernel's order
   const int* own; int nown;
   const int* bfirst; const int* blist; int nbc;
   const Tile* tiles; int ntile; int TX, TY, KZ;     // the 1-D stage kernel's tiles
