@@ -430,7 +430,76 @@ template <typename R> __device__ __forceinline__ void saurel(const R* p1, const 
   }
 }
 
+// The FP32-flux form's Rusanov flux with the two states of the face side by side in float2 pairs
+// (x: the left state, y: the right), so that one packed FFMA2 / FMUL2 / FADD2 does the work of the two
+// sides: the normal speeds, the closure's conservative variables, the pressure parts and the
+// normal pressure of the signal speeds. The same operations per side as rusanov's FP32 branch.
+__device__ __forceinline__ float2 sp2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+template <int CL> __device__ __forceinline__ void rusanov_pair(const float* p1, const float* p4, const float* n,
+                                                               float* f, float cp) {
+  constexpr int nc = NC<CL>::v;
+  float2 P[nc], C[nc], Q[nc];
+#pragma unroll
+  for (int v = 0; v < nc; ++v) P[v] = make_float2(p1[v], p4[v]);
+  const float2 n0 = sp2(n[0]), n1 = sp2(n[1]), n2 = sp2(n[2]);
+  const float2 un = fma2(P[3], n2, fma2(P[2], n1, mul2(P[1], n0)));
+  const float2 n2v = fma2(P[3], P[3], fma2(P[2], P[2], mul2(P[1], P[1])));
+  // conservative variables (prim2cons)
+  C[0] = P[0];
+  C[1] = mul2(P[0], P[1]); C[2] = mul2(P[0], P[2]); C[3] = mul2(P[0], P[3]);
+  float2 s = sp2(0.f);            // signal speeds
+#pragma unroll
+  for (int v = 0; v < nc; ++v) Q[v] = sp2(0.f);
+  const float eps = epsv<float>();
+  if constexpr (CL == MK) {
+    C[4] = fma2(mul2(P[0], sp2(cp)), P[4], mul2(mul2(sp2(0.5f), P[0]), n2v));
+    C[5] = P[5];
+  } else if constexpr (CL == IG) {
+    C[4] = fma2(P[0], n2v, mul2(sp2(3.f), P[4]));
+    C[5] = fma2(mul2(P[0], sp2(cp)), P[5], mul2(sp2(0.5f), C[4]));
+    C[6] = P[6];
+    Q[1] = mul2(P[4], n0); Q[2] = mul2(P[4], n1); Q[3] = mul2(P[4], n2);
+    Q[4] = mul2(mul2(sp2(2.f), P[4]), un); Q[5] = mul2(P[4], un);
+    const float2 pr = mul2(add2(add2(P[4], P[4]), P[4]), sp2(1.f / 3.f));
+    s = make_float2(sqrtf(3.f*pr.x / (P[0].x + eps)), sqrtf(3.f*pr.y / (P[0].y + eps)));
+  } else {
+    const float2 m0 = mul2(P[0], P[1]), m1 = mul2(P[0], P[2]), m2 = mul2(P[0], P[3]);
+    C[4] = fma2(m0, P[1], P[4]); C[5] = fma2(m0, P[2], P[5]); C[6] = fma2(m0, P[3], P[6]);
+    C[7] = fma2(m1, P[2], P[7]); C[8] = fma2(m1, P[3], P[8]); C[9] = fma2(m2, P[3], P[9]);
+    C[10] = fma2(mul2(P[0], sp2(cp)), P[10], mul2(sp2(0.5f), add2(add2(C[4], C[7]), C[9])));
+    C[11] = P[11];
+    const float2 p1n = fma2(P[6], n2, fma2(P[5], n1, mul2(P[4], n0)));
+    const float2 p2n = fma2(P[8], n2, fma2(P[7], n1, mul2(P[5], n0)));
+    const float2 p3n = fma2(P[9], n2, fma2(P[8], n1, mul2(P[6], n0)));
+    Q[1] = p1n; Q[2] = p2n; Q[3] = p3n;
+    Q[4] = mul2(mul2(sp2(2.f), P[1]), p1n); Q[5] = fma2(P[1], p2n, mul2(P[2], p1n)); Q[6] = fma2(P[1], p3n, mul2(P[3], p1n));
+    Q[7] = mul2(mul2(sp2(2.f), P[2]), p2n); Q[8] = fma2(P[2], p3n, mul2(P[3], p2n)); Q[9] = mul2(mul2(sp2(2.f), P[3]), p3n);
+    const float2 tr = add2(add2(P[4], P[7]), P[9]);
+    const float2 e = make_float2(eps / (P[0].x + eps), eps / (P[0].y + eps));
+    Q[10] = fma2(P[1], p1n, fma2(P[2], p2n, mul2(P[3], p3n)));
+    Q[10] = add2(Q[10], mul2(mul2(mul2(sp2(-0.5f), tr), un), e));
+    const float2 pnn = fma2(n2, p3n, fma2(n1, p2n, mul2(n0, p1n)));
+    s = make_float2(sqrtf(3.f*fmaxf(pnn.x, 0.f) / (P[0].x + eps)), sqrtf(3.f*fmaxf(pnn.y, 0.f) / (P[0].y + eps)));
+  }
+  float A = fabsf(un.x - s.x);
+  A = fmaxf(A, fabsf(un.y - s.y)); A = fmaxf(A, fabsf(un.x + s.x)); A = fmaxf(A, fabsf(un.y + s.y));
+  const float2 a = make_float2(un.x + A, un.y - A);
+#pragma unroll
+  for (int v = 0; v < nc; ++v) {
+    const float2 t = fma2(a, C[v], Q[v]);
+    f[v] = 0.5f * (t.x + t.y);
+  }
+}
+
 template <int CL, typename R> __device__ __forceinline__ void rusanov(const R* p1, const R* p4, const R* n, R* f, R cp) {
+  if constexpr (sizeof(R) == 4) {
+    rusanov_pair<CL>(p1, p4, n, f, cp);
+    return;
+  }
   constexpr int nc = NC<CL>::v;
   R c1[nc], c4[nc], f1[nc], f4[nc];
   R vn1 = p1[1]*n[0] + p1[2]*n[1] + p1[3]*n[2];
