@@ -34,12 +34,14 @@ void launch_family_t(const LaunchArgs& a) {
   cudaStream_t s = a.s;
   auto tick = [&](int cls) { if (a.tick) a.tick(a.tick_ctx, cls, s); };
   auto grid = [](long long n, int t) { return (unsigned)((n + t - 1) / t); };
-  // compute_source comes first in the stage (Mod_Explicit.f90:111-117): the staged stage kernel
-  // evaluates it per cell itself, unless the evaporation surrogate's source kernel runs first
+  // compute_source comes first in the stage (Mod_Explicit.f90:111-117). The staged stage kernel
+  // evaluates it per cell itself for a family without evaporation; an evaporating family's source
+  // (iterative, with lane-divergent trip counts) runs in its own kernel at full occupancy, or in the
+  // surrogate's source kernel, and the stage kernel reads it (FamDev::src_ready)
   if (a.F.coupled && a.mlp_img) {
     launch_source_mlp(CL, a, a.mlp_img, *a.mlp_norm);
     tick(KC_SOURCE);
-  } else if (a.F.coupled && a.ntile3 == 0) {
+  } else if (a.F.coupled && (a.ntile3 == 0 || a.F.src_ready)) {
     launch_source_of<CL>(a);
     tick(KC_SOURCE);
   }

@@ -242,7 +242,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   static const double RKC[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0/3.0}};
   F.rk = RKC[c->P.nrk - 1][srk - 1];
   F.write_tau = srk == c->P.nrk;
-  F.src_ready = sur_active(c, p) ? 1 : 0;
+  F.src_ready = (sur_active(c, p) || (c->staged && c->P.coupled && pf.evap != 0)) ? 1 : 0;
   return F;
 }
 
@@ -394,7 +394,7 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
     long long per = (H.nrec > 0 ? 1 : 0) + (c->P.shock_detector && !c->staged ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
-                    (c->P.coupled && (!c->staged || sur_active(c, p)) ? 1 : 0);
+                    (c->P.coupled && (!c->staged || sur_active(c, p) || c->P.fam[p].evap != 0) ? 1 : 0);
     per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
     n += per * c->P.nrk;
   }

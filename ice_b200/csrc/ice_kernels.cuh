@@ -634,8 +634,9 @@ __global__ void __launch_bounds__(256) k_source(Geo G, FamDev F) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= G.NI) return;
   const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
-  int i, j, k; decode(B, q, i, j, k);
-  const long long g = gidx(B, i, j, k);
+  const unsigned l = (unsigned)(q - B.ioff), ni = (unsigned)B.ni, nj = (unsigned)B.nj;   // < 2^31 cells a block
+  const unsigned i = l % ni, jk = l / ni, j = jk % nj, k = jk / nj;
+  const long long g = gidx(B, (int)i, (int)j, (int)k);
   R p[nc], gas[5], s[nc];
 #pragma unroll
   for (int v = 0; v < nc; ++v) p[v] = (R)F.Up[(long long)v * G.NG + g];

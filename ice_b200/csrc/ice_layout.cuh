@@ -108,7 +108,7 @@ struct FamDev {              // what the kernels of one family read
   double* resid;             // IRS: [v][NI]
   double rk;
   int write_tau;
-  int src_ready;             // S holds this stage's source already (the surrogate source kernel ran)
+  int src_ready;             // S holds this stage's source already (its own kernel or the surrogate's ran)
 };
 
 // bound_empty_dt's reductions over one family's cells, as the bits of non-negative doubles (which

@@ -440,7 +440,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       double s[nc];
 #pragma unroll
       for (int v = 0; v < nc; ++v) s[v] = 0.0;
-      if (F.coupled && F.src_ready) {           // the surrogate source kernel ran first
+      if (F.coupled && F.src_ready) {           // a source kernel ran first (evaporating family or surrogate)
 #pragma unroll
         for (int v = 0; v < nc; ++v) s[v] = F.S[(long long)v * G.NI + q];
       } else if (F.coupled) {                   // compute_source_ on the stage's state
