@@ -85,20 +85,23 @@ def sample_workload(name: str):
     return configs.riemann_1d(n=2000, steps=1), "the whole case"
 
 
-def algorithmic_bytes(case) -> float:
+def algorithmic_bytes(case, precision: int = abi.PREC_FP64) -> float:
     """Bytes one launch of the stage kernel must move per cell, averaged over the families and the RK
     stages: read U_(k-1) and U_0 and write U_k (24 nc, FP64 state); per direction the face normal and
-    area (32) and the cell length (8); the volume (8); the boundary map (4); in a coupled run the nine
-    frozen-gas values the source reads (72) and the relaxation time it writes on the last stage
-    (8 / nrk); the local dt (8) in steady mode; in 1-D runs the sensor weight (8) when the shock
-    detector is on (2-D and 3-D runs evaluate it from the staged density)."""
+    area (32) and the cell length (8) in FP64, or their single-precision copies (16 and 4) in the
+    FP32-flux form; the volume (8); the boundary map (4); in a coupled run the nine
+    frozen-gas values the fused source reads (72) and the relaxation time it writes on the last stage
+    (8 / nrk), or, for an evaporating family of a 2-D or 3-D run, the source its own kernel wrote
+    (8 nc); the local dt (8) in steady mode; in 1-D runs the sensor weight (8) when the shock detector
+    is on (2-D and 3-D runs evaluate it from the staged density)."""
     ndir = case.ndir
     nrk = case.params().nrk
     per = []
+    geo = 20 if precision == abi.PREC_FP32FLUX else 40
     for f in case.families:
-        b = 24 * f.nc + 40 * ndir + 8 + 4
+        b = 24 * f.nc + geo * ndir + 8 + 4
         if case.numerics.coupled:
-            b += 72 + 8 / nrk
+            b += 8 * f.nc if (ndir >= 2 and f.evap != "none") else 72 + 8 / nrk
         if case.numerics.shock_detector and ndir == 1:
             b += 8
         if not case.numerics.time_accurate:
@@ -110,8 +113,8 @@ def algorithmic_bytes(case) -> float:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one stage-kernel launch, from an
 # ncu capture of the 4-block case of the 48-block tree in the chosen form (second RK stage of each
 # family, 3,714,802 cells). The 48-block case is the same recipe with the same tile shapes, so its
-# launches move the same bytes per cell: traffic per launch = these x its cells.
-DRAM_BYTES_PER_CELL = {"MK": 393.97, "IG": 458.15, "AG": 626.42}
+# launches move about the same bytes per cell: traffic per launch = these x its cells.
+DRAM_BYTES_PER_CELL = {"MK": 328.85, "IG": 346.17, "AG": 578.97}
 
 
 def dram_traffic(case, workload: str, precision: int):
@@ -400,7 +403,7 @@ def run_ours(args, rank, world, dist):
         launches_per_step = nl.value / nprof
         nfam, nrk = len(case.families), case.params().nrk
         stage_ms = kt[KC_STAGE] / (nprof * nfam * nrk)
-        bpc = algorithmic_bytes(case)
+        bpc = algorithmic_bytes(case, prec)
         achieved = bpc * cells / (stage_ms * 1e-3) / 1e9
         peak, peak_kind = peaks()
         traffic = dram_traffic(case, args.workload, prec)
