@@ -6,17 +6,21 @@
 // CUDA graph of:
 //   k_begin        iteration counters, dt reset                      (Mod_Explicit.f90:40-44)
 //   k_dt_all       per-cell CFL dt of every family + global min (FP64)  (Mod_dt.f90:11-112,256-275)
+//   (k_empty_scan, k_empty_apply for a family with the coupler's imports: Mod_dt.f90:134-242)
 //   k_time         dtglobal, time += dt                               (Mod_Explicit.f90:67-73)
 //   per family, per RK stage:
+//     k_source     the source of an evaporating family (or a 1-D run), or the surrogate's
+//                  k_source_mlp                                        (Mod_Sources.f90:465-622)
 //     k_ghost      both ghost layers from the record list, block
 //                  connections as on-device copies in one HBM pool    (Lib_Ghost.f90:29-387)
 //     k_beta       Jameson sensor (when on; 1-D runs only)            (Mod_Fluxes.f90:366-389)
 //     k_conn       connection-face fluxes by their owner records      (Mod_BC_Fluxes.f90:151-170)
 //     k_bound      boundary cells, records summed in face order        (Mod_BC_Fluxes.f90:105-144)
-//     k_stage      interior face fluxes of a tile in shared memory, gathered per cell in the
-//                  odd-then-even order (Mod_Fluxes.f90:421-521), fused with the source
-//                  (Mod_Sources.f90:465-622), the residual (Lib_Residual.f90:147-156) and the RK
-//                  update with cons<->prim and the state checks (Lib_Newstate.f90:198-219)
+//     k_stage3     (k_stage in 1-D runs) interior face fluxes of a tile in shared memory, gathered
+//                  per cell in the odd-then-even order (Mod_Fluxes.f90:421-521), fused with the
+//                  source of a family without evaporation (Mod_Sources.f90:465-622), the residual
+//                  with the coupler's imports (Lib_Residual.f90:147-210) and the RK update with
+//                  cons<->prim and the state checks (Lib_Newstate.f90:198-219)
 //     (k_irs, k_update when implicit residual smoothing is on: Lib_IRS.f90:34-86)
 //
 // The state is stored structure-of-arrays, one contiguous array per variable over every block
