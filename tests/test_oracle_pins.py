@@ -9,6 +9,8 @@
 - test/unit/test_muscl_bounds.f90 B1-B5: the bounds of the limited slopes.
 - test/unit/test_empty_dt.f90 E1-E7: the steps of empty cells that the coupler's imports fill
   (bound_empty_dt), through a whole step (compute_dt gives the starting steps the unit test sets).
+- test/unit/test_radiation.f90 R1-R3: the radiative energy of a cell's source against its closed form.
+- test/unit/test_near_empty_cap.f90: the dispersion cap of near-empty IG and AG cells in cons_2_prim.
 """
 import math
 from pathlib import Path
@@ -223,3 +225,88 @@ def test_imports_are_checked(orc):
     assert orc.set_imports(s.ctx, 2, 1, abi.ptr(imp)) == abi.EINVAL
     imp[0, 0, 1, 0] = np.nan
     assert orc.set_imports(s.ctx, 1, 1, abi.ptr(imp)) == abi.EINVAL
+
+
+def _family(closure, **kw):
+    from ice_b200.case import Family
+    return Family(closure, **kw).to_c()
+
+
+def test_radiation_unit_cases(orc):
+    """R1-R3: MK drops of 30 um at rest at 2400 K in a gas at rest at 600 K, no drag, no heat, no
+    evaporation: the energy slot is eps sigma pi d^2 n (Tg^4 - Tp^4) to 1e-14 at emissivity 0.8, and 0
+    at emissivity 0 with every other slot unchanged (R4 needs an emissivity table, which this path
+    does not support)."""
+    import ctypes as C
+    sigma, d, rho_p, tp, tg = 5.670374419e-8, 30e-6, 1.0, 2400.0, 600.0
+    rg, gam, kg, mu = 287.05, 1.4, 0.05, 3e-5
+    n = rho_p / (2000.0 * math.pi / 6.0 * d ** 3)
+    cond = np.array([rho_p, 0.0, 0.0, 0.0, tp, n])
+    gas = np.array([101325.0 / (rg * tg), 0.0, 0.0, 0.0, tg])
+    out = {}
+    for name, em in (("grey", 0.8), ("off", 0.0)):
+        fam = _family("MK", rho_al=2000.0, cs_al=1000.0, emiss=em)
+        src = np.zeros(6)
+        tau = orc.cell_source(abi.CLOSURE["MK"], abi.ptr(cond), abi.ptr(gas), rg, gam, kg, mu, C.byref(fam),
+                              abi.DRAG["NoDrag"], abi.HEAT["NoHeat"], 0, abi.ptr(src))
+        out[name] = (src, tau)
+    q = 0.8 * sigma * math.pi * d * d * n * (tg ** 4 - tp ** 4)
+    assert abs(out["grey"][0][4] - q) <= 1e-14 * abs(q)                          # R1
+    s8, t8 = out["grey"]
+    s0, t0 = out["off"]
+    assert s0[4] == 0.0 and np.array_equal(s0[:4], s8[:4]) and s0[5] == s8[5] and t0 == t8    # R2, R3
+
+
+def test_near_empty_cap_unit_cases(orc):
+    import ctypes as C
+    cl, t0, eps = 1250.0, 300.0, float(np.float32(1e-25))
+    rho_empty, theta_cap = 1e-6, 1.0
+
+    def conv(closure, p):
+        fam = _family(closure, rho_al=2950.0, cs_al=cl)
+        p = np.array(p, dtype=np.float64)
+        c = np.zeros_like(p)
+        orc.prim2cons(abi.CLOSURE[closure], abi.ptr(p), abi.ptr(c), C.byref(fam))
+        return c
+
+    def back(closure, c):
+        fam = _family(closure, rho_al=2950.0, cs_al=cl)
+        c = np.array(c, dtype=np.float64)
+        q = np.zeros_like(c)
+        orc.cons2prim(abi.CLOSURE[closure], abi.ptr(c), abi.ptr(q), C.byref(fam))
+        return q
+
+    same_t = lambda t, ref: abs(t - ref) <= 8 * np.spacing(ref)
+    # IG (a): 1e-7 kg/m3 at P/rho = 10: P = rho theta_cap exactly, T that of the conservative variables
+    rho = 1e-7
+    c = conv("IG", [rho, 1.0, 0.5, 0.0, 10 * rho, t0, 1e3])
+    q = back("IG", c)
+    assert q[4] == q[0] * theta_cap
+    assert same_t(q[5], (c[5] - 0.5 * c[4]) / (cl * c[0] + eps)) and same_t(q[5], t0)
+    assert q[0] == rho and q[1] == c[1] / (c[0] + eps)
+    # (a') at rho_empty itself: capped; (b) 1e-5 (above rho_empty): untouched; below the cap: untouched
+    q = back("IG", conv("IG", [rho_empty, 1.0, 0.5, 0.0, 10 * rho_empty, t0, 1e3]))
+    assert q[4] == q[0] * theta_cap
+    q = back("IG", conv("IG", [1e-5, 1.0, 0.5, 0.0, 1e-4, t0, 1e3]))
+    assert abs(q[4] - 1e-4) <= 1e-12 * 1e-4
+    q = back("IG", conv("IG", [rho, 1.0, 0.5, 0.0, 0.5 * rho, t0, 1e3]))
+    assert abs(q[4] - 0.5 * rho) <= 1e-12 * 0.5 * rho
+    # AG (c): 1e-7 kg/m3, trace 30 rho: every component times 3 rho theta_cap / tr = 0.1
+    tens = rho * np.array([10.0, 2.0, 1.0, 12.0, 3.0, 8.0])
+    c = conv("AG", [rho, 1.0, 0.5, 0.25, *tens, t0, 1e3])
+    q = back("AG", c)
+    assert np.all(np.abs(q[4:10] - 0.1 * tens) <= 1e-12 * np.abs(tens))
+    assert abs(q[4] + q[7] + q[9] - 3 * rho * theta_cap) <= 1e-12 * rho
+    assert same_t(q[10], (c[10] - 0.5 * (c[4] + c[7] + c[9])) / (cl * c[0] + eps)) and same_t(q[10], t0)
+    p5 = 1e-5 * np.array([10.0, 2.0, 1.0, 12.0, 3.0, 8.0])
+    q = back("AG", conv("AG", [1e-5, 1.0, 0.5, 0.25, *p5, t0, 1e3]))
+    assert np.all(np.abs(q[4:10] - p5) <= 1e-12 * 1e-4)
+    # (d) a NaN second moment stays NaN (the cap is a test, which a NaN fails)
+    c = conv("IG", [rho, 1.0, 0.5, 0.0, 10 * rho, t0, 1e3]); c[4] = np.nan
+    assert np.isnan(back("IG", c)[4])
+    c = conv("AG", [rho, 1.0, 0.5, 0.25, *tens, t0, 1e3]); c[4] = np.nan
+    assert np.isnan(back("AG", c)[4])
+    # (e) a negative density: the floor overwrites every primitive, all finite
+    c = conv("AG", [1e-7, 1.0, 0.5, 0.25, *tens, t0, 1e3]); c[0] = -1e-10
+    q = back("AG", c)
+    assert np.all(np.isfinite(q)) and np.all(q[4:10] >= 0.0) and q[5] == 0.0 and q[0] > 0.0
