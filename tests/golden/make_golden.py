@@ -16,6 +16,10 @@ the donors of each 102 row: counts per ghost layer, then b i j k and weight per 
 density the reference's binary wrote after 5000 iterations (reference/part-field.tec), per block in
 (j, i) order.
 
+correlations.npz: the drag coefficient and the Nusselt number of every correlation the reference
+offers, from the reference's own Python restatement of them (test/verification/common.py:
+drag_coefficient, nusselt), on a grid of Reynolds, Mach, temperature-ratio and Prandtl numbers.
+
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
 import re
@@ -120,6 +124,29 @@ def chimera(ref):
     print("chimera_IG", rows.shape, don.shape, out["rho1"].shape, out["rho2"].shape)
 
 
+DRAG_LAWS = ["Newton", "Stokes", "Schlichting", "Schiller-Naumann", "Wen-Yu", "Putnam", "Clift-Gauvin",
+             "Morsi-Alexander", "Carlson-Hoglund", "Henderson", "Crowe", "Hermsen"]
+HEAT_LAWS = ["Stokes", "JAXA1", "JAXA2", "JAXA3", "JAXA4", "Ranz-Marshall", "Kavanau-Drake"]
+
+
+def correlations(ref):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("ice_verification_common", ref / "test" / "verification" / "common.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    re_ = np.concatenate([np.logspace(-2, 5, 29), [999.0, 1000.0, 1001.0, 2e5, 3e5]])
+    ma = np.array([0.05, 0.3, 0.8, 1.0, 1.2, 1.75, 2.5])
+    tr = np.array([0.5, 1.0, 2.0])
+    pr = np.array([0.7, 1.0])
+    out = {"Re": re_, "Ma": ma, "Tr": tr, "Pr": pr, "G": np.array(1.4)}
+    for law in DRAG_LAWS:
+        out["cd_" + law] = np.array([[[mod.drag_coefficient(law, R, M, 1.4, T) for T in tr] for M in ma] for R in re_])
+    for law in HEAT_LAWS:
+        out["nu_" + law] = np.array([[[mod.nusselt(law, R, P, M) for M in ma] for P in pr] for R in re_])
+    np.savez_compressed(HERE / "correlations.npz", **out)
+    print("correlations", len(DRAG_LAWS), len(HEAT_LAWS), re_.size)
+
+
 def main(ref):
     ref = Path(ref)
     for cl in ("MK", "IG", "AG"):
@@ -129,6 +156,7 @@ def main(ref):
         np.savez_compressed(HERE / f"crossing_jets_{cl}.npz", field=field, bc=bc)
         print(cl, field.shape, bc.shape)
     chimera(ref)
+    correlations(ref)
 
 
 if __name__ == "__main__":

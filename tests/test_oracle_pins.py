@@ -11,6 +11,8 @@
   (bound_empty_dt), through a whole step (compute_dt gives the starting steps the unit test sets).
 - test/unit/test_radiation.f90 R1-R3: the radiative energy of a cell's source against its closed form.
 - test/unit/test_near_empty_cap.f90: the dispersion cap of near-empty IG and AG cells in cons_2_prim.
+- test/verification/common.py: every drag and Nusselt correlation against the reference's own Python
+  restatement of them (tests/golden/correlations.npz), to 1e-13.
 """
 import math
 from pathlib import Path
@@ -310,3 +312,19 @@ def test_near_empty_cap_unit_cases(orc):
     c = conv("AG", [1e-7, 1.0, 0.5, 0.25, *tens, t0, 1e3]); c[0] = -1e-10
     q = back("AG", c)
     assert np.all(np.isfinite(q)) and np.all(q[4:10] >= 0.0) and q[5] == 0.0 and q[0] > 0.0
+
+
+def test_correlations_match_reference_restatement(orc):
+    g = np.load(GOLDEN / "correlations.npz")
+    Re, Ma, Tr, Pr, G = g["Re"], g["Ma"], g["Tr"], g["Pr"], float(g["G"])
+    for key in g.files:
+        if key.startswith("cd_"):
+            sel = abi.DRAG[key[3:]]
+            got = np.array([[[orc.drag(r, m, G, t, sel) for t in Tr] for m in Ma] for r in Re])
+        elif key.startswith("nu_"):
+            sel = abi.HEAT[key[3:]]
+            got = np.array([[[orc.heat(r, p, m, sel) for m in Ma] for p in Pr] for r in Re])
+        else:
+            continue
+        ref = g[key]
+        assert np.all(np.abs(got - ref) <= 1e-13 * np.abs(ref)), key
