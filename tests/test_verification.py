@@ -1,0 +1,94 @@
+"""The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
+B-thermal-relaxation) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
+reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
+density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
+the time integration within 0.35 of 2 (RK2) and 3 (RK3) when the CFL number halves. B: a cloud moving
+with the gas at 400 K in a 300 K gas relaxes as T_g + (T_p0 - T_g) exp(-t/tau_T), tau_T = rho_al cs
+dp^2 / (12 k), within 1e-5 of the initial gap; uniform to 1e-10 T_p0; velocity, density and number
+density unchanged."""
+import math
+
+import numpy as np
+import pytest
+
+from ice_b200 import abi, configs
+from ice_b200.solver import Solver
+
+TAU = 1000.0 * 1e-4 ** 2 / (18.0 * 1.8e-5)
+UG, TG = 10.0, 300.0
+
+
+def _gpu():
+    from ice_b200 import build
+    build.build()
+    return abi.load_gpu()
+
+
+def _relaxation_checks(lib):
+    for ratio in (0.1, 0.5, 1.0, 2.0, 3.0, 5.0):
+        n = int(math.ceil(ratio * TAU / 1e-4 - 1e-9))        # dt-max (1e-4 s) sets the step here
+        s = Solver(configs.relaxation_tube(steps=n), lib)
+        out = s.step(n)
+        assert out.status == 0 and out.dtglobal == 1e-4
+        p = s.download(0, 0)[2, 2, 2:-2]
+        exact = UG + (0.0 - UG) * math.exp(-out.time / TAU)
+        u = p[:, 1]
+        assert abs(u[0] - exact) <= 1e-5 * UG
+        assert u.max() - u.min() <= 1e-12 * UG
+        assert np.all(np.abs(p[:, 0] - 1.0) <= 1e-12)
+        assert np.all(np.abs(p[:, 5] / p[0, 5] - 1.0) <= 1e-9)
+        assert np.all(np.abs(p[:, 4] - TG) <= 1e-9 * TG)
+
+
+def _order_checks(lib):
+    for rk, expected in (("RK2", 2.0), ("RK3", 3.0)):
+        errors = []
+        for cfl in (0.8, 0.4, 0.2):
+            s = Solver(configs.relaxation_tube(nx=10, ny=2, lx=0.01, ly=1e-2, scheme=rk, cfl=cfl, vg=50.0), lib)
+            t = 0.0
+            while t < 0.02 - 1e-15:
+                t = s.step(1).time
+            u = s.download(0, 0)[2, 2, 2, 1]
+            errors.append(abs(u - (UG - UG * math.exp(-t / TAU))) / UG)
+        orders = [math.log(errors[i] / errors[i + 1]) / math.log(2.0) for i in range(2)]
+        usable = [o for o, e in zip(orders, errors[1:]) if e > 1e-12]
+        assert usable and min(usable) >= expected - 0.35, (rk, errors, orders)
+
+
+def _thermal_checks(lib):
+    tau_t = 1000.0 * 900.0 * 1e-4 ** 2 / (12.0 * 0.026)
+    for ratio in (0.1, 0.5, 1.0, 2.0, 3.0, 5.0):
+        n = int(math.ceil(ratio * tau_t / 1e-4 - 1e-9))
+        s = Solver(configs.relaxation_tube(steps=n, up0=UG, tp0=400.0), lib)
+        out = s.step(n)
+        assert out.status == 0
+        p = s.download(0, 0)[2, 2, 2:-2]
+        exact = TG + (400.0 - TG) * math.exp(-out.time / tau_t)
+        temp = p[:, 4]
+        assert abs(temp[0] - exact) <= 1e-5 * (400.0 - TG)
+        assert temp.max() - temp.min() <= 1e-10 * 400.0
+        assert np.all(np.abs(p[:, 1] - UG) <= 1e-12 * UG)
+        assert np.all(np.abs(p[:, 0] - 1.0) <= 1e-12)
+        assert np.all(np.abs(p[:, 5] / p[0, 5] - 1.0) <= 1e-9)
+
+
+def test_drag_relaxation_oracle(orc):
+    _relaxation_checks(orc)
+    _order_checks(orc)
+
+
+def test_thermal_relaxation_oracle(orc):
+    _thermal_checks(orc)
+
+
+@pytest.mark.gpu
+def test_drag_relaxation_gpu():
+    gpu = _gpu()
+    _relaxation_checks(gpu)
+    _order_checks(gpu)
+
+
+@pytest.mark.gpu
+def test_thermal_relaxation_gpu():
+    _thermal_checks(_gpu())
