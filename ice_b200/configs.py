@@ -127,10 +127,10 @@ def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
 
 
 def relaxation_tube(nx=8, ny=1, lx=1.0, ly=None, scheme="RK2", cfl=0.8, dt_max=1e-4, vg=0.0, steps=1,
-                    drag="Stokes", heat="Stokes", precision=0, up0=0.0, tp0=300.0):
+                    drag="Stokes", heat="Stokes", precision=0, up0=0.0, tp0=300.0, ug=10.0, lz=None):
     """The setting of the reference's drag-relaxation verification case (test/verification/
     A-drag-relaxation): a uniform MK cloud (1e-4 m drops of material density 1000, cp 900, volume
-    fraction 1e-3) at rest in a uniform gas stream (1.2 kg/m3, 10 m/s along x and vg along y, 300 K,
+    fraction 1e-3) at rest in a uniform gas stream (1.2 kg/m3, ug along x and vg along y, 300 K,
     R 287.05, gamma 1.4, mu 1.8e-5, k 0.026), one-way coupled with the given drag and heat laws,
     nx x ny cells of a slab lx long (ly wide: square cells by default), extrapolation on every face.
     With no gradient anywhere the particle velocity relaxes as u_g + (u_p0 - u_g) exp(-t/tau) with
@@ -138,7 +138,7 @@ def relaxation_tube(nx=8, ny=1, lx=1.0, ly=None, scheme="RK2", cfl=0.8, dt_max=1
     With up0 = 10 (no slip) and tp0 = 400 it is the thermal-relaxation case (test/verification/
     B-thermal-relaxation): T_g + (T_p0 - T_g) exp(-t/tau_T), tau_T = rho_al cs dp^2 / (12 k), Nu = 2."""
     ly = lx / nx * ny if ly is None else ly
-    dz = lx / nx
+    dz = lx / nx if lz is None else lz
     nodes = box_nodes(nx, ny, 1, size=(lx, ly, dz))
     fam = Family("MK", rho_al=1000.0, cs_al=900.0)
     num = Numerics(scheme=scheme, cfl=cfl, dt_max=dt_max, limiter="vanleer", coupled=True, drag=drag,
@@ -153,7 +153,7 @@ def relaxation_tube(nx=8, ny=1, lx=1.0, ly=None, scheme="RK2", cfl=0.8, dt_max=1
     st = empty_state((nx, ny, 1), 6)
     st[2:-2, 2:-2, 2:-2, :] = [rho_p, up0, vg, 0.0, tp0, n]
     case.state = [[st]]
-    case.gas = [_gas_layout(case, 0, 1.2, 10.0, vg, 0.0, 300.0)]
+    case.gas = [_gas_layout(case, 0, 1.2, ug, vg, 0.0, 300.0)]
     return case
 
 

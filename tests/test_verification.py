@@ -1,5 +1,5 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
-B-thermal-relaxation) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+B-thermal-relaxation, D-drag-matrix) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -73,6 +73,61 @@ def _thermal_checks(lib):
         assert np.all(np.abs(p[:, 5] / p[0, 5] - 1.0) <= 1e-9)
 
 
+DRAG_LAWS = ("Newton", "Stokes", "Schlichting", "Schiller-Naumann", "Wen-Yu", "Putnam", "Clift-Gauvin",
+             "Morsi-Alexander", "Carlson-Hoglund", "Henderson", "Crowe", "Hermsen")
+STOKES_LIMIT = ("Stokes", "Schlichting", "Schiller-Naumann", "Wen-Yu", "Putnam", "Clift-Gauvin", "Morsi-Alexander")
+COMPRESSIBLE = ("Carlson-Hoglund", "Henderson", "Crowe", "Hermsen")
+
+
+def _rk4_reference(orc, law, ug, t_end, steps=5000):
+    """du/dt = (u_g - u)/tau(u) with the solver's relaxation time 8 rho_al r_p / (3 rho_g Cd |slip| + 1e-20)
+    and Cd of the law (the oracle's correlation, itself pinned against the reference's), by classic RK4
+    with u(0) = 0 and the particles at the gas temperature."""
+    rho_g, mu, rp, rho_al = 1.2, 1.8e-5, 0.5e-4, 1000.0
+    sound = math.sqrt(1.4 * 287.05 * TG)
+    sel = abi.DRAG[law]
+
+    def rhs(u):
+        slip = ug - u
+        re = 2.0 * rho_g * rp * abs(slip) / mu
+        cd = orc.drag(re, abs(slip) / sound, 1.4, 1.0, sel)
+        return slip / (8.0 * rho_al * rp / (3.0 * rho_g * cd * abs(slip) + 1.0e-20))
+    h, u = t_end / steps, 0.0
+    for _ in range(steps):
+        k1 = rhs(u); k2 = rhs(u + 0.5 * h * k1); k3 = rhs(u + 0.5 * h * k2); k4 = rhs(u + h * k3)
+        u += h / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+    return u
+
+
+def _drag_run(lib, law, ug, t_end, **mesh):
+    s = Solver(configs.relaxation_tube(drag=law, ug=ug, vg=mesh.pop("vg", 0.0), **mesh), lib)
+    t = 0.0
+    while t < t_end - 1e-15:
+        out = s.step(1)
+        assert out.status == 0
+        t = out.time
+    p = s.download(0, 0)[2, 2:-2, 2:-2]
+    return t, p
+
+
+def _drag_matrix_checks(lib, orc):
+    # vanishing slip: the laws built as Stokes times a correction tend to the Stokes exponential
+    for law in STOKES_LIMIT:
+        t, p = _drag_run(lib, law, 1e-3, 0.03)
+        assert abs(p[0, 0, 1] - 1e-3 * (1.0 - math.exp(-t / TAU))) <= 0.01 * 1e-3, law
+    # Re = 67: every law against the integration of its own relaxation time; the temperature stays
+    for law in DRAG_LAWS:
+        t, p = _drag_run(lib, law, UG, 0.03)
+        assert abs(p[0, 0, 1] - _rk4_reference(orc, law, UG, t)) <= 1e-3 * UG, law
+        assert np.all(np.abs(p[..., 4] - TG) <= 1e-9 * TG), law
+    # above Re = 1000 (the branched laws switch formula), and transonic and supersonic slip (the
+    # compressible laws' branches), with a transverse velocity shared with the gas keeping dt short
+    for ug, laws, t_end in ((200.0, DRAG_LAWS, 4e-3), (450.0, COMPRESSIBLE, 2e-3), (900.0, COMPRESSIBLE, 2e-3)):
+        for law in laws:
+            t, p = _drag_run(lib, law, ug, t_end, vg=ug, lx=0.01, ly=2.5e-3, lz=1.25e-3, ny=2)
+            assert abs(p[0, 0, 1] - _rk4_reference(orc, law, ug, t)) <= 1e-3 * ug, (law, ug)
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -80,6 +135,10 @@ def test_drag_relaxation_oracle(orc):
 
 def test_thermal_relaxation_oracle(orc):
     _thermal_checks(orc)
+
+
+def test_drag_matrix_oracle(orc):
+    _drag_matrix_checks(orc, orc)
 
 
 @pytest.mark.gpu
@@ -92,3 +151,8 @@ def test_drag_relaxation_gpu():
 @pytest.mark.gpu
 def test_thermal_relaxation_gpu():
     _thermal_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_drag_matrix_gpu(orc):
+    _drag_matrix_checks(_gpu(), orc)
