@@ -1,5 +1,5 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
-B-thermal-relaxation, D-drag-matrix) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+B-thermal-relaxation, D-drag-matrix, E-heat-matrix) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -128,6 +128,64 @@ def _drag_matrix_checks(lib, orc):
             assert abs(p[0, 0, 1] - _rk4_reference(orc, law, ug, t)) <= 1e-3 * ug, (law, ug)
 
 
+HEAT_LAWS = ("Stokes", "JAXA1", "JAXA2", "JAXA3", "JAXA4", "Ranz-Marshall", "Kavanau-Drake")
+NU2_LIMIT = ("Stokes", "JAXA2", "JAXA3", "Ranz-Marshall")
+KG, CS, MU = 0.026, 900.0, 1.8e-5
+PR = 1.4 / 0.4 * 287.05 * MU / KG
+
+
+def _heat_rk4(orc, law, ug, t_end, tp0=400.0, steps=5000):
+    """du/dt = (u_g - u)/tau_Stokes and dT/dt = 2 Nu kg pi r_p n (T_g - T)/(rho_p cs), Nu of the law (the
+    oracle's correlation, pinned against the reference's) at the slip's Re and Ma, by classic RK4."""
+    rho_g, rp, rho_p = 1.2, 0.5e-4, 1.0
+    n = rho_p / (1000.0 * 4.0 / 3.0 * math.pi * rp ** 3)
+    sound = math.sqrt(1.4 * 287.05 * TG)
+    sel = abi.HEAT[law]
+
+    def rhs(u, T):
+        slip = ug - u
+        re = 2.0 * rho_g * rp * abs(slip) / MU
+        nu = orc.heat(re, PR, abs(slip) / sound, sel)
+        return slip / TAU, 2.0 * nu * KG * math.pi * rp * n * (TG - T) / (rho_p * CS)
+    h, u, T = t_end / steps, 0.0, tp0
+    for _ in range(steps):
+        k1 = rhs(u, T)
+        k2 = rhs(u + 0.5 * h * k1[0], T + 0.5 * h * k1[1])
+        k3 = rhs(u + 0.5 * h * k2[0], T + 0.5 * h * k2[1])
+        k4 = rhs(u + h * k3[0], T + h * k3[1])
+        u += h / 6.0 * (k1[0] + 2 * k2[0] + 2 * k3[0] + k4[0])
+        T += h / 6.0 * (k1[1] + 2 * k2[1] + 2 * k3[1] + k4[1])
+    return u, T
+
+
+def _heat_matrix_checks(lib, orc):
+    tau_t = 1000.0 * CS * 1e-4 ** 2 / (12.0 * KG)
+    # vanishing slip: the laws with Nu -> 2 follow the exact Nu = 2 relaxation
+    for law in NU2_LIMIT:
+        s = Solver(configs.relaxation_tube(heat=law, ug=1e-3, tp0=400.0, steps=300), lib)
+        out = s.step(300)
+        T = s.download(0, 0)[2, 2, 2, 4]
+        assert abs(T - (TG + 100.0 * math.exp(-out.time / tau_t))) <= 0.05 * 100.0, law
+    # Re = 67: temperature and velocity against the RK4 integration of the coupled pair
+    for law in HEAT_LAWS:
+        s = Solver(configs.relaxation_tube(heat=law, tp0=400.0, steps=300), lib)
+        out = s.step(300)
+        p = s.download(0, 0)[2, 2, 2:-2]
+        uref, tref = _heat_rk4(orc, law, UG, out.time)
+        assert abs(p[0, 4] - tref) <= 1e-3 * 100.0, law
+        assert abs(p[0, 1] - uref) <= 1e-3 * UG, law
+        assert p[:, 4].max() - p[:, 4].min() <= 1e-10 * 400.0, law
+    # constant slip (no drag): JAXA4's Nu is frozen and the cooling an exact exponential
+    sound = math.sqrt(1.4 * 287.05 * TG)
+    re = 2.0 * 1.2 * 0.5e-4 * UG / MU
+    tau_j = tau_t * 2.0 / orc.heat(re, PR, UG / sound, abi.HEAT["JAXA4"])
+    s = Solver(configs.relaxation_tube(heat="JAXA4", drag="NoDrag", tp0=400.0, steps=100), lib)
+    out = s.step(100)
+    p = s.download(0, 0)[2, 2, 2:-2]
+    assert abs(p[0, 4] - (TG + 100.0 * math.exp(-out.time / tau_j))) <= 3e-4 * 100.0
+    assert np.all(p[:, 1] == 0.0)
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -139,6 +197,10 @@ def test_thermal_relaxation_oracle(orc):
 
 def test_drag_matrix_oracle(orc):
     _drag_matrix_checks(orc, orc)
+
+
+def test_heat_matrix_oracle(orc):
+    _heat_matrix_checks(orc, orc)
 
 
 @pytest.mark.gpu
@@ -156,3 +218,8 @@ def test_thermal_relaxation_gpu():
 @pytest.mark.gpu
 def test_drag_matrix_gpu(orc):
     _drag_matrix_checks(_gpu(), orc)
+
+
+@pytest.mark.gpu
+def test_heat_matrix_gpu(orc):
+    _heat_matrix_checks(_gpu(), orc)
