@@ -127,7 +127,8 @@ def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
 
 
 def relaxation_tube(nx=8, ny=1, lx=1.0, ly=None, scheme="RK2", cfl=0.8, dt_max=1e-4, vg=0.0, steps=1,
-                    drag="Stokes", heat="Stokes", precision=0, up0=0.0, tp0=300.0, ug=10.0, lz=None):
+                    drag="Stokes", heat="Stokes", precision=0, up0=0.0, tp0=300.0, ug=10.0, lz=None,
+                    dp=1e-4, rho_al=1000.0, cs=900.0, rho_g=1.2, mu=1.8e-5, kg=0.026, tau_factor=1.0):
     """The setting of the reference's drag-relaxation verification case (test/verification/
     A-drag-relaxation): a uniform MK cloud (1e-4 m drops of material density 1000, cp 900, volume
     fraction 1e-3) at rest in a uniform gas stream (1.2 kg/m3, ug along x and vg along y, 300 K,
@@ -136,24 +137,26 @@ def relaxation_tube(nx=8, ny=1, lx=1.0, ly=None, scheme="RK2", cfl=0.8, dt_max=1
     With no gradient anywhere the particle velocity relaxes as u_g + (u_p0 - u_g) exp(-t/tau) with
     tau = rho_al dp^2 / (18 mu) under Stokes drag, and density, number density and temperature stay.
     With up0 = 10 (no slip) and tp0 = 400 it is the thermal-relaxation case (test/verification/
-    B-thermal-relaxation): T_g + (T_p0 - T_g) exp(-t/tau_T), tau_T = rho_al cs dp^2 / (12 k), Nu = 2."""
+    B-thermal-relaxation): T_g + (T_p0 - T_g) exp(-t/tau_T), tau_T = rho_al cs dp^2 / (12 k), Nu = 2.
+    dp, rho_al, cs (the drops) and rho_g, mu, kg (the gas) change the defaults above; tau_factor is the
+    step's bound by the relaxation time (the reference's tau-factor)."""
     ly = lx / nx * ny if ly is None else ly
     dz = lx / nx if lz is None else lz
     nodes = box_nodes(nx, ny, 1, size=(lx, ly, dz))
-    fam = Family("MK", rho_al=1000.0, cs_al=900.0)
+    fam = Family("MK", rho_al=rho_al, cs_al=cs)
     num = Numerics(scheme=scheme, cfl=cfl, dt_max=dt_max, limiter="vanleer", coupled=True, drag=drag,
-                   heat=heat, itermax=steps, precision=precision)
+                   heat=heat, itermax=steps, precision=precision, tau_factor=tau_factor)
     rows = box_bc(1, (nx, ny, 1), {f: 400 for f in range(1, 7)} if ny > 1 else
                   {1: 400, 2: 400, 3: 0, 4: 0, 5: 0, 6: 0})
     if ny > 1:
         rows = [(b, i, j, k, f, 0 if f >= 5 else code, pay) for (b, i, j, k, f, code, pay) in rows]
     case = Case("relaxation_tube", [nodes], [fam], num, rows)
-    rho_p = 1e-3 * 1000.0
-    n = rho_p / particle_mass(0.5e-4, 1000.0)
+    rho_p = 1e-3 * rho_al
+    n = rho_p / particle_mass(0.5 * dp, rho_al)
     st = empty_state((nx, ny, 1), 6)
     st[2:-2, 2:-2, 2:-2, :] = [rho_p, up0, vg, 0.0, tp0, n]
     case.state = [[st]]
-    case.gas = [_gas_layout(case, 0, 1.2, ug, vg, 0.0, 300.0)]
+    case.gas = [_gas_layout(case, 0, rho_g, ug, vg, 0.0, 300.0, k=kg, mu=mu)]
     return case
 
 

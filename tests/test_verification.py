@@ -1,5 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
-B-thermal-relaxation, D-drag-matrix, E-heat-matrix) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+B-thermal-relaxation, D-drag-matrix, E-heat-matrix, J-tau-limit) on the oracle and on the CUDA path
+(plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -186,6 +187,30 @@ def _heat_matrix_checks(lib, orc):
     assert np.all(p[:, 1] == 0.0)
 
 
+def _tau_limit_checks(lib):
+    """J1: drops of 2 um (tau_p = 2.2e-5 s = dt-max / 4.5) at rest in a 10 m/s stream, SSP-RK3. The first
+    step cannot know tau and takes dt-max; every later step is tau_p, so (t - dt-max)/tau_p is an
+    integer, and the cloud relaxes. J1a: tau-factor 0.2 and dt-max 5e-6 follow the exponential."""
+    kw = dict(dp=2e-6, rho_al=2000.0, cs=1000.0, rho_g=1.0, mu=2e-5, kg=0.025, scheme="RK3", cfl=0.8)
+    tau = 2000.0 * 2e-6 ** 2 / (18.0 * 2e-5)
+    for tf, dt_max, t_end, gate in ((1.0, 1e-4, 20.0 * tau, None), (0.2, 5e-6, 2.0 * tau, 5e-3)):
+        s = Solver(configs.relaxation_tube(tau_factor=tf, dt_max=dt_max, **kw), lib)
+        t = s.step(1).time
+        if tf == 1.0:       # the first step, dt-max = 4.5 tau: SSP-RK3's R(-4.5) = -8.5625, u_p = 95.625
+            assert abs(s.download(0, 0)[2, 2, 2, 1] - 95.625) <= 1e-10 * 95.625
+        while t < t_end - 1e-15:
+            out = s.step(1)
+            assert out.status == 0
+            t = out.time
+        u = s.download(0, 0)[2, 2, 2:-2, 1]
+        k = (t - dt_max) / (tf * tau)
+        assert k >= 1.0 and abs(k - round(k)) <= 1e-6, (tf, k)
+        if gate is None:
+            assert np.all(np.abs(u / UG - 1.0) < 1e-3)
+        else:
+            assert np.all(np.abs(u - UG * (1.0 - math.exp(-t / tau))) / UG < gate)
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -201,6 +226,10 @@ def test_drag_matrix_oracle(orc):
 
 def test_heat_matrix_oracle(orc):
     _heat_matrix_checks(orc, orc)
+
+
+def test_tau_limit_oracle(orc):
+    _tau_limit_checks(orc)
 
 
 @pytest.mark.gpu
@@ -223,3 +252,8 @@ def test_drag_matrix_gpu(orc):
 @pytest.mark.gpu
 def test_heat_matrix_gpu(orc):
     _heat_matrix_checks(_gpu(), orc)
+
+
+@pytest.mark.gpu
+def test_tau_limit_gpu():
+    _tau_limit_checks(_gpu())
