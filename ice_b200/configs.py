@@ -160,6 +160,39 @@ def relaxation_tube(nx=8, ny=1, lx=1.0, ly=None, scheme="RK2", cfl=0.8, dt_max=1
     return case
 
 
+def periodic_sine(nx=50, limiter="vanleer", steps=2500, scheme="RK2", precision=0):
+    """The setting of the reference's periodic sine-advection verification case (test/verification/
+    C-advection-sine): a pressureless MK cloud (1e-4 m drops of material density 1000) moving at 1 m/s
+    through nx cells of [0, 1] joined end to end (periodic connections, 201), no gas, density
+    10 + 5 sin(2 pi x) with the number density of 1e-4 m drops; CFL 0.8 under the default dt-max 1e-4 s,
+    so dt is 1e-4 on every grid. Free transport shifts the profile by the distance travelled.
+    limiter: "vanleer" (MUSCL) or "IORD" (first-order reconstruction)."""
+    dx = 1.0 / nx
+    nodes = box_nodes(nx, 1, 1, size=(1.0, dx, dx))
+    fam = Family("MK", rho_al=1000.0, cs_al=900.0)
+    num = Numerics(scheme=scheme, cfl=0.8, limiter=limiter, coupled=False, itermax=steps, precision=precision)
+    rows = []
+    for f, i0, src, fs in ((1, 1, nx, 2), (2, nx, 1, 1)):
+        rows.append((1, i0, 1, 1, f, 201, (1, src, 1, 1, fs)))
+    for f in (3, 4):
+        for i in range(1, nx + 1):
+            rows.append((1, i, 1, 1, f, 400, ()))
+    for f in (5, 6):
+        for i in range(1, nx + 1):
+            rows.append((1, i, 1, 1, f, 0, ()))
+    case = Case("periodic_sine", [nodes], [fam], num, rows)
+    x = (np.arange(nx) + 0.5) * dx
+    k = 2.0 * PI
+    # the cell averages of 10 + 5 sin(k x)
+    rho = 10.0 + 5.0 * (np.cos(k * (x - 0.5 * dx)) - np.cos(k * (x + 0.5 * dx))) / (k * dx)
+    st = empty_state((nx, 1, 1), 6)
+    I = st[2:3, 2:3, 2:-2]
+    I[0, 0, :, 0] = rho; I[0, 0, :, 1] = 1.0; I[0, 0, :, 2] = 0.0; I[0, 0, :, 3] = 0.0
+    I[0, 0, :, 4] = 300.0; I[0, 0, :, 5] = rho / particle_mass(0.5e-4, 1000.0)
+    case.state = [[st]]
+    return case
+
+
 # --------------------------------------------------- crossing jets (validation)
 def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
     """The crossing-jets validation case of the reference's suite (its Doisneau cases):

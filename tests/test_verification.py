@@ -1,6 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
-B-thermal-relaxation, D-drag-matrix, E-heat-matrix, J-tau-limit) on the oracle and on the CUDA path
-(plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, J-tau-limit) on the oracle and on
+the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -211,6 +211,36 @@ def _tau_limit_checks(lib):
             assert np.all(np.abs(u - UG * (1.0 - math.exp(-t / tau))) / UG < gate)
 
 
+def _advection_checks(lib):
+    """C: a sine density wave carried at 1 m/s around a periodic slab for 0.25 s at dt = 1e-4 on 25-200
+    cells: mass conserved to 1e-12, velocity uniform to 1e-10, the L1 error against the shifted exact
+    cell averages converging at order >= 1.5 (MUSCL, van Leer) and >= 0.85 (first order), MUSCL the more
+    accurate on every grid."""
+    k = 2.0 * math.pi
+
+    def avg(xl, xr, t):
+        return 10.0 + 5.0 * (math.cos(k * (xl - t)) - math.cos(k * (xr - t))) / (k * (xr - xl))
+    grids = (25, 50, 100, 200)
+    res = {}
+    for lim, expected in (("vanleer", 1.5), ("IORD", 0.85)):
+        errors = []
+        for nx in grids:
+            s = Solver(configs.periodic_sine(nx, lim), lib)
+            out = s.step(2500)
+            assert out.status == 0 and out.dtglobal == 1e-4
+            p = s.download(0, 0)[2, 2, 2:-2]
+            dx = 1.0 / nx
+            ref = np.array([avg(i * dx, (i + 1) * dx, out.time) for i in range(nx)])
+            errors.append(float(np.sum(np.abs(p[:, 0] - ref))) / nx / 5.0)
+            m0 = sum(avg(i * dx, (i + 1) * dx, 0.0) for i in range(nx)) * dx
+            assert abs(float(np.sum(p[:, 0])) * dx - m0) <= 1e-12 * m0
+            assert np.all(np.abs(p[:, 1] - 1.0) <= 1e-10)
+        orders = [math.log(errors[i] / errors[i + 1]) / math.log(2.0) for i in range(len(grids) - 1)]
+        assert min(orders) >= expected, (lim, errors, orders)
+        res[lim] = errors
+    assert all(a < b for a, b in zip(res["vanleer"], res["IORD"]))
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -230,6 +260,10 @@ def test_heat_matrix_oracle(orc):
 
 def test_tau_limit_oracle(orc):
     _tau_limit_checks(orc)
+
+
+def test_advection_oracle(orc):
+    _advection_checks(orc)
 
 
 @pytest.mark.gpu
@@ -257,3 +291,8 @@ def test_heat_matrix_gpu(orc):
 @pytest.mark.gpu
 def test_tau_limit_gpu():
     _tau_limit_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_advection_gpu():
+    _advection_checks(_gpu())
