@@ -20,6 +20,10 @@ correlations.npz: the drag coefficient and the Nusselt number of every correlati
 offers, from the reference's own Python restatement of them (test/verification/common.py:
 drag_coefficient, nusselt), on a grid of Reynolds, Mach, temperature-ratio and Prandtl numbers.
 
+evaporation.npz: the d-squared slopes K of the five evaporation models and the bulk density of the
+Langmuir-Knudsen case at 0.04 s, from the reference's own Python restatement of the published
+correlations (test/verification/F-evaporation/run.py: slope, coupled), at its part 1 conditions.
+
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
 import re
@@ -147,6 +151,20 @@ def correlations(ref):
     print("correlations", len(DRAG_LAWS), len(HEAT_LAWS), re_.size)
 
 
+def evaporation(ref):
+    import importlib.util
+    sys.path.insert(0, str(ref / "test" / "verification"))
+    spec = importlib.util.spec_from_file_location("ice_verification_f", ref / "test" / "verification" / "F-evaporation" / "run.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    models = list(mod.MODELS)
+    k = np.array([mod.slope(m) for m in models])
+    rho_lk, tp_lk = mod.coupled("CEM", 0.04, mod.CS_FROZEN, interface="LK")
+    np.savez_compressed(HERE / "evaporation.npz", models=np.array(models), K=k, t_lk=np.array(0.04),
+                        rho_lk=np.array(rho_lk), K_lk=np.array(mod.slope("CEM", interface="LK")))
+    print("evaporation", dict(zip(models, k)), rho_lk)
+
+
 def main(ref):
     ref = Path(ref)
     for cl in ("MK", "IG", "AG"):
@@ -157,6 +175,7 @@ def main(ref):
         print(cl, field.shape, bc.shape)
     chimera(ref)
     correlations(ref)
+    evaporation(ref)
 
 
 if __name__ == "__main__":

@@ -1,6 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
-B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, J-tau-limit) on the oracle and on
-the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, F-evaporation part 1, J-tau-limit)
+on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -241,6 +241,34 @@ def _advection_checks(lib):
     assert all(a < b for a, b in zip(res["vanleer"], res["IORD"]))
 
 
+def _evaporation_checks(lib):
+    """F, part 1: at frozen droplet temperature every evaporation model follows the d-squared law; its
+    slope K against the one the reference computes from the published correlations
+    (tests/golden/evaporation.npz) to 1e-6; the field uniform, the number density unchanged, the
+    temperature held to 1e-3 K. CEM with the Langmuir-Knudsen interface against the reference's RK4
+    integration, bulk density to 1e-8. Evaporation off: the bulk density untouched to 1e-14."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "evaporation.npz")
+    n0 = 1.0 / (4.0 / 3.0 * math.pi * 0.5e-4 ** 3 * 1000.0)
+    diameter = lambda r: 2.0 * (0.75 * r / (n0 * math.pi * 1000.0)) ** (1.0 / 3.0)
+    for model, k_ref in zip(g["models"], g["K"]):
+        s = Solver(configs.evaporating_tube(str(model)), lib)
+        out = s.step(2000)
+        assert out.status == 0
+        p = s.download(0, 0)[2, 2, 2:-2]
+        k_ice = (1e-4 ** 2 - diameter(p[0, 0]) ** 2) / out.time
+        assert abs(k_ice - k_ref) <= 1e-6 * k_ref, (model, k_ice, k_ref)
+        assert p[:, 0].max() - p[:, 0].min() <= 1e-12
+        assert np.all(np.abs(p[:, 5] - n0) <= 1e-9 * n0)
+        assert np.all(np.abs(p[:, 4] - 300.0) <= 1e-3)
+    s = Solver(configs.evaporating_tube("CEM", "LK"), lib)
+    s.step(2000)
+    assert abs(s.download(0, 0)[2, 2, 2, 0] - float(g["rho_lk"])) <= 1e-8
+    s = Solver(configs.evaporating_tube("none"), lib)
+    s.step(2000)
+    assert abs(s.download(0, 0)[2, 2, 2, 0] - 1.0) <= 1e-14
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -264,6 +292,10 @@ def test_tau_limit_oracle(orc):
 
 def test_advection_oracle(orc):
     _advection_checks(orc)
+
+
+def test_evaporation_oracle(orc):
+    _evaporation_checks(orc)
 
 
 @pytest.mark.gpu
@@ -296,3 +328,8 @@ def test_tau_limit_gpu():
 @pytest.mark.gpu
 def test_advection_gpu():
     _advection_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_evaporation_gpu():
+    _evaporation_checks(_gpu())
