@@ -193,23 +193,25 @@ def periodic_sine(nx=50, limiter="vanleer", steps=2500, scheme="RK2", precision=
     return case
 
 
-def evaporating_tube(model="CEM", interface="VLE", steps=2000, cs=1e12, dt_max=2e-5, precision=0):
+def evaporating_tube(model="CEM", interface="VLE", steps=2000, cs=1e12, dt_max=2e-5, precision=0, blowing=False,
+                     tp0=300.0):
     """The setting of the reference's droplet-evaporation verification case, part 1 (test/verification/
     F-evaporation): water droplets of 1e-4 m at volume fraction 1e-3, at rest at 300 K in air at rest at
     800 K and one atmosphere, 8 cells of a slab, the given evaporation model and interface (VLE or LK),
     drag and heat Stokes, no blowing correction, RK2, CFL 0.8, dt-max 2e-5 s. The default specific heat
-    (1e12) freezes the droplet temperature, so d^2 falls linearly in time (the d-squared law)."""
+    (1e12) freezes the droplet temperature, so d^2 falls linearly in time (the d-squared law); cs 4180
+    releases it; blowing switches the Miller-Harstad-Bellan correction on; tp0 the droplet temperature."""
     nx = 8
     nodes = box_nodes(nx, 1, 1, size=(1.0, 1.0 / nx, 1.0 / nx))
     fam = Family("MK", rho_al=1000.0, cs_al=cs, lv_al=2.26e6, emiss=0.0, evap=model, intf=interface,
                  Mv=18.015, cpv=0.0, Le=1.0, Yinf=0.0, Tboil=373.15, alphaE=1.0)
     num = Numerics(scheme="RK2", cfl=0.8, dt_max=dt_max, limiter="vanleer", coupled=True, drag="Stokes",
-                   heat="Stokes", blowing=False, itermax=steps, precision=precision)
+                   heat="Stokes", blowing=blowing, itermax=steps, precision=precision)
     rows = box_bc(1, (nx, 1, 1), {1: 400, 2: 400, 3: 0, 4: 0, 5: 0, 6: 0})
     case = Case("evaporating_tube", [nodes], [fam], num, rows)
     n = 1.0 / particle_mass(0.5e-4, 1000.0)
     st = empty_state((nx, 1, 1), 6)
-    st[2:-2, 2:-2, 2:-2, :] = [1.0, 0.0, 0.0, 0.0, 300.0, n]
+    st[2:-2, 2:-2, 2:-2, :] = [1.0, 0.0, 0.0, 0.0, tp0, n]
     case.state = [[st]]
     case.gas = [_gas_layout(case, 0, 101325.0 / (287.05 * 800.0), 0.0, 0.0, 0.0, 800.0)]
     return case

@@ -20,9 +20,11 @@ correlations.npz: the drag coefficient and the Nusselt number of every correlati
 offers, from the reference's own Python restatement of them (test/verification/common.py:
 drag_coefficient, nusselt), on a grid of Reynolds, Mach, temperature-ratio and Prandtl numbers.
 
-evaporation.npz: the d-squared slopes K of the five evaporation models and the bulk density of the
-Langmuir-Knudsen case at 0.04 s, from the reference's own Python restatement of the published
-correlations (test/verification/F-evaporation/run.py: slope, coupled), at its part 1 conditions.
+evaporation.npz: from the reference's own Python restatement of the published correlations
+(test/verification/F-evaporation/run.py: slope, coupled, surface_state), at the conditions of its parts
+1-4: the d-squared slopes K of the five evaporation models at 300 K and at the boiling clamp (380 K),
+the bulk density of the Langmuir-Knudsen case at both, and the RK4 bulk density and temperature of the
+d2-law, ASM and TC droplets with the temperature released (cp 4180) after 0.05 s.
 
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
@@ -160,9 +162,16 @@ def evaporation(ref):
     models = list(mod.MODELS)
     k = np.array([mod.slope(m) for m in models])
     rho_lk, tp_lk = mod.coupled("CEM", 0.04, mod.CS_FROZEN, interface="LK")
+    free = ["d2-law", "ASM", "TC"]
+    hot = np.array([mod.coupled(m, 0.05, mod.CS_L) for m in free])            # (rho_p, T_p) per model
+    t_boil = (1.0 - 0.9 ** (2.0 / 3.0)) * mod.D0 ** 2 / mod.slope("CEM", Tp=380.0)
+    k_boil = np.array([mod.slope(m, Tp=380.0) for m in models])
+    rho_lk_boil, _ = mod.coupled("CEM", t_boil, mod.CS_FROZEN, interface="LK", steps=4000, tp0=380.0)
     np.savez_compressed(HERE / "evaporation.npz", models=np.array(models), K=k, t_lk=np.array(0.04),
-                        rho_lk=np.array(rho_lk), K_lk=np.array(mod.slope("CEM", interface="LK")))
-    print("evaporation", dict(zip(models, k)), rho_lk)
+                        rho_lk=np.array(rho_lk), K_lk=np.array(mod.slope("CEM", interface="LK")),
+                        free=np.array(free), hot=hot, t_boil=np.array(t_boil), K_boil=k_boil,
+                        rho_lk_boil=np.array(rho_lk_boil))
+    print("evaporation", dict(zip(models, k)), rho_lk, hot, t_boil)
 
 
 def main(ref):

@@ -1,6 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
-B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, F-evaporation part 1, J-tau-limit)
-on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, F-evaporation parts 1-4,
+J-tau-limit) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -242,11 +242,12 @@ def _advection_checks(lib):
 
 
 def _evaporation_checks(lib):
-    """F, part 1: at frozen droplet temperature every evaporation model follows the d-squared law; its
+    """F, parts 1-4 (part 1: at frozen droplet temperature every evaporation model follows the d-squared law; its
     slope K against the one the reference computes from the published correlations
     (tests/golden/evaporation.npz) to 1e-6; the field uniform, the number density unchanged, the
     temperature held to 1e-3 K. CEM with the Langmuir-Knudsen interface against the reference's RK4
-    integration, bulk density to 1e-8. Evaporation off: the bulk density untouched to 1e-14."""
+    integration, bulk density to 1e-8. Evaporation off: the bulk density untouched to 1e-14. Parts 2-4
+    below.)"""
     from pathlib import Path
     g = np.load(Path(__file__).resolve().parent / "golden" / "evaporation.npz")
     n0 = 1.0 / (4.0 / 3.0 * math.pi * 0.5e-4 ** 3 * 1000.0)
@@ -267,6 +268,33 @@ def _evaporation_checks(lib):
     s = Solver(configs.evaporating_tube("none"), lib)
     s.step(2000)
     assert abs(s.download(0, 0)[2, 2, 2, 0] - 1.0) <= 1e-14
+    # part 2: the temperature released (cp 4180, 0.05 s at dt-max 5e-6) against the reference's RK4 of
+    # the coupled (rho_p, T_p) system: T_p to 1e-8 of the initial gap, rho_p to 1e-9
+    for model, (rho_ref, t_ref) in zip(g["free"], g["hot"]):
+        s = Solver(configs.evaporating_tube(str(model), cs=4180.0, dt_max=5e-6, steps=10000), lib)
+        s.step(10000)
+        p = s.download(0, 0)[2, 2, 2]
+        assert abs(p[4] - t_ref) <= 1e-8 * 500.0 and abs(p[0] - rho_ref) <= 1e-9, model
+    assert g["hot"][0][1] - 300.0 > 1.0                  # without blowing the d2-law droplet heats up
+    # part 3: d2-law with Nu = 2 and the blowing correction is exactly isothermal, on the d-squared law
+    s = Solver(configs.evaporating_tube("d2-law", cs=4180.0, dt_max=5e-6, steps=10000, blowing=True), lib)
+    out = s.step(10000)
+    p = s.download(0, 0)[2, 2, 2:-2]
+    assert np.all(np.abs(p[:, 4] - 300.0) <= 1e-8)
+    k_ice = (1e-4 ** 2 - diameter(p[0, 0]) ** 2) / out.time
+    assert abs(k_ice - g["K"][0]) <= 1e-6 * g["K"][0]
+    # part 4: above the boiling point (380 K) on the boiling clamp, each model's slope to 1e-5 and CEM
+    # with the Langmuir-Knudsen interface to 1e-8, over the time CEM takes to lose 10 % of its mass
+    t_boil = float(g["t_boil"])
+    for model, k_ref in zip(g["models"], g["K_boil"]):
+        s = Solver(configs.evaporating_tube(str(model), dt_max=t_boil / 1000.0, steps=1000, tp0=380.0), lib)
+        out = s.step(1000)
+        assert out.status == 0
+        k_ice = (1e-4 ** 2 - diameter(s.download(0, 0)[2, 2, 2, 0]) ** 2) / out.time
+        assert abs(k_ice - k_ref) <= 1e-5 * k_ref, model
+    s = Solver(configs.evaporating_tube("CEM", "LK", dt_max=t_boil / 1000.0, steps=1000, tp0=380.0), lib)
+    s.step(1000)
+    assert abs(s.download(0, 0)[2, 2, 2, 0] - float(g["rho_lk_boil"])) <= 1e-8
 
 
 def test_drag_relaxation_oracle(orc):
