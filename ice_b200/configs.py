@@ -217,6 +217,45 @@ def evaporating_tube(model="CEM", interface="VLE", steps=2000, cs=1e12, dt_max=2
     return case
 
 
+def cloud_profile(shape, x):
+    """The bulk-density profile of periodic_cloud at x in [0, 1): 10 (s(x) + 1e-6), s a Gaussian of
+    width 0.06 about 0.25 summed over its periodic images ("gauss"), or a top hat of half width 0.1
+    about 0.25 ("tophat")."""
+    x = np.asarray(x, dtype=np.float64)
+    if shape == "gauss":
+        s = sum(np.exp(-(x - 0.25 - m) ** 2 / (2.0 * 0.06 ** 2)) for m in (-1, 0, 1))
+    else:
+        d = (x - 0.25 + 0.5) % 1.0 - 0.5
+        s = np.where(np.abs(d) <= 0.1, 1.0, 0.0)
+    return 10.0 * (s + 1e-6)
+
+
+def periodic_cloud(nx=100, shape="gauss", dt_max=1e-5, steps=1, precision=0):
+    """The setting of the reference's cloud-translation verification case (test/verification/
+    G-cloud-translation): a cloud of 1e-4 m MK drops (material density 1000, cp 900) at rest, its bulk
+    density cloud_profile(shape) sampled at the cell centres of a periodic slab of nx cells (201
+    connections), number density proportional to it (one diameter everywhere), released into a frozen
+    uniform gas at 10 m/s (1.2 kg/m3, 300 K, mu 1.8e-5) with Stokes drag and heat; CFL 0.4 under dt-max.
+    The drops relax as u_p = 10 (1 - exp(-t/tau)) and the cloud translates rigidly by
+    10 t - 10 tau (1 - exp(-t/tau))."""
+    case = periodic_sine(nx, "vanleer", steps, "RK2", precision)
+    case.name = "periodic_cloud"
+    case.numerics.cfl = 0.4
+    case.numerics.dt_max = dt_max
+    case.numerics.coupled = True
+    case.numerics.drag = "Stokes"
+    case.numerics.heat = "Stokes"
+    dx = 1.0 / nx
+    rho = cloud_profile(shape, (np.arange(nx) + 0.5) * dx)
+    st = empty_state((nx, 1, 1), 6)
+    I = st[2:3, 2:3, 2:-2]
+    I[0, 0, :, 0] = rho; I[0, 0, :, 1] = 0.0; I[0, 0, :, 2] = 0.0; I[0, 0, :, 3] = 0.0
+    I[0, 0, :, 4] = 300.0; I[0, 0, :, 5] = rho / particle_mass(0.5e-4, 1000.0)
+    case.state = [[st]]
+    case.gas = [_gas_layout(case, 0, 1.2, 10.0, 0.0, 0.0, 300.0)]
+    return case
+
+
 # --------------------------------------------------- crossing jets (validation)
 def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
     """The crossing-jets validation case of the reference's suite (its Doisneau cases):

@@ -1,6 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
 B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, F-evaporation parts 1-4,
-J-tau-limit) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+G-cloud-translation, J-tau-limit) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -297,6 +297,56 @@ def _evaporation_checks(lib):
     assert abs(s.download(0, 0)[2, 2, 2, 0] - float(g["rho_lk_boil"])) <= 1e-8
 
 
+def _translation_checks(lib):
+    """G: a cloud at rest released into a uniform 10 m/s gas on a periodic slab translates rigidly while
+    its drops relax. Every run: the density-weighted particle velocity within 1e-6 of the exact
+    relaxation, mass to 1e-12, the centroid within 0.05 cells of the exact displacement. A smooth
+    (Gaussian) cloud converges in space at order >= 1.5 (50-200 cells); the spread of u_p vanishes at
+    order >= 1.8 in dt and is below 1e-6 at dt 5e-6; a top hat keeps mass and centroid."""
+    tau = TAU
+    t_end = 3.0 * tau
+
+    def avg(shape, xl, xr, shift, m=32):
+        h = (xr - xl) / m
+        return float(np.mean(configs.cloud_profile(shape, (xl + (np.arange(m) + 0.5) * h - shift) % 1.0)))
+
+    def run(nx, shape, dt):
+        n = int(math.ceil(t_end / dt - 1e-9))
+        s = Solver(configs.periodic_cloud(nx, shape, dt, n), lib)
+        out = s.step(n)
+        assert out.status == 0
+        return out.time, s.download(0, 0)[2, 2, 2:-2]
+
+    def common(t, p, shape, nx):
+        dx = 1.0 / nx
+        rho, up = p[:, 0], p[:, 1]
+        assert abs(float(np.sum(rho * up) / np.sum(rho)) - UG * (1.0 - math.exp(-t / tau))) <= 1e-6 * UG
+        m0 = sum(avg(shape, i * dx, (i + 1) * dx, 0.0) for i in range(nx)) * dx
+        assert abs(float(rho.sum()) * dx / m0 - 1.0) <= 1e-12
+        x = UG * t - UG * tau * (1.0 - math.exp(-t / tau))
+        ang = np.sum(rho * np.exp(2j * np.pi * (np.arange(nx) + 0.5) * dx))
+        drift = abs((math.atan2(ang.imag, ang.real) / (2.0 * math.pi)) % 1.0 - (0.25 + x) % 1.0)
+        assert min(drift, 1.0 - drift) <= 0.05 * dx
+        return x
+
+    errors = []
+    for nx in (50, 100, 200):
+        t, p = run(nx, "gauss", 1e-5)
+        x = common(t, p, "gauss", nx)
+        dx = 1.0 / nx
+        ref = np.array([avg("gauss", i * dx, (i + 1) * dx, x) for i in range(nx)])
+        errors.append(float(np.abs(p[:, 0] - ref).sum() / ref.sum()))
+    assert min(math.log(errors[i] / errors[i + 1]) / math.log(2.0) for i in range(2)) >= 1.5, errors
+    spreads = []
+    for dt in (2e-5, 1e-5, 5e-6):
+        _, p = run(100, "gauss", dt)
+        spreads.append(float(p[:, 1].max() - p[:, 1].min()) / UG)
+    assert min(math.log(spreads[i] / spreads[i + 1]) / math.log(2.0) for i in range(2)) >= 1.8, spreads
+    assert spreads[-1] <= 1e-6
+    t, p = run(100, "tophat", 1e-5)
+    common(t, p, "tophat", 100)
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -324,6 +374,10 @@ def test_advection_oracle(orc):
 
 def test_evaporation_oracle(orc):
     _evaporation_checks(orc)
+
+
+def test_translation_oracle(orc):
+    _translation_checks(orc)
 
 
 @pytest.mark.gpu
@@ -361,3 +415,8 @@ def test_advection_gpu():
 @pytest.mark.gpu
 def test_evaporation_gpu():
     _evaporation_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_translation_gpu():
+    _translation_checks(_gpu())
