@@ -256,6 +256,53 @@ def periodic_cloud(nx=100, shape="gauss", dt_max=1e-5, steps=1, precision=0):
     return case
 
 
+def strain_tube(nx=100, dp=1e-4, steps=1, precision=0):
+    """The setting of the reference's linear-strain verification case (test/verification/
+    H-linear-strain): a frozen gas (1.2 kg/m3, 300 K, mu 1.8e-5) in the uniform strain u_g = 2 + 6 x on
+    nx cells of [0, 1], extrapolation on every face; a Gaussian cloud 10 (exp(-(x - 0.2)^2 / (2 0.035^2))
+    + 1e-6) sampled at the cell centres, seeded at the local gas velocity, with the number density of
+    drops of diameter dp (material density 1000, cp 900); Stokes drag and heat, CFL 0.4, dt-max 2e-5.
+    With xi = x + 1/3 every drop is displaced by one factor C(t), so the solution is the affine map
+    rho_p(x, t) = rho_p0(xi / C - 1/3) / C, u_p = (C'/C) xi."""
+    case = relaxation_tube(nx=nx, cfl=0.4, dt_max=2e-5, steps=steps, precision=precision, dp=dp)
+    case.name = "strain_tube"
+    x = (np.arange(nx) + 0.5) / nx
+    rho = 10.0 * (np.exp(-(x - 0.2) ** 2 / (2.0 * 0.035 ** 2)) + 1e-6)
+    ug = 2.0 + 6.0 * x
+    st = empty_state((nx, 1, 1), 6)
+    I = st[2:3, 2:3, 2:-2]
+    I[0, 0, :, 0] = rho; I[0, 0, :, 1] = ug; I[0, 0, :, 2] = 0.0; I[0, 0, :, 3] = 0.0
+    I[0, 0, :, 4] = 300.0; I[0, 0, :, 5] = rho / particle_mass(0.5 * dp, 1000.0)
+    case.state = [[st]]
+    case.gas = [_gas_layout(case, 0, 1.2, ug, 0.0, 0.0, 300.0)]
+    return case
+
+
+def vortex_box(n=96, tau=0.1, steps=1, precision=0):
+    """The setting of the reference's vortex-cloud verification case (test/verification/I-vortex-cloud):
+    a frozen gas (1.2 kg/m3, 300 K, mu 1.8e-5) in solid-body rotation u_g = -y, v_g = x on n x n cells of
+    [-2, 2]^2 (cells 4/n thick), extrapolation on every side; a Gaussian cloud 10 (exp(-((x - 0.6)^2 +
+    y^2) / (2 0.12^2)) + 1e-8) sampled at the cell centres, seeded at the local gas velocity, with the
+    number density of drops whose Stokes time is tau (material density 1000, cp 900); Stokes drag and
+    heat, CFL 0.4, dt-max 1e-3. In z = x + i y every drop is displaced by one complex factor C(t), so
+    rho_p(z, t) = rho_p0(z / C) / |C|^2 and u_p + i v_p = (C'/C) z."""
+    dp = math.sqrt(18.0 * 1.8e-5 * tau / 1000.0)
+    case = relaxation_tube(nx=n, ny=n, lx=4.0, ly=4.0, lz=4.0 / n, cfl=0.4, dt_max=1e-3, steps=steps,
+                           precision=precision, dp=dp)
+    case.name = "vortex_box"
+    case.nodes = [box_nodes(n, n, 1, lo=(-2.0, -2.0, 0.0), size=(4.0, 4.0, 4.0 / n))]
+    c = -2.0 + (np.arange(n) + 0.5) * (4.0 / n)
+    Y, X = np.meshgrid(c, c, indexing="ij")
+    rho = 10.0 * (np.exp(-((X - 0.6) ** 2 + Y ** 2) / (2.0 * 0.12 ** 2)) + 1e-8)
+    st = empty_state((n, n, 1), 6)
+    I = st[2, 2:-2, 2:-2]
+    I[:, :, 0] = rho; I[:, :, 1] = -Y; I[:, :, 2] = X; I[:, :, 3] = 0.0
+    I[:, :, 4] = 300.0; I[:, :, 5] = rho / particle_mass(0.5 * dp, 1000.0)
+    case.state = [[st]]
+    case.gas = [_gas_layout(case, 0, 1.2, -Y, X, 0.0, 300.0)]
+    return case
+
+
 # --------------------------------------------------- crossing jets (validation)
 def crossing_jets(closure="IG", n=100, steps=5000, upper=None):
     """The crossing-jets validation case of the reference's suite (its Doisneau cases):

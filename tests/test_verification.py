@@ -1,6 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
 B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, F-evaporation parts 1-4,
-G-cloud-translation, J-tau-limit) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+G-cloud-translation, H-linear-strain, I-vortex-cloud, J-tau-limit) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -8,6 +8,7 @@ the time integration within 0.35 of 2 (RK2) and 3 (RK3) when the CFL number halv
 with the gas at 400 K in a 300 K gas relaxes as T_g + (T_p0 - T_g) exp(-t/tau_T), tau_T = rho_al cs
 dp^2 / (12 k), within 1e-5 of the initial gap; uniform to 1e-10 T_p0; velocity, density and number
 density unchanged."""
+import cmath
 import math
 
 import numpy as np
@@ -347,6 +348,119 @@ def _translation_checks(lib):
     common(t, p, "tophat", 100)
 
 
+def _strain_checks(lib):
+    """H: a Gaussian cloud seeded at the local velocity of a frozen gas in the uniform strain
+    u_g = 2 + 6 x. With xi = x + 1/3 every drop is displaced by one factor C(t) (C'' tau + C' = 6 C,
+    C(0) = 1, C'(0) = 6), so rho_p = rho_p0(xi / C - 1/3) / C and u_p = (C'/C) xi exactly. At St = 0.185,
+    on 100-400 cells: centroid within 0.05 cells, the density-weighted slope of u_p against xi within
+    2e-4 of C'/C, mass within 2e-3 of the exact stretch, L1 order >= 1.5. Over St = 0.2 to 0.025 on 200
+    cells the slip coefficient 6 - slope tends to the asymptote 36 tau monotonically, departs from it by
+    1.3-2.2 St, and is within 5 % of it at St = 0.025."""
+    def stretch(tau, t, a=6.0):
+        root = math.sqrt(1.0 + 4.0 * a * tau)
+        lp, lm = (-1.0 + root) / (2.0 * tau), (-1.0 - root) / (2.0 * tau)
+        ca, cb = (a - lm) / (lp - lm), (lp - a) / (lp - lm)
+        return (ca * math.exp(lp * t) + cb * math.exp(lm * t),
+                ca * lp * math.exp(lp * t) + cb * lm * math.exp(lm * t))
+
+    def profile(x):
+        return 10.0 * (np.exp(-(x - 0.2) ** 2 / (2.0 * 0.035 ** 2)) + 1e-6)
+
+    def run(nx, tau):
+        n = int(math.ceil(0.1 / 2e-5 - 1e-9))
+        s = Solver(configs.strain_tube(nx, math.sqrt(18.0 * 1.8e-5 * tau / 1000.0), n), lib)
+        out = s.step(n)
+        assert out.status == 0
+        p = s.download(0, 0)[2, 2, 2:-2]
+        xi = (np.arange(nx) + 0.5) / nx + 1.0 / 3.0
+        slope = float(np.sum(p[:, 0] * p[:, 1] * xi) / np.sum(p[:, 0] * xi ** 2))
+        return out.time, p, xi, slope
+
+    errors = []
+    for nx in (100, 200, 400):
+        t, p, xi, slope = run(nx, TAU)
+        c, cdot = stretch(TAU, t)
+        dx = 1.0 / nx
+        sub = np.arange(nx)[:, None] * dx + (np.arange(32)[None, :] + 0.5) * (dx / 32) + 1.0 / 3.0
+        ref = (profile(sub / c - 1.0 / 3.0) / c).mean(axis=1)
+        rho = p[:, 0]
+        errors.append(float(np.abs(rho - ref).sum() / ref.sum()))
+        xbar = float(np.sum(rho * xi) / rho.sum())
+        assert abs(xbar - c * (0.2 + 1.0 / 3.0)) <= 0.05 * dx
+        assert abs(slope / (cdot / c) - 1.0) <= 2e-4
+        assert abs(float(rho.sum() / ref.sum()) - 1.0) <= 2e-3
+    assert min(math.log(errors[i] / errors[i + 1]) / math.log(2.0) for i in range(2)) >= 1.5, errors
+    stokes, ratios = (0.2, 0.1, 0.05, 0.025), []
+    for st in stokes:
+        tau = st / 6.0
+        t, p, xi, slope = run(200, tau)
+        c, cdot = stretch(tau, t)
+        assert abs(slope / (cdot / c) - 1.0) <= 5e-4
+        ratios.append((6.0 - slope) / (36.0 * tau))
+    assert all(a < b for a, b in zip(ratios[:-1], ratios[1:])), ratios
+    assert all(1.3 * st <= 1.0 - r <= 2.2 * st for r, st in zip(ratios, stokes)), ratios
+    assert abs(ratios[-1] - 1.0) <= 0.05
+
+
+def _vortex_checks(lib):
+    """I: a Gaussian cloud seeded at the local velocity of a frozen gas in solid-body rotation
+    (Omega = 1) on [-2, 2]^2, a quarter turn. In z = x + i y every drop is displaced by one complex
+    factor C(t), so rho_p = rho_p0(z / C) / |C|^2 and u_p + i v_p = (C'/C) z. At St = 0.1 on 48-192
+    cells a side: centroid within 0.1 cells of C z_0, L1 and centroid orders >= 1.5. Over St = 0.01 to 10
+    on 96 cells: radius within 5e-3 and phase lag within 5e-3 rad of C, the velocity slope within 1e-2
+    of C'/C, L1 <= 0.15, mass within 1e-3; lag and radius grow with St, St = 0.01 is a tracer (lag
+    <= 5e-3, radius within 0.02) and St = 10 lags at least 0.4 rad."""
+    quarter = 0.5 * math.pi
+
+    def stretch(tau, t):
+        root = cmath.sqrt(1.0 + 4.0j * tau)
+        lp, lm = (-1.0 + root) / (2.0 * tau), (-1.0 - root) / (2.0 * tau)
+        ca, cb = (1.0j - lm) / (lp - lm), (lp - 1.0j) / (lp - lm)
+        return (ca * cmath.exp(lp * t) + cb * cmath.exp(lm * t),
+                ca * lp * cmath.exp(lp * t) + cb * lm * cmath.exp(lm * t))
+
+    def run(n, tau):
+        steps = int(math.ceil(quarter / 1e-3 - 1e-9))
+        s = Solver(configs.vortex_box(n, tau, steps), lib)
+        out = s.step(steps)
+        assert out.status == 0
+        p = s.download(0, 0)[2, 2:-2, 2:-2]
+        c = -2.0 + (np.arange(n) + 0.5) * (4.0 / n)
+        y, x = np.meshgrid(c, c, indexing="ij")
+        z = x + 1j * y
+        rho, w = p[..., 0], p[..., 1] + 1j * p[..., 2]
+        c_t, cdot = stretch(tau, out.time)
+        z0 = z / c_t
+        ref = 10.0 * (np.exp(-((z0.real - 0.6) ** 2 + z0.imag ** 2) / (2.0 * 0.12 ** 2)) + 1e-8) / abs(c_t) ** 2
+        centre = complex(np.sum(rho * z) / rho.sum())
+        slope = complex(np.sum(rho * w * z.conj()) / np.sum(rho * abs(z) ** 2))
+        err = float(np.abs(rho - ref).sum() / ref.sum())
+        return out.time, c_t, cdot, centre, slope, err, float(rho.sum() / ref.sum())
+
+    errors, drifts = [], []
+    for n in (48, 96, 192):
+        _, c_t, _, centre, _, err, _ = run(n, 0.1)
+        errors.append(err)
+        drifts.append(abs(centre - 0.6 * c_t))
+        assert drifts[-1] <= 0.1 * 4.0 / n
+    for e in (errors, drifts):
+        assert min(math.log(e[i] / e[i + 1]) / math.log(2.0) for i in range(2)) >= 1.5, e
+    lags, radii = [], []
+    for st in (0.01, 0.1, 1.0, 10.0):
+        t, c_t, cdot, centre, slope, err, mass = run(96, st)
+        lags.append(t - cmath.phase(centre))
+        radii.append(abs(centre) / 0.6)
+        assert abs(radii[-1] / abs(c_t) - 1.0) <= 5e-3
+        assert abs(lags[-1] - (t - cmath.phase(c_t))) <= 5e-3
+        assert abs(slope / (cdot / c_t) - 1.0) <= 1e-2
+        assert err <= 0.15
+        assert abs(mass - 1.0) <= 1e-3
+    assert all(a < b for a, b in zip(lags[:-1], lags[1:])), lags
+    assert all(a < b for a, b in zip(radii[:-1], radii[1:])), radii
+    assert lags[0] <= 5e-3 and abs(radii[0] - 1.0) <= 0.02
+    assert lags[-1] >= 0.4
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -378,6 +492,14 @@ def test_evaporation_oracle(orc):
 
 def test_translation_oracle(orc):
     _translation_checks(orc)
+
+
+def test_strain_oracle(orc):
+    _strain_checks(orc)
+
+
+def test_vortex_oracle(orc):
+    _vortex_checks(orc)
 
 
 @pytest.mark.gpu
@@ -420,3 +542,13 @@ def test_evaporation_gpu():
 @pytest.mark.gpu
 def test_translation_gpu():
     _translation_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_strain_gpu():
+    _strain_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_vortex_gpu():
+    _vortex_checks(_gpu())
