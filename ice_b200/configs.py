@@ -103,6 +103,27 @@ def riemann_1d(n=2000, steps=1000):
     return case
 
 
+def ag_tube(ic, x0=-0.5, lx=1.0, ny=1, ly=1e-3, h=1e-3, side_code=0, scheme="RK2", limiter="mc", cfl=0.5,
+            dt_max=1e-4, t_end=0.125, riemann="Rusanov", rho_al=2700.0, cs=1598.0):
+    """A 1-D Riemann problem of the anisotropic Gaussian closure, the setting of the reference's Berthon
+    cases (test/Berthon/*: 500 cells of [-0.5, 0.5], 1e-3 wide and thick, extrapolation at the ends,
+    MUSCL with the MC limiter, RK2, CFL 0.5, material 2700 kg/m3, cp 1598) and of its anisotropic Sod
+    tube (test/Riemann/AG). ic: the 12 AG primitives (rho, u, v, w, P11, P12, P13, P22, P23, P33, T, n)
+    per cell along x, shape (12, nx), repeated over the ny rows; side_code: the boundary code of the
+    j faces (0 none, 300 wall); the k faces are 0. No gas; the run ends at time >= t_end."""
+    ic = np.asarray(ic, dtype=np.float64)
+    nx = ic.shape[1]
+    nodes = box_nodes(nx, ny, 1, lo=(x0, 0.0, -0.5 * h), size=(lx, ly, h))
+    fam = Family("AG", riemann=riemann, rho_al=rho_al, cs_al=cs)
+    num = Numerics(scheme=scheme, cfl=cfl, dt_max=dt_max, limiter=limiter, time_threshold=t_end)
+    rows = box_bc(1, (nx, ny, 1), {1: 400, 2: 400, 3: side_code, 4: side_code, 5: 0, 6: 0})
+    case = Case("ag_tube", [nodes], [fam], num, rows)
+    st = empty_state((nx, ny, 1), 12)
+    st[2, 2:-2, 2:-2, :] = ic.T[None, :, :]
+    case.state = [[st]]
+    return case
+
+
 def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
     """The setting of the reference's unit test of the steps of empty cells a source fills
     (test/unit/test_empty_dt.f90): one block of 4 x 1 x 1 cells of 1 mm (the last 0.1 mm wide when

@@ -26,6 +26,14 @@ evaporation.npz: from the reference's own Python restatement of the published co
 the bulk density of the Langmuir-Knudsen case at both, and the RK4 bulk density and temperature of the
 d2-law, ASM and TC droplets with the temperature released (cp 4180) after 0.05 s.
 
+ag_riemann.npz: the reference's Riemann problems of the anisotropic Gaussian closure. For each Berthon case
+(test/Berthon/{SCS,RCS,RCR,SCS-hlle}): the initial cell states (INPUT/part-ic.tec, the 12 primitives
+along x), the time threshold (input.ini), the L1 tolerance its verify.py passes and the tabulated exact
+wave pattern (Results/<case>/<case>_exact.tec: abscissae and values of the six piecewise-linear profiles,
+density, u, v, P11, P22 and det P, in that order). For the anisotropic Sod tube (test/Riemann/AG): the
+constants of make_case.py (grid, states, drop radius and density), the time threshold and the gates of
+its verify.py.
+
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
 import re
@@ -174,6 +182,59 @@ def evaporation(ref):
     print("evaporation", dict(zip(models, k)), rho_lk, hot, t_boil)
 
 
+BERTHON_ZONES = ("Density", "X Velocity", "Y Velocity", "XX Pressure", "YY Pressure", "Det Pressure")
+
+
+def ag_riemann(ref):
+    out = {}
+    for case in ("SCS", "RCS", "RCR", "SCS-hlle"):
+        d = ref / "test" / "Berthon" / case
+        key = case.replace("-", "_")
+        text = (d / "INPUT" / "part-ic.tec").read_text().split("\n")
+        zi = next(i for i, l in enumerate(text) if "ZONE" in l)
+        g = lambda k: int(re.search(r"\b%s\s*=\s*(\d+)" % k, text[zi]).group(1))
+        I, J, K = g("I"), g("J"), g("K")
+        vals = np.array([float(t) for l in text[zi + 1:] for t in l.split()])
+        nn, nc = I * J * K, (I - 1) * (J - 1) * (K - 1)
+        out[key + "_x"] = vals[:I]
+        out[key + "_ic"] = vals[3 * nn:3 * nn + 12 * nc].reshape(12, K - 1, J - 1, I - 1)[:, 0, 0, :]
+        ini = (d / "input.ini").read_text()
+        out[key + "_t"] = np.array(float(re.search(r"time-threshold\s*=\s*([-+.\deE]+)", ini).group(1)))
+        out[key + "_hlle"] = np.array("HLLE" in ini)
+        out[key + "_tol"] = np.array(float(re.search(r"tol\s*=\s*([-+.\deE]+)", (d / "verify.py").read_text()).group(1)))
+        src = case.split("-")[0]
+        lines = (ref / "test" / "Berthon" / "Results" / src / f"{src}_exact.tec").read_text().split("\n")
+        zones = {}
+        q = 0
+        while q < len(lines):
+            m = re.search(r'ZONE\s+T\s*=\s*"([^"]+)"', lines[q])
+            if not m:
+                q += 1
+                continue
+            n = int(re.search(r"\bI\s*=\s*(\d+)", lines[q + 1]).group(1))
+            q += 3
+            v = []
+            while len(v) < 2 * n:
+                v += [float(t) for t in lines[q].split()]
+                q += 1
+            zones[m.group(1)] = np.array(v[:2 * n])
+        for z, name in enumerate(BERTHON_ZONES):
+            out[f"{key}_exact{z}"] = zones[name].reshape(2, -1)
+    d = ref / "test" / "Riemann" / "AG"
+    mc = (d / "make_case.py").read_text()
+    for lhs, rhs in re.findall(r"^((?:NX|X0),[^=]*)=\s*(.*)$", mc, re.M):
+        for name, v in zip(lhs.split(","), rhs.split(",")):
+            out["sod_" + name.strip()] = np.array(float(v))
+    ini = (d / "input.ini").read_text()
+    out["sod_t"] = np.array(float(re.search(r"time-threshold\s*=\s*([-+.\deE]+)", ini).group(1)))
+    gates = re.search(r"^NAME, GAMMA, T_END, L1_TOL, P11_MIN, PT_TOL, TV_TOL\s*=\s*(.*)$",
+                      (d / "verify.py").read_text(), re.M).group(1).split(",")[1:]
+    for name, v in zip(("GAMMA", "T_END", "L1_TOL", "P11_MIN", "PT_TOL", "TV_TOL"), gates):
+        out["sod_" + name] = np.array(float(v))
+    np.savez_compressed(HERE / "ag_riemann.npz", **out)
+    print("ag_riemann", {k: v for k, v in out.items() if v.ndim == 0})
+
+
 def main(ref):
     ref = Path(ref)
     for cl in ("MK", "IG", "AG"):
@@ -185,6 +246,7 @@ def main(ref):
     chimera(ref)
     correlations(ref)
     evaporation(ref)
+    ag_riemann(ref)
 
 
 if __name__ == "__main__":
