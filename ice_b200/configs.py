@@ -124,6 +124,113 @@ def ag_tube(ic, x0=-0.5, lx=1.0, ny=1, ly=1e-3, h=1e-3, side_code=0, scheme="RK2
     return case
 
 
+def _cell_centres(nodes):
+    """Cell centres as the mean of the 8 corner nodes, arrays (ni, nj, nk) per coordinate."""
+    c = sum(nodes[a:a + nodes.shape[0] - 1, b:b + nodes.shape[1] - 1, d:d + nodes.shape[2] - 1]
+            for a in (0, 1) for b in (0, 1) for d in (0, 1)) / 8.0
+    return c[..., 0], c[..., 1], c[..., 2]
+
+
+def _single_block(name, nodes, fam, num, codes, prims, payload=None):
+    """One block with the given boundary codes per face and the interior primitives prims (a list of
+    nc arrays or scalars over the (ni, nj, nk) cells)."""
+    dims = tuple(s - 1 for s in nodes.shape[:3])
+    case = Case(name, [nodes], [fam], num, box_bc(1, dims, codes, payload))
+    st = empty_state(dims, fam.nc)
+    for q, a in enumerate(prims):
+        st[2:-2, 2:-2, 2:-2, q] = np.broadcast_to(a, dims).transpose(2, 1, 0)
+    case.state = [[st]]
+    return case
+
+
+def noexchange_slab(precision=0):
+    """The reference's no-exchange invariant case (test/NoExchange/MK): 10 x 4 cells of a 0.1 x 0.04 m
+    slab 1 mm thick, an MK cloud at rest at 300 K (1e-3 kg/m3 of 1 um drops of material density 2000,
+    cp 1000) in a gas at 10 m/s and 400 K (1.0 kg/m3, R 287, gamma 1.4, k 0.025, mu 2e-5), coupled with
+    NoDrag, NoHeat and no emissivity; extrapolation on the i and j faces, RK3, CFL 0.8, MUSCL van Leer,
+    20 steps. Nothing couples the phases, so the state stays at its initial value exactly."""
+    nodes = box_nodes(10, 4, 1, lo=(0.0, 0.0, -0.5e-3), size=(0.1, 0.04, 1e-3))
+    fam = Family("MK", rho_al=2000.0, cs_al=1000.0)
+    num = Numerics(scheme="RK3", cfl=0.8, limiter="vanleer", coupled=True, drag="NoDrag", heat="NoHeat",
+                   itermax=20, precision=precision)
+    n = 1e-3 / particle_mass(1e-6, 2000.0)
+    case = _single_block("noexchange_slab", nodes, fam, num, {1: 400, 2: 400, 3: 400, 4: 400, 5: 0, 6: 0},
+                         [1e-3, 0.0, 0.0, 0.0, 300.0, n])
+    case.gas = [_gas_layout(case, 0, 1.0, 10.0, 0.0, 0.0, 400.0, R=287.0, gam=1.4, k=0.025, mu=2e-5)]
+    return case
+
+
+def reflect_blob(precision=0):
+    """The reference's symmetry-plane case of the AG closure (test/Reflect/AG): 200 x 100 cells of
+    [0, 2] x [0, 1], 0.01 thick; the upper half of a sheared AG blob, rho = 0.01 + g with
+    g = exp(-((x - 1)^2 + y^2) / (2 0.1^2)), moving at u = 1 along the code-200 plane y = 0 (face 3);
+    P11 = P22 = P33 = rho, P12 = 0.3 g y / 0.1, T = 1, 1 um drops of material density 2000, cp 1; faces 1,
+    2 and 4 extrapolation. RK3, CFL 0.8, MUSCL van Leer, dt-max 1e-2, to t = 0.1. The mirrored tensor
+    exerts no shear on the plane, so the x-momentum is conserved."""
+    nodes = box_nodes(200, 100, 1, lo=(0.0, 0.0, -0.005), size=(2.0, 1.0, 0.01))
+    x, y, _ = _cell_centres(nodes)
+    blob = np.exp(-((x - 1.0) ** 2 + y ** 2) / (2.0 * 0.1 ** 2))
+    rho = 0.01 + blob
+    fam = Family("AG", riemann="Rusanov", rho_al=2000.0, cs_al=1.0)
+    num = Numerics(scheme="RK3", cfl=0.8, dt_max=1e-2, limiter="vanleer", time_threshold=0.1,
+                   precision=precision)
+    return _single_block("reflect_blob", nodes, fam, num, {1: 400, 2: 400, 3: 200, 4: 400, 5: 0, 6: 0},
+                         [rho, 1.0, 0.0, 0.0, rho, 0.3 * blob * y / 0.1, 0.0, rho, 0.0, rho, 1.0,
+                          rho / particle_mass(1e-6, 2000.0)])
+
+
+def thermal_blob(closure="IG", precision=0):
+    """The reference's thermal-energy invariant cases (test/Thermal/{IG,AG}): a pressurised blob
+    rho = 0.01 + exp(-((x - 0.5)^2 + (y - 0.5)^2) / (2 0.05^2)) at rest, P = rho (isotropic for AG), T = 1,
+    1 um drops of material density 2000 and cp 1, in a closed box of 100 x 100 cells of [0, 1]^2, 0.01
+    thick (walls, code 300, on the four sides). RK3, CFL 0.5 (IG) or 0.8 (AG), MUSCL van Leer, dt-max
+    1e-2, to t = 0.1. With the pressure work in the energy flux the temperature stays uniform."""
+    nodes = box_nodes(100, 100, 1, lo=(0.0, 0.0, -0.005), size=(1.0, 1.0, 0.01))
+    x, y, _ = _cell_centres(nodes)
+    rho = 0.01 + np.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / (2.0 * 0.05 ** 2))
+    n = rho / particle_mass(1e-6, 2000.0)
+    fam = Family(closure, riemann="Rusanov", rho_al=2000.0, cs_al=1.0)
+    num = Numerics(scheme="RK3", cfl=0.5 if closure == "IG" else 0.8, dt_max=1e-2, limiter="vanleer",
+                   time_threshold=0.1, precision=precision)
+    prims = ([rho, 0.0, 0.0, 0.0, rho, 1.0, n] if closure == "IG" else
+             [rho, 0.0, 0.0, 0.0, rho, 0.0, 0.0, rho, 0.0, rho, 1.0, n])
+    return _single_block("thermal_blob", nodes, fam, num, {1: 300, 2: 300, 3: 300, 4: 300, 5: 0, 6: 0}, prims)
+
+
+def axis_wedge(closure="MK", precision=0):
+    """The reference's axisymmetric-wedge cases (test/Axis/{MK,IG,AG}): a one-degree wedge about x,
+    40 x 20 cells of x in [0, 0.1], r in [1e-8, 0.05] (the axis row at r = 1e-8, face 3, code 300), the
+    wedge sides (faces 5, 6) code 200; drops of 10 um, material density 2000, cp 1000, T 300.
+    MK: a cloud moving along x at 20 m/s with rho = 1 + 4 (r / 0.05)^2, fed through face 1 by a 402 inlet
+    of the same profile along the face normal; face 2 extrapolation, face 4 a wall; RK3, MUSCL van Leer
+    with the Jameson sensor, CFL 0.8, local steps, 200 iterations: the field is stationary.
+    IG, AG: a uniform cloud at rest (rho 1, P = 1, isotropic for AG) closed by walls on faces 1-4; RK2,
+    MUSCL van Leer, CFL 0.8, local steps, 500 iterations: the side faces carry the hoop pressure and
+    the cloud stays at rest."""
+    x = np.linspace(0.0, 0.1, 41)
+    r = np.linspace(1e-8, 0.05, 21)
+    th = np.radians([-0.5, 0.5])
+    X, R, T = np.meshgrid(x, r, th, indexing="ij")
+    nodes = np.stack([X, R * np.cos(T), R * np.sin(T)], axis=-1)
+    _, yc, zc = _cell_centres(nodes)
+    mk = closure == "MK"
+    fam = Family(closure, rho_al=2000.0, cs_al=1000.0)
+    num = Numerics(scheme="RK3" if mk else "RK2", cfl=0.8, limiter="vanleer", shock_detector=mk,
+                   time_accurate=False, itermax=200 if mk else 500, precision=precision)
+    mp = particle_mass(1e-5, 2000.0)
+    if mk:
+        rho = 1.0 + 4.0 * (np.sqrt(yc ** 2 + zc ** 2) / 0.05) ** 2
+        prims = [rho, 20.0, 0.0, 0.0, 300.0, rho / mp]
+        codes = {1: 402, 2: 400, 3: 300, 4: 300, 5: 200, 6: 200}
+        payload = lambda f, i, j, k: (rho[0, j - 1, k - 1] * 20.0, 20.0, 0.0, 0.0, 300.0, 1e-5, 0.0, 1.0)
+    else:
+        prims = ([1.0, 0.0, 0.0, 0.0, 1.0, 300.0, 1.0 / mp] if closure == "IG" else
+                 [1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 1.0, 0.0, 1.0, 300.0, 1.0 / mp])
+        codes = {1: 300, 2: 300, 3: 300, 4: 300, 5: 200, 6: 200}
+        payload = None
+    return _single_block("axis_wedge", nodes, fam, num, codes, prims, payload)
+
+
 def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
     """The setting of the reference's unit test of the steps of empty cells a source fills
     (test/unit/test_empty_dt.f90): one block of 4 x 1 x 1 cells of 1 mm (the last 0.1 mm wide when
