@@ -46,7 +46,12 @@ void launch_family_t(const LaunchArgs& a) {
     tick(KC_SOURCE);
   }
   if (a.nrec > 0) {
-    k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.grecs, a.nrec);
+    if (a.ghost_split) {
+      k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.grecs, a.nrec, 1);
+      k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.grecs, a.nrec, 2);
+    } else {
+      k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.grecs, a.nrec, 3);
+    }
     tick(KC_GHOST);
   }
   // the Jameson sensor: the staged stage kernel and the boundary kernels evaluate it from the

@@ -11,7 +11,8 @@
 //   per family, per RK stage:
 //     k_source     the source of an evaporating family (or a 1-D run), or the surrogate's
 //                  k_source_mlp                                        (Mod_Sources.f90:465-622)
-//     k_ghost      both ghost layers from the record list, block
+//     k_ghost      both ghost layers from the record list (two launches, layer 1 then
+//                  layer 2, where a block is one cell deep along a record's face), block
 //                  connections as on-device copies in one HBM pool    (Lib_Ghost.f90:29-387)
 //     k_beta       Jameson sensor (when on; 1-D runs only)            (Mod_Fluxes.f90:366-389)
 //     k_conn       connection-face fluxes by their owner records      (Mod_BC_Fluxes.f90:151-170)
@@ -78,6 +79,7 @@ struct FamHost {
   DevBuf<double> Rb, connF, resid, resid2, resid3, src;
   DevBuf<DRec> recs;
   DevBuf<DRec> grecs;                        // the same records ordered for the ghost kernel (upload_recs)
+  bool ghost_split = false;                  // the ghost layers in two launches (upload_recs)
   DevBuf<int> bfirst, blist, own;
   DevBuf<CUtensorMap> maps[3];               // per state buffer, per block: the staged kernel's TMA maps
   DevBuf<Tile> tiles3;                       // the staged kernel's tiles (the tile shape is the closure's)
@@ -302,7 +304,7 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   LaunchArgs a;
   a.G = make_geo(c);
   a.F = make_famdev(c, p, srk, phase);
-  a.recs = H.recs.p; a.nrec = H.nrec; a.grecs = H.grecs.p;
+  a.recs = H.recs.p; a.nrec = H.nrec; a.grecs = H.grecs.p; a.ghost_split = H.ghost_split;
   a.own = H.own.p; a.nown = H.nown;
   a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc;
   a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.KZ = c->KZ;
@@ -397,7 +399,7 @@ static long long launches_per_step(const ice_gpu_ctx* c) {
   for (int p = 0; p < c->P.nfam; ++p) n += c->fam[p].have_imp ? 3 : 0;
   for (int p = 0; p < c->P.nfam; ++p) {
     const FamHost& H = c->fam[p];
-    long long per = (H.nrec > 0 ? 1 : 0) + (c->P.shock_detector && !c->staged ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
+    long long per = (H.nrec > 0 ? (H.ghost_split ? 2 : 1) : 0) + (c->P.shock_detector && !c->staged ? 1 : 0) + (H.nown > 0) + (H.nbc > 0) +
                     (c->P.coupled && (!c->staged || sur_active(c, p) || c->P.fam[p].evap != 0) ? 1 : 0);
     per += c->P.irs ? (2 + 2 * c->P.ndir) : 1;
     n += per * c->P.nrk;
@@ -798,12 +800,20 @@ int ice_gpu_update_params(ice_gpu_ctx* c, const ice_gpu_params* P) {
 
 // The family's device records (table order, which the boundary and connection kernels index), and a
 // copy for the ghost kernel ordered by block, face and cell with the first index fastest, so that the
-// threads of a warp fill neighbouring ghost cells of one face (a record's ghosts are its own, and what
-// it reads no other record writes: the order of the fills does not change a value).
+// threads of a warp fill neighbouring ghost cells of one face (a record's ghosts are its own, so the
+// order of the fills does not change a value). ghost_split: some record's block (or, for a connection,
+// its source block) is one cell deep along the record's face direction, so that record's second ghost
+// layer reads the first layer of the opposite face's record; the ghost kernel then runs as two launches.
 static int upload_recs(ice_gpu_ctx* c, FamHost& H) {
   const std::vector<DRec>& dr = H.h_recs;
   CK(H.recs.alloc(dr.size()));
   CK(H.grecs.alloc(dr.size()));
+  H.ghost_split = false;
+  for (const DRec& r : dr) {
+    if (r.type == 0 || r.type == 102) continue;
+    if (c->dims[3 * r.b + (r.f - 1) / 2] == 1) H.ghost_split = true;
+    if ((r.type == 101 || r.type == 201) && c->dims[3 * r.bs + (r.fs - 1) / 2] == 1) H.ghost_split = true;
+  }
   if (dr.empty()) return 0;
   CK(cudaMemcpy(H.recs.p, dr.data(), dr.size() * sizeof(DRec), cudaMemcpyHostToDevice));
   std::vector<int> ord(dr.size());

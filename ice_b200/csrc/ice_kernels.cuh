@@ -564,17 +564,20 @@ __device__ __forceinline__ void ghost2_rec(const Geo& G, const FamDev& F, const 
   }
 }
 
-// Both ghost layers of every record, one thread per record. compute_ghost fills layer 1 of every
-// record and then fill_second_ghost layer 2 (Lib_Ghost.f90:29-387); a record's layer 2 reads only its
-// own layer-1 cell and interior cells (of its block, or of the source block of a connection), never a
-// cell another record writes, so one thread can do both in turn with the same result.
+// The ghost layers of every record, one thread per record; layers: 1 the first, 2 the second, 3 both.
+// compute_ghost fills layer 1 of every record and then fill_second_ghost layer 2 (Lib_Ghost.f90:29-387).
+// A record's layer 2 reads its own layer-1 cell and the cell one further inside (of its block, or of the
+// source block of a connection). Where that block is two cells or more deep along the record's face
+// direction the cell is interior, no other record writes it, and one thread does both layers in turn
+// (layers = 3). Where it is one cell deep the cell is the opposite face's layer-1 ghost, which another
+// record writes: then the host launches layer 1 of every record first and layer 2 after it.
 template <int CL>
-__global__ void k_ghost(Geo G, FamDev F, const DRec* recs, int nrec) {
+__global__ void k_ghost(Geo G, FamDev F, const DRec* recs, int nrec, int layers) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nrec) return;
   const DRec r = recs[n];
-  ghost1_rec<CL>(G, F, r);
-  ghost2_rec<CL>(G, F, r);
+  if (layers & 1) ghost1_rec<CL>(G, F, r);
+  if (layers & 2) ghost2_rec<CL>(G, F, r);
 }
 
 // ------------------------------------------------------------------ boundary fluxes

@@ -129,6 +129,7 @@ struct LaunchArgs {
   FamDev F;
   const DRec* recs; int nrec;
   const DRec* grecs;                                 // the records in the ghost kernel's order
+  int ghost_split;                                   // a record's second layer reads another's first
   const int* own; int nown;
   const int* bfirst; const int* blist; int nbc;
   const Tile* tiles; int ntile; int TX, TY, KZ;     // the 1-D stage kernel's tiles

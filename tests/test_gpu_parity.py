@@ -275,6 +275,28 @@ def test_cloud_3d_evaporating_ag(gpu, orc):
     run_pair(gpu, orc, lambda: configs.cloud_3d(n=24, steps=12, length=0.0024), 12)
 
 
+@pytest.mark.parametrize("closure", ["MK", "IG", "AG"])
+def test_wedge_one_cell_deep_bit_exact(gpu, orc, closure):
+    # the reference's one-degree wedge (one cell deep in k, code 200 on both k faces): each k face's
+    # second ghost layer is the other face's first, so the ghost layers run as two launches. A seeded
+    # perturbation of the density (5 %, one drop size) and the axial velocity makes every ghost value
+    # matter. The perturbed AG cloud leaves the realisable states after a dozen local steps (on the
+    # oracle as well), so it runs 10.
+    steps = 10 if closure == "AG" else 40
+
+    def make():
+        case = configs.axis_wedge(closure)
+        case.numerics.itermax = steps
+        I = case.state[0][0][2:-2, 2:-2, 2:-2]
+        rng = np.random.default_rng(5)
+        mp = I[..., -1] / I[..., 0]
+        I[..., 0] *= 1.0 + rng.uniform(-0.05, 0.05, I[..., 0].shape)
+        I[..., 1] += rng.uniform(-0.1, 0.1, I[..., 1].shape)
+        I[..., -1] = I[..., 0] * mp
+        return case
+    run_pair(gpu, orc, make, steps, exact=True)
+
+
 def test_multiblock_three_families(gpu, orc):
     # config 4 shape: a seeded tree of blocks joined by 101 connections, MK + IG + AG
     run_pair(gpu, orc, lambda: configs.multiblock_tree(nblocks=8, seed=3, lo=5, hi=11, steps=6), 6)
