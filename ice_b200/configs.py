@@ -345,6 +345,16 @@ def evaporating_tube(model="CEM", interface="VLE", steps=2000, cs=1e12, dt_max=2
     return case
 
 
+def with_families(case, families):
+    """The case with the given families in place of its one, each starting from the first family's
+    initial state (the reference's several-materials cases, test/verification/L-materials: one family
+    per material line, each reading its own material)."""
+    st = case.state[0][0]
+    case.families = list(families)
+    case.state = [[st.copy() for _ in case.families]]
+    return case
+
+
 def cloud_profile(shape, x):
     """The bulk-density profile of periodic_cloud at x in [0, 1): 10 (s(x) + 1e-6), s a Gaussian of
     width 0.06 about 0.25 summed over its periodic images ("gauss"), or a top hat of half width 0.1

@@ -1,6 +1,6 @@
 """The reference's drag- and thermal-relaxation verification cases (test/verification/A-drag-relaxation,
 B-thermal-relaxation, C-advection-sine, D-drag-matrix, E-heat-matrix, F-evaporation parts 1-4,
-G-cloud-translation, H-linear-strain, I-vortex-cloud, J-tau-limit) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
+G-cloud-translation, H-linear-strain, I-vortex-cloud, J-tau-limit, L-materials legs 1 and 2) on the oracle and on the CUDA path (plain FP64 form). A: a uniform MK cloud at rest in a uniform gas stream under
 Stokes drag relaxes as u_g + (u_p0 - u_g) exp(-t/tau), tau = rho_al dp^2 / (18 mu). The gates are the
 reference's: the velocity within 1e-5 of u_g at t/tau = 0.1 ... 5, the field uniform to 1e-12 u_g,
 density unchanged to 1e-12, number density to 1e-9, temperature to 1e-9 T_g; and observed orders of
@@ -461,6 +461,55 @@ def _vortex_checks(lib):
     assert lags[-1] >= 0.4
 
 
+def _materials_checks(lib):
+    """L, legs 1 and 2: several MK families in one case, each on its own material. L1: two families
+    with the same state (2 kg/m3, 1e-4 m drops of density 2000) at rest at 300 K in a gas at rest at
+    400 K, NoDrag, heat Stokes; materials A (cp 1000, density 2000) and B (cp 2000, density 1000); each
+    relaxes with its own tau = rho_p cp / (4 pi k R_p n), R_p from the state and its own density, to
+    1e-6 of the gap at t = tau_A (dt-max = tau_A / 1000); L1b: families 1 and 2 on A, 3 on B. L2: case F's
+    frozen cloud, family A evaporating (CEM) on the d-squared slope of the reference's correlations to
+    1e-6, family B (evaporation off, cp 2000, density 2000) keeps its bulk and number densities to the
+    last bit."""
+    from pathlib import Path
+    rho_p = 1e-3 * 2000.0
+    n = rho_p / (2000.0 * 4.0 / 3.0 * math.pi * 0.5e-4 ** 3)
+    mats = {"A": (1000.0, 2000.0), "B": (2000.0, 1000.0)}
+
+    def tau(m):
+        cp, rho_m = mats[m]
+        rp = (0.75 * rho_p / (n * math.pi * rho_m)) ** (1.0 / 3.0)
+        return rho_p * cp / (4.0 * math.pi * 0.026 * rp * n)
+
+    for fam_mat in (("A", "B"), ("A", "A", "B")):
+        t_end, dt = tau("A"), min(tau("A"), tau("B")) / 1000.0
+        steps = int(math.ceil(t_end / dt - 1e-9))
+        case = configs.relaxation_tube(dt_max=dt, steps=steps, drag="NoDrag", heat="Stokes", ug=0.0,
+                                       rho_al=2000.0, cs=1000.0)
+        case.gas = [configs._gas_layout(case, 0, 1.2, 0.0, 0.0, 0.0, 400.0)]
+        configs.with_families(case, [configs.Family("MK", rho_al=mats[m][1], cs_al=mats[m][0]) for m in fam_mat])
+        s = Solver(case, lib)
+        out = s.step(steps)
+        assert out.status == 0 and out.time >= t_end * (1.0 - 1e-12)
+        for q, m in enumerate(fam_mat):
+            temp = s.download(0, q)[2, 2, 2:-2, 4]
+            ref = 400.0 - 100.0 * math.exp(-out.time / tau(m))
+            assert float(np.abs(temp - ref).max()) / 100.0 <= 1e-6, (fam_mat, q, m)
+    g = np.load(Path(__file__).resolve().parent / "golden" / "evaporation.npz")
+    k_ref = float(g["K"][list(g["models"]).index("CEM")])
+    case = configs.evaporating_tube("CEM")
+    b = configs.Family("MK", rho_al=2000.0, cs_al=2000.0, lv_al=2.26e6, evap="none", Mv=18.015, Tboil=373.15)
+    configs.with_families(case, [case.families[0], b])
+    s = Solver(case, lib)
+    out = s.step(2000)
+    assert out.status == 0
+    n0 = 1.0 / (4.0 / 3.0 * math.pi * 0.5e-4 ** 3 * 1000.0)
+    pa, pb = s.download(0, 0)[2, 2, 2:-2], s.download(0, 1)[2, 2, 2:-2]
+    k_ice = (1e-4 ** 2 - (2.0 * (0.75 * pa[0, 0] / (n0 * math.pi * 1000.0)) ** (1.0 / 3.0)) ** 2) / out.time
+    assert abs(k_ice - k_ref) <= 1e-6 * k_ref
+    assert pa[:, 0].max() - pa[:, 0].min() <= 1e-12
+    assert np.all(pb[:, 0] == 1.0) and np.all(pb[:, 5] == n0)
+
+
 def test_drag_relaxation_oracle(orc):
     _relaxation_checks(orc)
     _order_checks(orc)
@@ -500,6 +549,10 @@ def test_strain_oracle(orc):
 
 def test_vortex_oracle(orc):
     _vortex_checks(orc)
+
+
+def test_materials_oracle(orc):
+    _materials_checks(orc)
 
 
 @pytest.mark.gpu
@@ -552,3 +605,8 @@ def test_strain_gpu():
 @pytest.mark.gpu
 def test_vortex_gpu():
     _vortex_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_materials_gpu():
+    _materials_checks(_gpu())
