@@ -19,6 +19,41 @@ from . import abi
 
 GUIDE = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]])
 
+MESH_FIT = 1e-2     # node planes match a turn or a translation to this fraction of a block's thickness
+MESH_ANGLE = 1e-6   # a node this close to the x axis, relative to the farthest, has no azimuth
+MIRROR = (200, 300, 301)
+
+
+class SetupError(ValueError):
+    """A case the reference's set-up stops on."""
+
+
+def _thickness(nodes, d):
+    """The largest move of a node from node plane 0 to plane 1 of direction d (1 = j, 2 = k), over the three
+    coordinates (Mod_Metrics.f90:286-303)."""
+    a, b = (nodes[:, 0], nodes[:, 1]) if d == 1 else (nodes[:, :, 0], nodes[:, :, 1])
+    return float(np.abs(b - a).max())
+
+
+def _plane_fit(nodes, d, delthe):
+    """How far the node planes 0 and 1 of direction d lie from the mirror planes they should be, over the
+    thickness of the block: planes normal to y (d = 1) or z (d = 2), or, on a wedge of angle delthe, the
+    planes through the x axis at -/+ delthe/2 (Mod_Metrics.f90:312-355)."""
+    thick = _thickness(nodes, d)
+    off = 0.0
+    for s in (0, 1):
+        if d == 1:
+            pl = nodes[:, s, :, 1]
+            off = max(off, float(np.abs(pl - pl[0, 0]).max()))
+        elif delthe == 0.0:
+            pl = nodes[:, :, s, 2]
+            off = max(off, float(np.abs(pl - pl[0, 0]).max()))
+        else:
+            ang = (s - 0.5) * delthe
+            pl = nodes[:, :, s]
+            off = max(off, float(np.abs(pl[..., 2] * np.cos(ang) - pl[..., 1] * np.sin(ang)).max()))
+    return off / thick if thick > 0.0 else np.inf
+
 
 # --------------------------------------------------------------------- metrics
 def _cross(u, v):
@@ -245,6 +280,102 @@ class Case:
             if nk > 1:
                 d = 3
         return d
+
+    def wedge_angle(self) -> float:
+        """check_mesh_type (Mod_Metrics.f90:103-176): on a 2-D mesh, the angle of the axisymmetric wedge when in
+        every block the k = 1 node plane is the k = 0 plane turned about the x axis by one angle, 0 when it
+        is the k = 0 plane translated; misfits are measured against the block's thickness. A block that is
+        neither, wedges of different angles, and wedge blocks beside plane ones stop the set-up."""
+        if self.ndir != 2:
+            return 0.0
+        rmax = max(float(np.hypot(n[..., 1], n[..., 2]).max()) for n in self.nodes)
+        angles = []
+        for b, n in enumerate(self.nodes):
+            p0, p1 = n[:, :, 0], n[:, :, 1]
+            thick = _thickness(n, 2)
+            move = p1 - p0
+            fit_move = float(np.abs(move - move[0, 0]).max()) / thick
+            r0 = np.hypot(p0[..., 1], p0[..., 2])
+            far = r0 > MESH_ANGLE * rmax
+            fit_turn, ang = np.inf, 0.0
+            if far.any():
+                turn = np.arctan2(p1[..., 2], p1[..., 1]) - np.arctan2(p0[..., 2], p0[..., 1])
+                ang = float(np.median(turn[far]))
+                c, s_ = np.cos(ang), np.sin(ang)
+                rot = np.stack([p0[..., 0], c * p0[..., 1] - s_ * p0[..., 2], s_ * p0[..., 1] + c * p0[..., 2]], axis=-1)
+                fit_turn = float(np.abs(p1 - rot).max()) / thick
+            turned = fit_turn <= MESH_FIT and fit_turn < fit_move and abs(ang) > MESH_ANGLE
+            moved = fit_move <= MESH_FIT and not turned
+            if not (turned or moved):
+                raise SetupError(f"block {b + 1}: its k = 1 node plane is neither the k = 0 plane turned about the x "
+                                 f"axis nor translated (the turn fits to {fit_turn:.2e} of its thickness, the "
+                                 f"translation to {fit_move:.2e})")
+            angles.append(ang if turned else None)
+        turned = [a for a in angles if a is not None]
+        if not turned:
+            return 0.0
+        if len(turned) != len(angles):
+            raise SetupError(f"{len(turned)} of the {len(angles)} blocks of the 2-D mesh are axisymmetric wedges, "
+                             "the others plane")
+        if any(abs(a - turned[0]) > MESH_FIT * abs(turned[0]) for a in turned):
+            raise SetupError("the blocks of the 2-D mesh are wedges of different angles")
+        return turned[0]
+
+    def setup_freeze(self):
+        """setup_freeze (Mod_Freeze.f90:30-140): between two faces that mirror the flow one cell apart (the k
+        faces of a 2-D mesh, the j and k faces of a 1-D one) the components odd across them have a mode the
+        time step does not resolve; they are set to zero here and not integrated (the families' frozen
+        slots, which zero their source and residual). w across mirror k faces that are planes normal to z,
+        or on an axisymmetric wedge (whose k faces must all be 200); v across mirror j faces normal to y on
+        a 1-D mesh; with AG also P13 (w), P12 (v) and P23 (either). Returns the reference's warning, or
+        None when nothing is frozen."""
+        ndir, delthe = self.ndir, self.wedge_angle()
+        nj = nk = nmj = nmk = 0
+        other = None
+        for (b, i, j, k, f, code, _pay) in self.bc_rows:
+            if f in (3, 4):
+                nj += 1
+                nmj += code in MIRROR
+            elif f in (5, 6):
+                nk += 1
+                nmk += code in MIRROR
+                if code != 200 and other is None:
+                    other = (b, i, j, f, code)
+        freeze_v = freeze_w = False
+        if ndir == 2 and delthe != 0.0:
+            if other is not None:
+                b, i, j, f, code = other
+                raise SetupError(f"face {f} of the cell (block i j) {b} {i} {j} carries {code}: the k faces of an "
+                                 "axisymmetric wedge must carry 200, the mirror that keeps the flow axisymmetric")
+            if max(_plane_fit(n, 2, delthe) for n in self.nodes) > MESH_FIT:
+                raise SetupError("the k node planes of the axisymmetric wedge are not the planes at -/+ delthe/2 "
+                                 "about z = 0: the wedge must be symmetric about the plane z = 0")
+            freeze_w = True
+        elif ndir <= 2:
+            if nk > 0 and nmk == nk:
+                freeze_w = max(_plane_fit(n, 2, 0.0) for n in self.nodes) <= MESH_FIT
+            if ndir == 1 and nj > 0 and nmj == nj:
+                freeze_v = max(_plane_fit(n, 1, 0.0) for n in self.nodes) <= MESH_FIT
+        for p, fam in enumerate(self.families):
+            odd = {3: freeze_v, 4: freeze_w}
+            if fam.closure == "AG":
+                odd.update({6: freeze_v, 7: freeze_w, 9: freeze_v or freeze_w})
+            fam.frozen = tuple(sorted(slot for slot, on in odd.items() if on))
+            for per_fam in self.state:
+                for slot in fam.frozen:
+                    per_fam[p][..., slot - 1] = 0.0
+        if not (freeze_v or freeze_w):
+            return None
+        ag = any(f.closure == "AG" for f in self.families)
+        if freeze_v and freeze_w:
+            what, faces = ("v and w (with AG also P12, P13 and P23)" if ag else "v and w"), "j and k"
+        elif freeze_v:
+            what, faces = ("v (with AG also P12 and P23)" if ag else "v"), "j"
+        else:
+            what, faces = ("w (with AG also P13 and P23)" if ag else "w"), "k"
+        if ndir == 2 and delthe != 0.0:
+            return f"axisymmetric wedge: the swirl {what} set to zero and not integrated"
+        return f"{'2-D plane' if ndir == 2 else '1-D'} mesh with mirror {faces} faces: {what} set to zero and not integrated"
 
     @property
     def ncells(self):

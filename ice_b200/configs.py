@@ -231,6 +231,45 @@ def axis_wedge(closure="MK", precision=0):
     return _single_block("axis_wedge", nodes, fam, num, codes, prims, payload)
 
 
+def mirror_layer(kind="slab", closure="IG", side_code=300):
+    """The reference's mirror-modes cases (test/fast/mirror-modes): a cloud at rest (rho 1, P = 1, T 300,
+    10 um drops of density 2000, cp 1000) whose components odd across the mirror faces start at 1e-8 of
+    the signal speed: s = 1e-8 sin(2 pi x / L) cos(pi y / H_y), w = sqrt(3) s (AG: P13 = P23 = s; the tube
+    also v = sqrt(3) s, AG P12 = s), every face code 300 (a wall); RK2, CFL 0.8, dt-max 1e3, local steps,
+    MUSCL van Leer, 200 steps. slab: 16 x 8 cells of 2.5 mm, 1e-5 m thick; tube: 32 cells along 0.04 m,
+    1e-5 m across; wedge: the slab's x and 8 radial cells from r = 1e-8 to 0.02 turned by one degree, its
+    k faces carrying side_code."""
+    h, n_x, n_y, length = 1e-5, 16, 8, 0.04
+    if kind == "tube":
+        nodes = box_nodes(2 * n_x, 1, 1, lo=(0.0, -0.5 * h, -0.5 * h), size=(length, h, h))
+    elif kind == "slab":
+        nodes = box_nodes(n_x, n_y, 1, lo=(0.0, 0.0, -0.5 * h), size=(length, 0.5 * length, h))
+    else:
+        X, R, T = np.meshgrid(np.linspace(0.0, length, n_x + 1), np.linspace(1e-8, 0.5 * length, n_y + 1),
+                              np.radians([-0.5, 0.5]), indexing="ij")
+        nodes = np.stack([X, R * np.cos(T), R * np.sin(T)], axis=-1)
+    x, y, _ = _cell_centres(nodes)
+    y0, y1 = float(nodes[..., 1].min()), float(nodes[:, -1, 0, 1].max())
+    s = 1e-8 * np.sin(2.0 * math.pi * x / length) * np.cos(math.pi * (y - y0) / (y1 - y0))
+    odd_v = kind == "tube"
+    c = math.sqrt(3.0)
+    w = c * s if kind != "wedge" else 0.0 * s
+    v = c * s if odd_v else 0.0 * s
+    n = 1.0 / particle_mass(1e-5, 2000.0)
+    fam = Family(closure, rho_al=2000.0, cs_al=1000.0)
+    num = Numerics(scheme="RK2", cfl=0.8, dt_max=1e3, limiter="vanleer", time_accurate=False, itermax=200)
+    codes = {f: 300 for f in range(1, 7)}
+    if kind == "wedge":
+        codes[5] = codes[6] = side_code
+    if closure == "IG":
+        prims = [1.0, 0.0, v, w, 1.0, 300.0, n]
+    else:
+        odd = kind != "wedge"
+        prims = [1.0, 0.0, v, w, 1.0, s if odd_v else 0.0 * s, s if odd else 0.0 * s, 1.0,
+                 s if odd else 0.0 * s, 1.0, 300.0, n]
+    return _single_block("mirror_layer", nodes, fam, num, codes, prims)
+
+
 def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
     """The setting of the reference's unit test of the steps of empty cells a source fills
     (test/unit/test_empty_dt.f90): one block of 4 x 1 x 1 cells of 1 mm (the last 0.1 mm wide when

@@ -24,6 +24,7 @@ class Solver:
             case.build_geometry()
         if case.rec_int is None:
             case.build_records(self.lib)
+        self.freeze_note = case.setup_freeze()
         self.params = case.params()
         dims = np.array(case.dims, dtype=np.int32).reshape(-1)
         ctx = C.c_void_p()

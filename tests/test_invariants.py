@@ -1,12 +1,14 @@
 """The reference's invariant cases, on the oracle and on the CUDA path, with the gates of their verify.py:
 test/NoExchange/MK (an uncoupled cloud keeps its state bit for bit), test/Reflect/AG (x-momentum
 conserved along a symmetry plane), test/Thermal/{IG,AG} (the temperature of an expanding blob stays
-uniform) and test/Axis/{MK,IG,AG} (a one-degree wedge about x: a stationary MK stream keeps its axis
-row, IG and AG clouds at rest stay at rest)."""
+uniform), test/Axis/{MK,IG,AG} (a one-degree wedge about x: a stationary MK stream keeps its axis
+row, IG and AG clouds at rest stay at rest), and test/fast/mirror-modes (the components odd across
+mirror faces one cell apart are set to zero at set-up and not integrated)."""
 import numpy as np
 import pytest
 
 from ice_b200 import abi, configs
+from ice_b200.case import SetupError
 from ice_b200.solver import Solver
 
 
@@ -80,6 +82,38 @@ def _axis(lib, closure):
     assert float((np.abs(v[..., 1:4]).max(-1) / c).max()) < 1e-10
     assert float(np.abs(v[..., 0] - 1.0).max()) < 1e-10
     assert max(float(np.abs(v[..., q] - 1.0).max()) for q in diag) < 1e-10
+
+
+def _mirror_modes(lib):
+    """slab (IG, AG): a 2-D layer 1e-5 m thick between wall k faces under cells of 2.5 mm, its odd
+    components seeded at 1e-8: after 200 steps w (AG also P13, P23) is zero in every cell, the cloud at
+    rest (|u|, |v| below 1e-10), and the set-up's warning names w. tube (IG): a 1-D tube between wall j
+    and k faces: v and w zero. A wedge whose k faces are walls instead of 200: the set-up stops and says
+    why (mirror-modes/run.py)."""
+    for closure, odd in (("IG", [3]), ("AG", [3, 6, 8])):
+        s = Solver(configs.mirror_layer("slab", closure), lib)
+        assert "2-D plane mesh with mirror k faces: w" in s.freeze_note
+        out = s.step(200)
+        assert out.status == 0
+        v = s.download(0, 0)[2:-2, 2:-2, 2:-2]
+        assert all(float(np.abs(v[..., q]).max()) == 0.0 for q in odd)
+        assert float(np.abs(v[..., 1:3]).max()) < 1e-10
+    s = Solver(configs.mirror_layer("tube", "IG"), lib)
+    assert "1-D mesh with mirror j and k faces: v and w" in s.freeze_note
+    assert s.step(200).status == 0
+    v = s.download(0, 0)[2:-2, 2:-2, 2:-2]
+    assert float(np.abs(v[..., 2:4]).max()) == 0.0
+    with pytest.raises(SetupError, match="the k faces of an axisymmetric wedge must carry 200"):
+        Solver(configs.mirror_layer("wedge", "IG", side_code=300), lib)
+
+
+def test_mirror_modes_oracle(orc):
+    _mirror_modes(orc)
+
+
+@pytest.mark.gpu
+def test_mirror_modes_gpu():
+    _mirror_modes(_gpu())
 
 
 def test_noexchange_oracle(orc):
