@@ -98,6 +98,8 @@ _SIGNATURES = [
     ("upload_state", C.c_int, [_vp, C.c_int32, C.c_int32, _dp, _u8p]),
     ("download_state", C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),
     ("set_time", C.c_int, [_vp, C.c_double, C.c_int32, C.c_int32]),
+    ("set_res_reference", C.c_int, [_vp, C.c_double]),
+    ("get_res_reference", C.c_int, [_vp, _dp]),
     ("step", C.c_int, [_vp, C.c_int32, C.POINTER(StepOut)]),
     ("residual_norm", C.c_int, [_vp, _dp, _dp]),
     ("update_params", C.c_int, [_vp, C.POINTER(Params)]),

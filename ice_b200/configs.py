@@ -270,6 +270,58 @@ def mirror_layer(kind="slab", closure="IG", side_code=300):
     return _single_block("mirror_layer", nodes, fam, num, codes, prims)
 
 
+def inlet_duct(kind="normal"):
+    """The reference's inlet-direction case (test/fast/inlet-direction): a 1-D duct of 16 cells along
+    0.16 m, an MK cloud at rest (1e-3 kg/m3 of 10 um drops of density 1000, 300 K), extrapolation on the
+    i and j faces, the inlet on face 2 (x = 0.16, whose normal points out of the domain); RK2, CFL 0.5,
+    NoDrag, NoHeat, 200 steps. normal: a 402 inlet of 1 kg/(s m2) at 10 m/s along the face normal, 300 K,
+    10 um, no gas. angles: a 401 inlet (mass ratio 1, kV = kT = 1) with explicit angles alpha = 180 deg,
+    beta = 0, in a gas (1.2 kg/m3, 300 K) moving along -x at 10 m/s."""
+    nx, lx = 16, 0.16
+    nodes = box_nodes(nx, 1, 1, size=(lx, lx / nx, lx / nx))
+    fam = Family("MK", rho_al=1000.0, cs_al=900.0)
+    num = Numerics(scheme="RK2", cfl=0.5, limiter="vanleer", coupled=kind == "angles", drag="NoDrag",
+                   heat="NoHeat", itermax=200)
+    mass = particle_mass(1e-5, 1000.0)
+    if kind == "normal":
+        code, pay = 402, (1.0, 10.0, 0.0, 0.0, 300.0, 1e-5, 0.0, 1.0)
+    else:
+        code, pay = 401, (1.0, 1.0, math.pi, 0.0, 1.0, 1e-5, 0.0, 0.0)
+    case = _single_block("inlet_duct", nodes, fam, num, {1: 400, 2: code, 3: 400, 4: 400, 5: 0, 6: 0},
+                         [1e-3, 0.0, 0.0, 0.0, 300.0, 1e-3 / mass], lambda f, i, j, k: pay)
+    if kind == "angles":
+        case.gas = [_gas_layout(case, 0, 1.2, -10.0, 0.0, 0.0, 300.0)]
+    return case
+
+
+def stream_tube(kind="scaling", scale=1.0):
+    """The reference's res-threshold cases (test/fast/res-threshold), steady (local steps), res-threshold
+    1e-5, MK drops of 10 um and density 1000 at 300 K, extrapolation on every face but the inlet.
+    scaling: 32 cells along 0.32 m, rho = scale (1 + 0.5 sin(2 pi x / 0.32)) moving at 10 m/s, fed through
+    face 1 by a 402 inlet of scale x 10 kg/(s m2) at 10 m/s along the normal; RK2, CFL 0.8, NoDrag, NoHeat.
+    at_rest: the same density at rest in a uniform gas at 10 m/s (1.2 kg/m3, 300 K), Stokes drag and
+    heat, one-stage Euler steps, no inlet. frozen: 16 cells along 0.16 m of a uniform cloud (1 kg/m3)
+    moving at 10 m/s out through face 2; RK2, 40 iterations."""
+    mass = particle_mass(1e-5, 1000.0)
+    nx, lx = (16, 0.16) if kind == "frozen" else (32, 0.32)
+    nodes = box_nodes(nx, 1, 1, size=(lx, lx / nx, lx / nx))
+    fam = Family("MK", rho_al=1000.0, cs_al=900.0)
+    num = Numerics(scheme="euler" if kind == "at_rest" else "RK2", cfl=0.8, limiter="vanleer",
+                   time_accurate=False, coupled=kind == "at_rest",
+                   drag="Stokes" if kind == "at_rest" else "NoDrag", heat="Stokes" if kind == "at_rest" else "NoHeat",
+                   itermax=40 if kind == "frozen" else 20000, res_threshold=1e-5)
+    x = (np.arange(nx) + 0.5) * (lx / nx)
+    rho = np.ones(nx) if kind == "frozen" else scale * (1.0 + 0.5 * np.sin(2.0 * math.pi * x / lx))
+    u = 0.0 if kind == "at_rest" else 10.0
+    codes = {1: 402 if kind == "scaling" else 400, 2: 400, 3: 400, 4: 400, 5: 0, 6: 0}
+    pay = (scale * 10.0, 10.0, 0.0, 0.0, 300.0, 1e-5, 0.0, 1.0)
+    prims = [rho[:, None, None], u, 0.0, 0.0, 300.0, (rho / mass)[:, None, None]]
+    case = _single_block("stream_tube", nodes, fam, num, codes, prims, lambda f, i, j, k: pay)
+    if kind == "at_rest":
+        case.gas = [_gas_layout(case, 0, 1.2, 10.0, 0.0, 0.0, 300.0)]
+    return case
+
+
 def empty_tube(n_occupied=2, time_accurate=False, narrow_last=False, steps=1):
     """The setting of the reference's unit test of the steps of empty cells a source fills
     (test/unit/test_empty_dt.f90): one block of 4 x 1 x 1 cells of 1 mm (the last 0.1 mm wide when

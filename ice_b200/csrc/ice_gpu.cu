@@ -143,6 +143,9 @@ struct ice_gpu_ctx {
   DevBuf<double> xall;
   int phase = 0;          // buffer holding the current state
   int prev_phase = -1;    // buffer holding the state before the last step
+  double res_reference = 0.0;  // the first non-zero density residual of a steady run (0: none yet)
+  bool res_end = false;        // the last step ended the run on res-threshold
+  double last_norm[5] = {0, 0, 0, 0, 0};
   bool profiling = false;
   double kms[KC_N] = {0};
   long long nlaunch = 0;
@@ -776,6 +779,19 @@ int ice_gpu_set_time(ice_gpu_ctx* c, double time, int32_t iter, int32_t iter_fro
   return 0;
 }
 
+int ice_gpu_set_res_reference(ice_gpu_ctx* c, double ref) {
+  if (!c) return ICE_GPU_EINVAL;
+  c->res_reference = ref;
+  return 0;
+}
+
+int ice_gpu_get_res_reference(ice_gpu_ctx* c, double* ref) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (!ref) return fail(c, ICE_GPU_EINVAL, "get_res_reference: null pointer");
+  *ref = c->res_reference;
+  return 0;
+}
+
 int ice_gpu_update_params(ice_gpu_ctx* c, const ice_gpu_params* P) {
   if (!c || !P) return ICE_GPU_EINVAL;
   if (P->nfam != c->P.nfam || P->ndir != c->P.ndir) return fail(c, ICE_GPU_EINVAL, "update_params: nfam and ndir may not change");
@@ -1119,10 +1135,15 @@ int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
     for (double& x : c->kms) x = 0.0;
     c->nlaunch = 0;
   }
+  // res-threshold ends a steady run once its density residual has fallen by res_threshold from the
+  // first non-zero one (Mod_Explicit.f90:193-240): such a run takes the norm after every step and the
+  // call ends at the step that meets it
+  const bool res_stop = !c->P.time_accurate && c->P.res_threshold > 0.0;
+  c->res_end = false;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   CK(cudaEventCreate(&t0)); CK(cudaEventCreate(&t1));
   CK(cudaEventRecord(t0, s));
-  for (int n = 0; n < nsteps; ++n) {
+  for (int n = 0; n < nsteps && !c->res_end; ++n) {
     int ph = c->phase;
     if (c->profiling) {
       CK(cudaEventRecord(c->ev0, s));
@@ -1141,6 +1162,14 @@ int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
     }
     c->prev_phase = ph;
     c->phase = next_phase(c, ph);
+    if (res_stop) {
+      if (int rc = ice_gpu_residual_norm(c, c->last_norm, nullptr)) {
+        cudaEventDestroy(t0); cudaEventDestroy(t1);
+        return rc;
+      }
+      if (c->res_reference == 0.0) c->res_reference = c->last_norm[0];
+      c->res_end = c->res_reference > 0.0 && c->last_norm[0] <= c->P.res_threshold * c->res_reference;
+    }
   }
   CK(cudaEventRecord(t1, s));
   CK(cudaStreamSynchronize(s));
@@ -1158,11 +1187,12 @@ static int finish_step(ice_gpu_ctx* c, ice_gpu_step_out* out, float dms) {
   int rc = 0;
   if (out) {
     out->dtglobal = h.dtglobal; out->time = h.time; out->iter = h.iter; out->status = (int)h.flags;
-    out->nfloored = (int64_t)h.nfloored; out->have_norm = 0;
-    bool endsim = h.iter_from_call >= c->P.itermax || h.time >= c->P.time_threshold;
+    const bool res_stop = !c->P.time_accurate && c->P.res_threshold > 0.0;
+    out->nfloored = (int64_t)h.nfloored; out->have_norm = res_stop ? 1 : 0;
+    bool endsim = h.iter_from_call >= c->P.itermax || c->res_end || h.time >= c->P.time_threshold;
     bool iosim = c->P.sol_diter > 0 && h.iter % c->P.sol_diter == 0;
     out->todo = endsim ? 3 : iosim ? 2 : 1;
-    for (int m = 0; m < 5; ++m) out->residual[m] = 0.0;
+    for (int m = 0; m < 5; ++m) out->residual[m] = res_stop ? c->last_norm[m] : 0.0;
     out->device_ms = dms;
   }
   if (h.flags & (ICE_GPU_ST_NAN_STATE | ICE_GPU_ST_BAD_RECON)) {
@@ -1189,7 +1219,9 @@ int ice_gpu_step_host(ice_gpu_ctx* c, int32_t nsteps, const double* const* prim_
   for (int q = 0; q < c->nb * nf; ++q)
     if (!prim_in[q] || !prim_out[q]) return fail(c, ICE_GPU_EINVAL, "step_host: null array for block %d family %d",
                                                  q / nf + 1, q % nf + 1);
-  if (c->profiling) {                 // per-class timing: the plain calls, one after another
+  if (c->profiling || (!c->P.time_accurate && c->P.res_threshold > 0.0)) {
+    // per-class timing, or a steady run that may end on res-threshold inside the call: the plain
+    // calls, one after another
     for (int b = 0; b < c->nb; ++b)
       for (int p = 0; p < nf; ++p)
         if (int rc = ice_gpu_upload_state(c, b + 1, p + 1, prim_in[b * nf + p], nullptr)) return rc;

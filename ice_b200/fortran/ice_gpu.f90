@@ -44,7 +44,8 @@ module ice_gpu
   public :: ice_gpu_create, ice_gpu_set_block, ice_gpu_set_records, ice_gpu_set_chimera, ice_gpu_set_gas, &
             ice_gpu_set_imports, ice_gpu_set_exchange, ice_gpu_exchange_rate, ice_gpu_step_host, &
             ice_gpu_upload_state, &
-            ice_gpu_download_state, ice_gpu_set_time, ice_gpu_step, ice_gpu_residual_norm, ice_gpu_update_params, &
+            ice_gpu_download_state, ice_gpu_set_time, ice_gpu_set_res_reference, ice_gpu_get_res_reference, &
+            ice_gpu_step, ice_gpu_residual_norm, ice_gpu_update_params, &
             ice_gpu_last_error, ice_gpu_destroy, ice_gpu_pair_connections
 
   interface
@@ -136,6 +137,18 @@ module ice_gpu
       type(c_ptr), value        :: ctx
       real(c_double), value     :: time
       integer(c_int32_t), value :: iter, iter_from_call
+    end function
+
+    integer(c_int) function ice_gpu_set_res_reference(ctx, ref) bind(C, name='ice_gpu_set_res_reference')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value    :: ctx
+      real(c_double), value :: ref
+    end function
+
+    integer(c_int) function ice_gpu_get_res_reference(ctx, ref) bind(C, name='ice_gpu_get_res_reference')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value          :: ctx
+      real(c_double), intent(out) :: ref
     end function
 
     integer(c_int) function ice_gpu_step(ctx, nsteps, out) bind(C, name='ice_gpu_step')

@@ -239,9 +239,19 @@ int ice_gpu_download_state(ice_gpu_ctx* ctx, int32_t b, int32_t p, double* prim)
 /* Simulated time and iteration count (a restart, or a second call of the solver). */
 int ice_gpu_set_time(ice_gpu_ctx* ctx, double time, int32_t iter, int32_t iter_from_call);
 
+/* The unit of res-threshold: the first non-zero density residual of a steady run (0 until one has
+ * come; set from a restart's counters, read to write them).
+ * replaces: obj_sim_param%res_reference (config/Config_Types_m.f90:45; driver/Wrap_Setup.f90:197-215,
+ * io/IO_Solution.f90:244,440). */
+int ice_gpu_set_res_reference(ice_gpu_ctx* ctx, double ref);
+int ice_gpu_get_res_reference(ice_gpu_ctx* ctx, double* ref);
+
 /* nsteps time steps. replaces: call Explicit_Step(grid) (driver/Wrap_Solve.f90:26),
  * numerics/time/explicit/Mod_Explicit.f90:11-245. Returns ICE_GPU_ESTATE when a
- * step ended on a state the reference stops on (out->status says which). */
+ * step ended on a state the reference stops on (out->status says which). A steady run with
+ * res_threshold > 0 takes the residual norm after every step (out->residual) and the call ends at
+ * the step whose density residual is at most res_threshold times the run's first non-zero one
+ * (out->todo = 3), as the driver's loop ends on TODO = 3. */
 int ice_gpu_step(ice_gpu_ctx* ctx, int32_t nsteps, ice_gpu_step_out* out);
 
 /* nsteps time steps for a driver that keeps the state on the host. prim_in[(b-1)*nfam + (p-1)]

@@ -75,6 +75,8 @@ typedef struct orc_ctx {
     int status;
     double residuo[5], residuofam[5*MAXF];
     int have_norm;
+    double res_reference; /* the first non-zero density residual of a steady run (0: none yet) */
+    int res_end;          /* the last step ended the run on res-threshold */
     double* fbuf;         /* face flux scratch */
     size_t fbuf_n;
     char err[512];
@@ -223,6 +225,17 @@ int orc_download_aux(const orc_ctx* c, int b1, int p1, double* dt, double* tau, 
 
 int orc_set_time(orc_ctx* c, double time, int iter, int iter_from_call) {
     c->time = time; c->iter = iter; c->iter_from_call = iter_from_call;
+    return 0;
+}
+
+int orc_set_res_reference(orc_ctx* c, double ref) {
+    c->res_reference = ref;
+    return 0;
+}
+
+int orc_get_res_reference(orc_ctx* c, double* ref) {
+    if (!ref) return seterr(c, ICE_GPU_EINVAL, "get_res_reference: null pointer");
+    *ref = c->res_reference;
     return 0;
 }
 
@@ -1196,12 +1209,17 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
             if (state_update(c, p, srk)) { c->status |= ICE_GPU_ST_NAN_STATE; return ICE_GPU_ESTATE; }
         }
     }
+    /* res-threshold ends a steady run once its density residual has fallen by res_threshold from the
+     * first non-zero one (Mod_Explicit.f90:193-240): a residual of zero (a cloud at rest at its first
+     * one-stage step) is no reference, and until one has come the residual ends nothing */
     int res_stop = !c->P.time_accurate && c->P.res_threshold > 0.0;
     int need_norm = res_stop || due(c->iter, c->P.res_diter) || due(c->iter, c->P.shell_diter) ||
                     c->iter_from_call >= c->P.itermax || c->time >= c->P.time_threshold;
     c->have_norm = 0;
     if (need_norm) residual_norm(c);
-    int endsim = c->iter_from_call >= c->P.itermax || c->time >= c->P.time_threshold;
+    if (res_stop && c->res_reference == 0.0) c->res_reference = c->residuo[0];
+    c->res_end = res_stop && c->res_reference > 0.0 && c->residuo[0] <= c->P.res_threshold * c->res_reference;
+    int endsim = c->iter_from_call >= c->P.itermax || c->res_end || c->time >= c->P.time_threshold;
     int iosim = (c->P.sol_diter > 0 && c->iter % c->P.sol_diter == 0);
     if (out) {
         out->todo = endsim ? 3 : iosim ? 2 : 1;
@@ -1215,7 +1233,8 @@ int orc_step(orc_ctx* c, int nsteps, ice_gpu_step_out* out) {
     int rc = 0;
     if (c->nchim > 0 && !c->have_chim)
         return seterr(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (set_chimera)", c->nchim);
-    for (int s = 0; s < nsteps && !rc; ++s) rc = explicit_step(c, out);
+    c->res_end = 0;
+    for (int s = 0; s < nsteps && !rc && !c->res_end; ++s) rc = explicit_step(c, out);
     if (out) {
         out->dtglobal = c->dtglobal; out->time = c->time; out->iter = c->iter;
         out->status = c->status; out->nfloored = c->nfloored; out->device_ms = 0.0;

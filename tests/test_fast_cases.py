@@ -1,0 +1,105 @@
+"""The reference's fast cases that exercise the step, on the oracle and on the CUDA path:
+test/fast/inlet-direction (an inlet on a face whose normal points out of the domain injects into it)
+and test/fast/res-threshold (a steady run ends when its density residual has fallen by res-threshold
+from the first non-zero one; Mod_Explicit.f90:193-240)."""
+import numpy as np
+import pytest
+
+from ice_b200 import abi, configs
+from ice_b200.solver import Solver
+
+THR, ITERS = 1e-5, 20000
+
+
+def _gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    return abi.load_gpu()
+
+
+def _inlet_direction(lib):
+    """normal: a 402 inlet along the normal of face 2 gives the inlet cell u = -10 m/s and the injected
+    density gp / v = 0.1 after 200 steps, to 1e-9. angles: a 401 inlet at alpha = 180 deg in a gas moving
+    along -x gives u = -kV 10 m/s there (inlet-direction/run.py: normal, angles)."""
+    s = Solver(configs.inlet_duct("normal"), lib)
+    assert s.step(200).status == 0
+    p = s.download(0, 0)[2, 2, 2:-2]
+    assert abs(p[-1, 1] + 10.0) <= 1e-9 * 10.0 and abs(p[-1, 0] - 0.1) <= 1e-9 * 0.1
+    s = Solver(configs.inlet_duct("angles"), lib)
+    assert s.step(200).status == 0
+    p = s.download(0, 0)[2, 2, 2:-2]
+    assert abs(p[-1, 1] + 10.0) <= 1e-9 * 10.0
+
+
+def _history(lib, case):
+    """The density residual of every step, one call per step, up to the step that ends the run."""
+    s = Solver(case, lib)
+    rows = []
+    for _ in range(ITERS):
+        out = s.step(1)
+        assert out.status == 0 and out.have_norm == 1
+        rows.append((out.iter, out.residual[0]))
+        if out.todo == 3:
+            break
+    ref = np.zeros(1)
+    assert lib.get_res_reference(s.ctx, abi.ptr(ref)) == abi.OK
+    return rows, float(ref[0])
+
+
+def _ended_on_residual(rows, ref):
+    """The last row is the first after the first non-zero residual at or below THR times it."""
+    k0 = next(k for k, (_, r) in enumerate(rows) if r > 0.0)
+    assert ref == rows[k0][1]
+    below = [k for k, (_, r) in enumerate(rows) if k > k0 and r <= THR * ref]
+    return bool(below) and below[0] == len(rows) - 1
+
+
+def _res_threshold(lib):
+    """scaling: a density wave carried out of a 1-D stream, at loading 1 and 2^-16 (an exact scaling of
+    the MK equations): both end on their first residual below 1e-5 of their first, at the same
+    iteration, and one call of 20000 steps ends at that step. at rest: the first one-stage step moves no
+    mass, its residual is exactly zero and ends nothing. frozen: every residual is zero, the run goes to
+    its 40 iterations (res-threshold/run.py)."""
+    ends = []
+    for scale in (1.0, 2.0 ** -16):
+        rows, ref = _history(lib, configs.stream_tube("scaling", scale))
+        assert _ended_on_residual(rows, ref)
+        ends.append(rows[-1][0])
+        out = Solver(configs.stream_tube("scaling", scale), lib).step(ITERS)
+        assert out.todo == 3 and out.iter == rows[-1][0]
+    assert ends[0] == ends[1] and 1 < ends[0] < ITERS
+    rows, ref = _history(lib, configs.stream_tube("at_rest"))
+    assert rows[0][1] == 0.0 and len(rows) > 1 and _ended_on_residual(rows, ref) and rows[-1][0] < ITERS
+    s = Solver(configs.stream_tube("frozen"), lib)
+    out = s.step(40)
+    assert out.iter == 40 and out.todo == 3 and out.residual[0] == 0.0
+    ref = np.zeros(1)
+    assert lib.get_res_reference(s.ctx, abi.ptr(ref)) == abi.OK and ref[0] == 0.0
+
+
+def test_inlet_direction_oracle(orc):
+    _inlet_direction(orc)
+
+
+def test_res_threshold_oracle(orc):
+    _res_threshold(orc)
+
+
+def test_res_reference_is_settable(orc):
+    """A restart gives the run its reference back: with one larger than any residual of the run, the
+    first step ends it."""
+    s = Solver(configs.stream_tube("scaling"), orc)
+    assert orc.set_res_reference(s.ctx, 1e30) == abi.OK
+    out = s.step(ITERS)
+    assert out.iter == 1 and out.todo == 3
+
+
+@pytest.mark.gpu
+def test_inlet_direction_gpu():
+    _inlet_direction(_gpu())
+
+
+@pytest.mark.gpu
+def test_res_threshold_gpu():
+    _res_threshold(_gpu())
