@@ -1,7 +1,8 @@
 """The reference's fast cases that exercise the step, on the oracle and on the CUDA path:
-test/fast/inlet-direction (an inlet on a face whose normal points out of the domain injects into it)
-and test/fast/res-threshold (a steady run ends when its density residual has fallen by res-threshold
-from the first non-zero one; Mod_Explicit.f90:193-240)."""
+test/fast/inlet-direction (an inlet on a face whose normal points out of the domain injects into it),
+test/fast/res-threshold (a steady run ends when its density residual has fallen by res-threshold
+from the first non-zero one; Mod_Explicit.f90:193-240) and the family leg of test/fast/equiv3d (a
+family in company steps as it does alone)."""
 import numpy as np
 import pytest
 
@@ -78,6 +79,33 @@ def _res_threshold(lib):
     assert lib.get_res_reference(s.ctx, abi.ptr(ref)) == abi.OK and ref[0] == 0.0
 
 
+def _family_company(lib, precision=0):
+    """The MK + IG + AG multi-block case (8 blocks joined by connections, drag, heat, radiation and
+    evaporation) against each family run alone: within a step the families are independent, and with
+    dt-max binding every cell the step is the same, so family K in company equals family K alone value
+    for value (equiv3d/run.py, family leg)."""
+    def make(solo=None):
+        c = configs.multiblock_tree(nblocks=8, seed=3, lo=5, hi=11, steps=6, precision=precision)
+        c.numerics.dt_max = 1e-9
+        if solo is not None:
+            c.families = [c.families[solo]]
+            c.state = [[per_fam[solo]] for per_fam in c.state]
+        return c
+    case = make()
+    s = Solver(case, lib)
+    out = s.step(6)
+    assert out.status == 0 and out.dtglobal == 1e-9
+    for k in range(3):
+        alone = Solver(make(k), lib)
+        assert alone.step(6).status == 0
+        for b in range(len(case.nodes)):
+            assert np.array_equal(alone.download(b, 0)[2:-2, 2:-2, 2:-2], s.download(b, k)[2:-2, 2:-2, 2:-2]), (k, b)
+
+
+def test_family_company_oracle(orc):
+    _family_company(orc)
+
+
 def test_inlet_direction_oracle(orc):
     _inlet_direction(orc)
 
@@ -103,3 +131,9 @@ def test_inlet_direction_gpu():
 @pytest.mark.gpu
 def test_res_threshold_gpu():
     _res_threshold(_gpu())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_FP32FLUX], ids=["fp64", "fp32flux"])
+def test_family_company_gpu(precision):
+    _family_company(_gpu(), precision)
