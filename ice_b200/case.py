@@ -266,6 +266,10 @@ class Case:
     chim_n: np.ndarray = None
     chim_donor: np.ndarray = None
     chim_weight: np.ndarray = None
+    # per-family copies of the table (ATLAS writes one copy per population, each with its own inlet
+    # data; copy c drives family c): None, one copy (it speaks for every family) or one per family.
+    # Every copy lists the same rows; only the inlet payloads differ.
+    bc_copies: list = None
 
     @property
     def dims(self):
@@ -408,15 +412,26 @@ class Case:
         self.geoms = [Geometry(n) for n in self.nodes]
 
     def build_records(self, lib: abi.Backend):
-        """Fan one copy of the table out over the families (IO_BC.f90:296-330) and pair
-        the connections with the library's ice_gpu_pair_connections."""
+        """The records of every family, record n of family p at n * nfam + p: one copy of the table
+        speaks for every family, one copy per family (bc_copies) each for its own, any other count stops
+        the set-up (IO_BC.f90:290-320); then the connections paired by the library's
+        ice_gpu_pair_connections."""
         ng = len(self.families)
         nrow = len(self.bc_rows)
+        copies = [self.bc_rows] * ng
+        if self.bc_copies is not None:
+            if len(self.bc_copies) not in (1, ng):
+                raise SetupError(f"{len(self.bc_copies)} copies of the boundary table for {ng} families: one "
+                                 "copy speaks for every family, else one copy per family")
+            copies = list(self.bc_copies) * (ng if len(self.bc_copies) == 1 else 1)
+            for c, rows in enumerate(copies):
+                if len(rows) != nrow or any(r[:6] != q[:6] for r, q in zip(rows, self.bc_rows)):
+                    raise SetupError(f"copy {c + 1} of the boundary table does not list the rows of the first")
         ri = np.zeros((nrow * ng, abi.REC_INTS), dtype=np.int32)
         rr = np.zeros((nrow * ng, abi.REC_REALS), dtype=np.float64)
-        for n, row in enumerate(self.bc_rows):
-            b, i, j, k, f, code, pay = row
+        for n in range(nrow):
             for p in range(ng):
+                b, i, j, k, f, code, pay = copies[p][n]
                 idx = n * ng + p
                 ri[idx, :7] = (b, i, j, k, f, code, p + 1)
                 if code in (101, 201):

@@ -294,6 +294,36 @@ def inlet_duct(kind="normal"):
     return case
 
 
+def population_duct(copies=3, families=3, scaled=True):
+    """The reference's populations case (test/fast/populations): a duct of 16 x 4 cells over 0.16 x 0.04 m,
+    MK families of 10 um drops (density 1000) at rest at 300 K, loaded 1e-3 kg/m3 (times 2^(p-1) for
+    family p when scaled); a 402 inlet on face 1 (10 m/s along the normal, 300 K, 10 um) whose mass flux is
+    2 kg/(s m2) times 2^c in copy c of the boundary table; extrapolation on faces 2-4; RK2, CFL 0.8,
+    30 steps, no gas."""
+    mass = particle_mass(1e-5, 1000.0)
+    nodes = box_nodes(16, 4, 1, size=(0.16, 0.04, 0.01))
+    fam = Family("MK", rho_al=1000.0, cs_al=900.0)
+    num = Numerics(scheme="RK2", cfl=0.8, limiter="vanleer", itermax=30)
+    codes = {1: 402, 2: 400, 3: 400, 4: 400, 5: 0, 6: 0}
+    tables = [box_bc(1, (16, 4, 1), codes, lambda f, i, j, k, c=c: (2.0 * 2.0 ** c, 10.0, 0.0, 0.0, 300.0, 1e-5,
+                                                                     0.0, 1.0))
+              for c in range(copies)]
+    case = _single_block("population_duct", nodes, fam, num, codes, [1e-3, 0.0, 0.0, 0.0, 300.0, 1e-3 / mass])
+    case.bc_rows = tables[0]
+    case.bc_copies = tables
+    st = case.state[0][0]
+    case.families = [Family("MK", rho_al=1000.0, cs_al=900.0) for _ in range(families)]
+    per_fam = []
+    for p in range(families):
+        q = st.copy()
+        if scaled:
+            q[..., 0] *= 2.0 ** p
+            q[..., 5] *= 2.0 ** p
+        per_fam.append(q)
+    case.state = [per_fam]
+    return case
+
+
 def stream_tube(kind="scaling", scale=1.0):
     """The reference's res-threshold cases (test/fast/res-threshold), steady (local steps), res-threshold
     1e-5, MK drops of 10 um and density 1000 at 300 K, extrapolation on every face but the inlet.

@@ -1,12 +1,14 @@
 """The reference's fast cases that exercise the step, on the oracle and on the CUDA path:
 test/fast/inlet-direction (an inlet on a face whose normal points out of the domain injects into it),
 test/fast/res-threshold (a steady run ends when its density residual has fallen by res-threshold
-from the first non-zero one; Mod_Explicit.f90:193-240) and the family leg of test/fast/equiv3d (a
-family in company steps as it does alone)."""
+from the first non-zero one; Mod_Explicit.f90:193-240), the family leg of test/fast/equiv3d (a
+family in company steps as it does alone) and test/fast/populations (copy c of the boundary table
+drives family c)."""
 import numpy as np
 import pytest
 
 from ice_b200 import abi, configs
+from ice_b200.case import SetupError
 from ice_b200.solver import Solver
 
 THR, ITERS = 1e-5, 20000
@@ -102,6 +104,42 @@ def _family_company(lib, precision=0):
             assert np.array_equal(alone.download(b, 0)[2:-2, 2:-2, 2:-2], s.download(b, k)[2:-2, 2:-2, 2:-2]), (k, b)
 
 
+def _populations(lib):
+    """proportional: three copies of the table whose inlet mass fluxes are 1, 2 and 4 times the first,
+    and loadings scaled alike: family p is 2^(p-1) times family 1 in density and number density and
+    equal in velocity and temperature, to 1e-12 of each field, as are its density residual (scaled) and
+    its velocity and temperature residuals; the domain's norms are the roots of the sums of the
+    families' squares. shared: one copy, three families: the families are identical. mismatch: two
+    copies for three families stop the set-up (populations/run.py)."""
+    rel = lambda a, b: float(np.abs(a - b).max()) / max(float(np.abs(b).max()), 1e-300)
+    s = Solver(configs.population_duct(3, 3, True), lib)
+    assert s.step(30).status == 0
+    f = [s.download(0, p)[2:-2, 2:-2, 2:-2] for p in range(3)]
+    assert float(f[0][..., 0].max()) > 1e-3
+    for p in (1, 2):
+        for v in (0, 5):
+            assert rel(f[p][..., v], 2.0 ** p * f[0][..., v]) <= 1e-12
+        for v in (1, 2, 3, 4):
+            assert rel(f[p][..., v], f[0][..., v]) <= 1e-12
+    tot, fam = np.zeros(5), np.zeros(15)
+    assert lib.residual_norm(s.ctx, abi.ptr(tot), abi.ptr(fam)) == abi.OK
+    fam = fam.reshape(3, 5)
+    for p in (1, 2):
+        assert abs(fam[p, 0] / (2.0 ** p * fam[0, 0]) - 1.0) <= 1e-12
+        assert np.all(np.abs(fam[p, 1:] - fam[0, 1:]) <= 1e-12 * np.abs(fam[0, 1:]).max())
+    assert np.all(np.abs(tot - np.sqrt((fam ** 2).sum(0))) <= 1e-12 * np.abs(tot).max())
+    s = Solver(configs.population_duct(1, 3, False), lib)
+    assert s.step(30).status == 0
+    f = [s.download(0, p)[2:-2, 2:-2, 2:-2] for p in range(3)]
+    assert np.array_equal(f[1], f[0]) and np.array_equal(f[2], f[0])
+    with pytest.raises(SetupError, match="copies of the boundary table"):
+        Solver(configs.population_duct(2, 3, False), lib)
+
+
+def test_populations_oracle(orc):
+    _populations(orc)
+
+
 def test_family_company_oracle(orc):
     _family_company(orc)
 
@@ -137,3 +175,8 @@ def test_res_threshold_gpu():
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_FP32FLUX], ids=["fp64", "fp32flux"])
 def test_family_company_gpu(precision):
     _family_company(_gpu(), precision)
+
+
+@pytest.mark.gpu
+def test_populations_gpu():
+    _populations(_gpu())
