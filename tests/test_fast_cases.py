@@ -2,8 +2,9 @@
 test/fast/inlet-direction (an inlet on a face whose normal points out of the domain injects into it),
 test/fast/res-threshold (a steady run ends when its density residual has fallen by res-threshold
 from the first non-zero one; Mod_Explicit.f90:193-240), the family leg of test/fast/equiv3d (a
-family in company steps as it does alone) and test/fast/populations (copy c of the boundary table
-drives family c)."""
+family in company steps as it does alone), test/fast/populations (copy c of the boundary table
+drives family c) and the step-level legs of test/fast/restart-exact (a restart goes on as the
+uninterrupted run would)."""
 import numpy as np
 import pytest
 
@@ -136,6 +137,50 @@ def _populations(lib):
         Solver(configs.population_duct(2, 3, False), lib)
 
 
+def _restart(lib, make, n, total):
+    """Run A: `total` steps in one call. Run B: n steps, its state, time, iteration and residual reference
+    taken into a new context, then the rest. Returns both final reports and states."""
+    a = Solver(make(), lib)
+    oa = a.step(total)
+    b = Solver(make(), lib)
+    ob = b.step(n)
+    mid = b.download_all()
+    ref = np.zeros(1)
+    assert lib.get_res_reference(b.ctx, abi.ptr(ref)) == abi.OK
+    c = Solver(make(), lib, upload=False)
+    c.upload(mid)
+    c.set_time(ob.time, ob.iter, ob.iter)
+    assert lib.set_res_reference(c.ctx, float(ref[0])) == abi.OK
+    oc = c.step(total - n)
+    return oa, oc, a.download_all(), c.download_all()
+
+
+def _restart_checks(lib):
+    """res-threshold: a steady stream that res-threshold stops at iteration 444; restarted at 200, with
+    its residual reference carried over, it stops at 444 too, in the same state. wedge: the one-degree
+    wedge of Axis/AG with its cloud moving along x at 1 m/s (w, P13 and P23 frozen), 40 = 20 + 20 steps.
+    families: the populations duct, copy c driving family c, 30 = 15 + 15 steps. Every state equal bit
+    for bit (restart-exact/run.py)."""
+    oa, oc, ra, rc = _restart(lib, lambda: configs.stream_tube("scaling"), 200, ITERS)
+    assert 200 < oa.iter == oc.iter < ITERS and oa.todo == oc.todo == 3
+
+    def wedge():
+        c = configs.axis_wedge("AG")
+        c.numerics.itermax = 40
+        c.state[0][0][2:-2, 2:-2, 2:-2, 1] = 1.0
+        return c
+    cases = [(ra, rc), _restart(lib, wedge, 20, 40)[2:], _restart(lib, lambda: configs.population_duct(3, 3, True),
+                                                               15, 30)[2:]]
+    for a, c in cases:
+        for per_a, per_c in zip(a, c):
+            for x, y in zip(per_a, per_c):
+                assert np.array_equal(x[2:-2, 2:-2, 2:-2], y[2:-2, 2:-2, 2:-2])
+
+
+def test_restart_oracle(orc):
+    _restart_checks(orc)
+
+
 def test_populations_oracle(orc):
     _populations(orc)
 
@@ -180,3 +225,8 @@ def test_family_company_gpu(precision):
 @pytest.mark.gpu
 def test_populations_gpu():
     _populations(_gpu())
+
+
+@pytest.mark.gpu
+def test_restart_gpu():
+    _restart_checks(_gpu())
