@@ -34,6 +34,10 @@ density, u, v, P11, P22 and det P, in that order). For the anisotropic Sod tube 
 constants of make_case.py (grid, states, drop radius and density), the time threshold and the gates of
 its verify.py.
 
+restart_counters.npz: the counters the reference's binary stored beside its crossing-jets solutions
+(test/Doisneau/{MK,IG,AG,IG-chimera}/reference/part-field.tec, DATASETAUXDATA): CYCLE, ICE_ITERATION,
+ICE_RES_REFERENCE (the first non-zero density residual of the run: the unit of res-threshold), per case.
+
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
 import re
@@ -235,6 +239,18 @@ def ag_riemann(ref):
     print("ag_riemann", {k: v for k, v in out.items() if v.ndim == 0})
 
 
+def restart_counters(ref):
+    out = {}
+    for case in ("MK", "IG", "AG", "IG-chimera"):
+        text = (ref / "test" / "Doisneau" / case / "reference" / "part-field.tec").read_text()
+        key = case.replace("-", "_")
+        for name in ("CYCLE", "ICE_ITERATION", "ICE_RES_REFERENCE"):
+            m = re.search(r'DATASETAUXDATA\s+%s\s*=\s*"([^"]+)"' % name, text)
+            out[f"{key}_{name}"] = np.array(float(m.group(1)))
+    np.savez_compressed(HERE / "restart_counters.npz", **out)
+    print("restart_counters", {k: float(v) for k, v in out.items()})
+
+
 def main(ref):
     ref = Path(ref)
     for cl in ("MK", "IG", "AG"):
@@ -247,6 +263,7 @@ def main(ref):
     correlations(ref)
     evaporation(ref)
     ag_riemann(ref)
+    restart_counters(ref)
 
 
 if __name__ == "__main__":

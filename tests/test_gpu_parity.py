@@ -96,6 +96,24 @@ def test_crossing_jets_matches_reference_output(gpu):
     assert l2 <= 1e-12
 
 
+def test_res_reference_matches_reference_output(gpu):
+    """The first non-zero density residual of the crossing-jets and chimera cases against the value the
+    reference's binary stored with its solutions (the oracle's pin, through the CUDA path)."""
+    from pathlib import Path
+    gold = Path(__file__).resolve().parent / "golden"
+    g = np.load(gold / "restart_counters.npz")
+    chim = dict(np.load(gold / "chimera_IG.npz"))
+    cases = [(configs.crossing_jets(cl, steps=5000), float(g[f"{cl}_ICE_RES_REFERENCE"])) for cl in ("MK", "IG", "AG")]
+    cases.append((configs.doisneau_chimera(chim), float(g["IG_chimera_ICE_RES_REFERENCE"])))
+    for case, want in cases:
+        case.numerics.res_threshold = 1e-10
+        s = Solver(case, gpu)
+        assert s.step(1).status == 0
+        got = np.zeros(1)
+        assert gpu.get_res_reference(s.ctx, abi.ptr(got)) == abi.OK
+        assert abs(got[0] / want - 1.0) <= 1e-12, (got[0], want)
+
+
 def _chimera(steps):
     from pathlib import Path
     g = dict(np.load(Path(__file__).resolve().parent / "golden" / "chimera_IG.npz"))

@@ -28,6 +28,36 @@ ZERO_AT_NEG = ["vanleer", "mc", "superbee", "koren", "umist", "osher", "sweby", 
 ALL_LIM = ZERO_AT_NEG + ["vanalbada", "ospre"]
 
 
+def res_reference_cases():
+    """The four crossing-jets cases with the reference's default res-threshold (1e-10), each with the
+    first non-zero density residual its binary stored (tests/golden/restart_counters.npz)."""
+    g = np.load(GOLDEN / "restart_counters.npz")
+    cases = [(lambda cl=cl: configs.crossing_jets(cl, steps=5000), float(g[f"{cl}_ICE_RES_REFERENCE"]))
+             for cl in ("MK", "IG", "AG")]
+    chim = dict(np.load(GOLDEN / "chimera_IG.npz"))
+    cases.append((lambda: configs.doisneau_chimera(chim), float(g["IG_chimera_ICE_RES_REFERENCE"])))
+    return cases
+
+
+def check_res_reference(lib):
+    """The unit of res-threshold (Mod_Explicit.f90:222-223), the density residual norm of the first
+    step (Mod_Diagnostic.f90:22-83), against the value the reference's binary stored with its
+    solutions (ICE_RES_REFERENCE), to 1e-12 relative: the MK case to the last bit, the others to the
+    contraction of the reference binary's arithmetic (1.6e-13)."""
+    for make, want in res_reference_cases():
+        case = make()
+        case.numerics.res_threshold = 1e-10
+        s = Solver(case, lib)
+        assert s.step(1).status == 0
+        got = np.zeros(1)
+        assert lib.get_res_reference(s.ctx, abi.ptr(got)) == abi.OK
+        assert abs(got[0] / want - 1.0) <= 1e-12, (got[0], want)
+
+
+def test_res_reference_matches_reference_output(orc):
+    check_res_reference(orc)
+
+
 @pytest.mark.slow
 def test_chimera_matches_reference_output(orc):
     g = dict(np.load(GOLDEN / "chimera_IG.npz"))
