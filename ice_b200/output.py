@@ -1,0 +1,172 @@
+"""Solution output and restart in the reference's Tecplot ASCII layout (the part-field.tec files its
+driver writes through its Tecplot library: io/IO_Solution.f90:197-288 writes, 408-445 reads back).
+
+The layout, as the reference's stored solutions hold it: a VARIABLES line (x y z, then every family's
+primitives named <var>_p<family>), one ZONE per block (I, J, K node counts, DATAPACKING=BLOCK, the
+coordinates nodal and the primitives cell-centred, SOLUTIONTIME = the time of a time-accurate run, minus
+the iteration count of a steady one), the node coordinates then the cell values with i fastest, one
+value per line, and after the last zone the counters a restart reads back, as data set auxiliary data:
+CYCLE, ICE_ITERATION, ICE_OUTPUT_NUMBER, ICE_GRID_LEVEL, ICE_LAST_OUTPUT_TIME, ICE_RES_REFERENCE. Every
+value is printed with 17 significant digits, so it reads back as the same double.
+
+write_solution_async overlaps the formatting of a solution with the steps that follow it: the state
+is copied off the device first (the download is the only part the next step waits for), and a host
+thread formats and writes the file while the device steps on.
+"""
+from __future__ import annotations
+
+import re
+from concurrent.futures import Future, ThreadPoolExecutor
+
+import numpy as np
+
+from .case import Case, empty_state
+
+NAMES = {"MK": ["rho", "u", "v", "w", "T", "n"],
+         "IG": ["rho", "u", "v", "w", "P", "T", "n"],
+         "AG": ["rho", "u", "v", "w", "P11", "P12", "P13", "P22", "P23", "P33", "T", "n"]}
+COUNTERS = ("ICE_ITERATION", "ICE_OUTPUT_NUMBER", "ICE_GRID_LEVEL", "ICE_LAST_OUTPUT_TIME", "ICE_RES_REFERENCE")
+
+
+def fortran_e(x: float) -> str:
+    """x as the reference's files print it: a blank or a minus, 0. and 17 significant digits, E and a
+    signed three-digit exponent (0.10000000000000001E+000 for 0.1)."""
+    x = float(x)
+    if x == 0.0:
+        return (" " if np.copysign(1.0, x) > 0 else "-") + "0.00000000000000000E+000"
+    digits = "%.16E" % abs(x)                      # d.ddddddddddddddddE+xx, 17 digits correctly rounded
+    mant = digits[0] + digits[2:18]
+    exp = int(digits[19:]) + 1
+    return ("-" if x < 0 else " ") + "0." + mant + "E" + ("-" if exp < 0 else "+") + "%03d" % abs(exp)
+
+
+def variable_names(case: Case) -> list:
+    return [f"{v}_p{p + 1}" for p, fam in enumerate(case.families) for v in NAMES[fam.closure]]
+
+
+def header_lines(case: Case, b: int, solution_time: float) -> list:
+    """The VARIABLES line (first zone only) and the ZONE line of block b (0-based)."""
+    ni, nj, nk = case.dims[b]
+    nv = len(variable_names(case))
+    zone = (f" ZONE  T = Block{b + 1}, I={ni + 1}, J={nj + 1}, K={nk + 1}, DATAPACKING=BLOCK, "
+            f"VARLOCATION=([1-3]=NODAL,[4-{3 + nv}]=CELLCENTERED), SOLUTIONTIME={fortran_e(solution_time).strip()}")
+    head = [" VARIABLES = x y z" + "".join("   " + n for n in variable_names(case))] if b == 0 else []
+    return head + [zone]
+
+
+def aux_lines(cycle: int, counters: dict) -> list:
+    """The restart counters as data set auxiliary data."""
+    out = [f'DATASETAUXDATA CYCLE = "{int(cycle)}"']
+    out += [f'DATASETAUXDATA {k} = "{fortran_e(counters[k]).strip()}"' for k in COUNTERS]
+    return out
+
+
+def solution_text(case: Case, states, solution_time: float, cycle: int, counters: dict) -> str:
+    """The whole file for the given states (per block, per family, in the layout of upload_state)."""
+    lines = []
+    for b, nodes in enumerate(case.nodes):
+        lines += header_lines(case, b, solution_time)
+        for c in range(3):
+            lines += [fortran_e(v) for v in nodes[..., c].transpose(2, 1, 0).ravel()]
+        for p, fam in enumerate(case.families):
+            cells = np.asarray(states[b][p])[2:-2, 2:-2, 2:-2]
+            for v in range(fam.nc):
+                lines += [fortran_e(x) for x in cells[..., v].ravel()]
+    lines += aux_lines(cycle, counters)
+    return "\n".join(lines) + "\n"
+
+
+def counters_of(solver, out, output_number: int = 0) -> tuple:
+    """SOLUTIONTIME, CYCLE and the counters of a solver after a step report `out` (ICE_LAST_OUTPUT_TIME:
+    the run's time at this output)."""
+    from . import abi
+    ref = np.zeros(1)
+    rc = solver.lib.get_res_reference(solver.ctx, abi.ptr(ref))
+    if rc != 0:
+        raise RuntimeError("get_res_reference failed")
+    steady = not solver.case.numerics.time_accurate
+    time = -float(out.iter) if steady else float(out.time)
+    counters = {"ICE_ITERATION": float(out.iter), "ICE_OUTPUT_NUMBER": float(output_number), "ICE_GRID_LEVEL": 1.0,
+                "ICE_LAST_OUTPUT_TIME": float(out.time), "ICE_RES_REFERENCE": float(ref[0])}
+    return time, int(out.iter), counters
+
+
+def write_solution(path, solver, out, output_number: int = 0):
+    """Download the solver's state and write it with its counters to path."""
+    time, cycle, counters = counters_of(solver, out, output_number)
+    text = solution_text(solver.case, solver.download_all(), time, cycle, counters)
+    with open(path, "w") as f:
+        f.write(text)
+
+
+_POOL = ThreadPoolExecutor(max_workers=1)
+
+
+def write_solution_async(path, solver, out, output_number: int = 0) -> Future:
+    """write_solution with the formatting and the write on a host thread: the state is downloaded now,
+    and the solver may step on as soon as this returns. The future's result is the path."""
+    time, cycle, counters = counters_of(solver, out, output_number)
+    states = solver.download_all()
+    case = solver.case
+
+    def work():
+        text = solution_text(case, states, time, cycle, counters)
+        with open(path, "w") as f:
+            f.write(text)
+        return path
+    return _POOL.submit(work)
+
+
+def read_solution(path) -> dict:
+    """The zones of a solution file: per block (I, J, K), node coordinates (I, J, K, 3) and cell values
+    (nv, K-1, J-1, I-1); SOLUTIONTIME; the auxiliary data as numbers."""
+    text = open(path).read().split("\n")
+    zones = [n for n, l in enumerate(text) if l.lstrip().startswith("ZONE")]
+    aux = {}
+    for l in text:
+        m = re.match(r'DATASETAUXDATA\s+(\S+)\s*=\s*"([^"]*)"', l)
+        if m:
+            aux[m.group(1)] = float(m.group(2))
+    nv = len(text[0].split("=", 1)[1].split()) - 3
+    blocks, time = [], None
+    for z, start in enumerate(zones):
+        hdr = text[start]
+        g = lambda k: int(re.search(r"\b%s=(\d+)" % k, hdr).group(1))
+        I, J, K = g("I"), g("J"), g("K")
+        time = float(re.search(r"SOLUTIONTIME=(\S+)", hdr).group(1))
+        end = zones[z + 1] if z + 1 < len(zones) else len(text)
+        vals = np.array([float(l) for l in text[start + 1:end] if l.strip() and not l.startswith("DATASETAUXDATA")])
+        nn, ncl = I * J * K, (I - 1) * (J - 1) * (K - 1)
+        nodes = np.stack([vals[c * nn:(c + 1) * nn].reshape(K, J, I).transpose(2, 1, 0) for c in range(3)], axis=-1)
+        cells = vals[3 * nn:3 * nn + nv * ncl].reshape(nv, K - 1, J - 1, I - 1)
+        blocks.append(((I, J, K), nodes, cells))
+    return {"blocks": blocks, "time": time, "aux": aux}
+
+
+def states_from_solution(case: Case, sol: dict) -> list:
+    """The per-block, per-family states of upload_state from a solution: the cell values of the file,
+    the ghost cells unset (every step fills both ghost layers before it reads them)."""
+    states = []
+    for b, (_, _, cells) in enumerate(sol["blocks"]):
+        per_fam, v0 = [], 0
+        for fam in case.families:
+            st = empty_state(case.dims[b], fam.nc)
+            st[2:-2, 2:-2, 2:-2, :] = np.moveaxis(cells[v0:v0 + fam.nc], 0, -1)
+            per_fam.append(st)
+            v0 += fam.nc
+        states.append(per_fam)
+    return states
+
+
+def restart(solver, sol: dict):
+    """Put a solution into a fresh solver (built with upload=False): the state, the iteration count
+    and the residual reference of its counters, and for a time-accurate run its time (read_vtk_tec,
+    IO_Solution.f90:408-445)."""
+    from . import abi
+    solver.upload(states_from_solution(solver.case, sol))
+    it = int(sol["aux"]["ICE_ITERATION"])
+    time = sol["time"] if solver.case.numerics.time_accurate else sol["aux"]["ICE_LAST_OUTPUT_TIME"]
+    solver.set_time(time, it, it)
+    rc = solver.lib.set_res_reference(solver.ctx, sol["aux"]["ICE_RES_REFERENCE"])
+    if rc != abi.OK:
+        raise RuntimeError("set_res_reference failed")

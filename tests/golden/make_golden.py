@@ -38,6 +38,11 @@ restart_counters.npz: the counters the reference's binary stored beside its cros
 (test/Doisneau/{MK,IG,AG,IG-chimera}/reference/part-field.tec, DATASETAUXDATA): CYCLE, ICE_ITERATION,
 ICE_RES_REFERENCE (the first non-zero density residual of the run: the unit of res-threshold), per case.
 
+tecplot_sample.npz: the text of the reference's solution files (test/Doisneau/{MK,IG,AG}/reference/
+part-field.tec, written by its Tecplot writer): per case the two header lines, the data set auxiliary
+data lines of the restart counters, and a sample of the value lines (every 97th, and the first 200
+negative ones), as strings.
+
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
 import re
@@ -251,6 +256,20 @@ def restart_counters(ref):
     print("restart_counters", {k: float(v) for k, v in out.items()})
 
 
+def tecplot_sample(ref):
+    out = {}
+    for case in ("MK", "IG", "AG"):
+        lines = (ref / "test" / "Doisneau" / case / "reference" / "part-field.tec").read_text().split("\n")
+        head, body = lines[:2], [l for l in lines[2:] if l and not l.startswith("DATASETAUXDATA")]
+        aux = [l for l in lines if l.startswith("DATASETAUXDATA")]
+        sample = body[::97] + [l for l in body if l.startswith("-")][:200]
+        out[f"{case}_head"] = np.array(head)
+        out[f"{case}_aux"] = np.array(aux)
+        out[f"{case}_values"] = np.array(sample)
+    np.savez_compressed(HERE / "tecplot_sample.npz", **out)
+    print("tecplot_sample", {k: len(v) for k, v in out.items()})
+
+
 def main(ref):
     ref = Path(ref)
     for cl in ("MK", "IG", "AG"):
@@ -264,6 +283,7 @@ def main(ref):
     evaporation(ref)
     ag_riemann(ref)
     restart_counters(ref)
+    tecplot_sample(ref)
 
 
 if __name__ == "__main__":
