@@ -185,6 +185,27 @@ def test_populations_oracle(orc):
     _populations(orc)
 
 
+def test_thread_count_equivalence_oracle(orc):
+    """equiv3d's threads leg (and openmp-equiv): a 12-block, three-family case steps to the same bits on
+    1, 2, 3, 4 and 8 threads. The oracle computes each face flux once and sums a cell's boundary
+    records in face order, as the reference's owner-computes loops do, so no sum depends on the
+    schedule."""
+    runs = []
+    before = orc.set_threads(0)                 # 0 reads the count and changes nothing
+    try:
+        for nt in (1, 2, 3, 4, 8):
+            orc.set_threads(nt)
+            s = Solver(configs.multiblock_tree(nblocks=12, seed=1, lo=6, hi=10, steps=4), orc)
+            assert s.step(4).status == 0
+            runs.append(s.download_all())
+    finally:
+        orc.set_threads(before)
+    for r in runs[1:]:
+        for pa, pb in zip(runs[0], r):
+            for a, b in zip(pa, pb):
+                assert np.array_equal(a[2:-2, 2:-2, 2:-2], b[2:-2, 2:-2, 2:-2])
+
+
 def test_family_company_oracle(orc):
     _family_company(orc)
 
