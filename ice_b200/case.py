@@ -245,6 +245,7 @@ class Numerics:
     itermax: int = 1_000_000_000
     time_threshold: float = 1e30
     res_threshold: float = 0.0
+    sol_diter: int = 0                # a solution every sol_diter iterations (0: at the end only)
 
 
 @dataclass
@@ -401,7 +402,7 @@ class Case:
         P.drag, P.heat, P.blow = abi.DRAG[nm.drag], abi.HEAT[nm.heat], int(nm.blowing)
         P.precision = nm.precision
         P.itermax = nm.itermax
-        P.sol_diter, P.shell_diter, P.res_diter = 0, 0, 0
+        P.sol_diter, P.shell_diter, P.res_diter = nm.sol_diter, 0, 0
         P.time_threshold, P.res_threshold, P.sol_dtime = nm.time_threshold, nm.res_threshold, 1e30
         for p, f in enumerate(self.families):
             P.fam[p] = f.to_c()

@@ -167,6 +167,36 @@ def restart(solver, sol: dict):
     it = int(sol["aux"]["ICE_ITERATION"])
     time = sol["time"] if solver.case.numerics.time_accurate else sol["aux"]["ICE_LAST_OUTPUT_TIME"]
     solver.set_time(time, it, it)
+    solver.last.iter = it                          # the iteration the next output is counted from
     rc = solver.lib.set_res_reference(solver.ctx, sol["aux"]["ICE_RES_REFERENCE"])
     if rc != abi.OK:
         raise RuntimeError("set_res_reference failed")
+
+
+def run(solver, out_dir, chunk: int = 1000) -> list:
+    """The driver's loop (Wrap_Solve.f90, ICE_postprocess): step until the step reports the end of the run
+    (itermax, time-threshold or res-threshold: todo 3), writing part-field.tec in out_dir at every
+    output iteration (sol_diter: todo 2) and at the end, each written on the host thread while the
+    steps go on. Steps are taken in calls of up to `chunk`, cut at the next output iteration and at
+    itermax (a call ends early only on res-threshold); with a time threshold, one step per call, since
+    the step that reaches it is not known ahead. Returns the iterations written, the last at the end
+    of the run."""
+    import os
+    nm = solver.case.numerics
+    path = os.path.join(out_dir, "part-field.tec")
+    written, pending, number = [], None, 0
+    while True:
+        it = solver.last.iter
+        n = 1 if nm.time_threshold < 1e30 else min(chunk, max(nm.itermax - it, 1))
+        if nm.sol_diter > 0:
+            n = min(n, nm.sol_diter - it % nm.sol_diter)
+        out = solver.step(n)
+        if out.todo in (2, 3):
+            if pending is not None:
+                pending.result()
+            pending = write_solution_async(path, solver, out, number)
+            written.append(int(out.iter))
+            number += 1
+        if out.todo == 3:
+            pending.result()
+            return written

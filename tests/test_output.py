@@ -86,6 +86,32 @@ def _async_checks(lib, tmp_path):
     assert sol["aux"]["ICE_ITERATION"] == 5.0 and sol["time"] == t5
 
 
+def _run_checks(lib, tmp_path):
+    """The driver's loop: a 12-iteration run with a solution every 5 writes at 5, 10 and 12, the last
+    file holding the final state; a steady run ends on res-threshold at 444 with its counters in the
+    file."""
+    s = Solver(configs.multiblock_tree(nblocks=3, seed=2, lo=4, hi=6, steps=12), lib)
+    s.case.numerics.sol_diter = 5
+    s.update_params(s.case.params())
+    assert output.run(s, str(tmp_path)) == [5, 10, 12]
+    sol = output.read_solution(tmp_path / "part-field.tec")
+    for per_w, per_g in zip(s.download_all(), output.states_from_solution(s.case, sol)):
+        for x, y in zip(per_w, per_g):
+            assert np.array_equal(x[2:-2, 2:-2, 2:-2], y[2:-2, 2:-2, 2:-2])
+    assert sol["aux"]["ICE_ITERATION"] == 12.0 and sol["aux"]["ICE_OUTPUT_NUMBER"] == 2.0
+    s = Solver(configs.stream_tube("scaling"), lib)
+    written = output.run(s, str(tmp_path))
+    sol = output.read_solution(tmp_path / "part-field.tec")
+    ref = np.zeros(1)
+    assert lib.get_res_reference(s.ctx, abi.ptr(ref)) == abi.OK
+    assert written == [s.last.iter] and 200 < written[0] < 20000
+    assert sol["time"] == -float(written[0]) and sol["aux"]["ICE_RES_REFERENCE"] == ref[0]
+
+
+def test_run_loop_oracle(orc, tmp_path):
+    _run_checks(orc, tmp_path)
+
+
 def test_restart_through_file_oracle(orc, tmp_path):
     _restart_checks(orc, tmp_path)
 
@@ -102,3 +128,8 @@ def test_restart_through_file_gpu(tmp_path):
 @pytest.mark.gpu
 def test_async_output_gpu(tmp_path):
     _async_checks(_gpu(), tmp_path)
+
+
+@pytest.mark.gpu
+def test_run_loop_gpu(tmp_path):
+    _run_checks(_gpu(), tmp_path)
