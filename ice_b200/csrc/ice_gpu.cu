@@ -118,6 +118,8 @@ struct ice_gpu_ctx {
   bool geo32_ok = false;
   bool have_gas = false;
   std::vector<bool> have_block;
+  std::vector<bool> gas_set;     // per block: ice_gpu_set_gas was called
+  int ngas_inlet = 0;            // 401 and 403 records, whose ghosts read the gas
   bool have_records = false;
   bool exchange = false;  // two-way coupling: the step's weighted source is kept for the gas
   int nchim = 0;          // 102 records of the table
@@ -589,6 +591,7 @@ int ice_gpu_create(const ice_gpu_params* P, int32_t nblocks, const int32_t* dims
   c->nb = nblocks;
   c->dims.assign(dims, dims + 3 * nblocks);
   c->have_block.assign(nblocks, false);
+  c->gas_set.assign(nblocks, false);
   long long G = 0, I = 0, R = 0, F0 = 0, F1 = 0, F2 = 0;
   for (int b = 0; b < nblocks; ++b) {
     int ni = dims[3 * b], nj = dims[3 * b + 1], nk = dims[3 * b + 2];
@@ -724,7 +727,8 @@ int ice_gpu_set_gas(ice_gpu_ctx* c, int32_t b1, const double* prim5, const doubl
   const double* rest[4] = {R, gam, k, mu};
   for (int comp = 0; comp < 4; ++comp)
     CK(cudaMemcpy(c->gas.p + (long long)(5 + comp) * c->NI + B.ioff, rest[comp], n * sizeof(double), cudaMemcpyHostToDevice));
-  c->have_gas = true;
+  c->gas_set[b1 - 1] = true;
+  c->have_gas = std::all_of(c->gas_set.begin(), c->gas_set.end(), [](bool x) { return x; });
   return 0;
 }
 
@@ -854,11 +858,13 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
   if (!c) return ICE_GPU_EINVAL;
   if (nrec < 0 || (nrec > 0 && (!ri || !rr))) return fail(c, ICE_GPU_EINVAL, "set_records: bad arguments");
   c->recs.resize(nrec);
+  c->ngas_inlet = 0;
   for (int n = 0; n < nrec; ++n) {
     const int32_t* q = ri + (long long)n * ICE_GPU_REC_INTS;
     const double* x = rr + (long long)n * ICE_GPU_REC_REALS;
     HRec& r = c->recs[n];
     r.b = q[0]; r.i = q[1]; r.j = q[2]; r.k = q[3]; r.f = q[4]; r.type = q[5]; r.p = q[6];
+    if (r.type == 401 || r.type == 403) ++c->ngas_inlet;
     r.bs = q[7]; r.is = q[8]; r.js = q[9]; r.ks = q[10]; r.fs = q[11]; r.partner = q[12]; r.owner = q[13]; r.cf = q[14];
     r.massflux = x[0]; r.velocity = x[1]; r.alpha = x[2]; r.beta = x[3]; r.temperature = x[4]; r.radius = x[5];
     r.gfixed = x[6]; r.normal_dir = x[7];
@@ -1119,7 +1125,12 @@ static int check_ready(ice_gpu_ctx* c) {
   if (!c->have_records) return fail(c, ICE_GPU_ENOTREADY, "no boundary table");
   if (!c->have_chimera)
     return fail(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (ice_gpu_set_chimera)", c->nchim);
-  if (c->P.coupled && !c->have_gas) return fail(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas");
+  // the sources of a coupled run and the ghosts of 401 and 403 inlets read the gas: refused here, before
+  // any launch, where a block has none (the reference refuses an inlet 401 or 403 without a gas at set-up)
+  if (c->P.coupled && !c->have_gas) return fail(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas of every block");
+  if (c->ngas_inlet > 0 && !c->have_gas)
+    return fail(c, ICE_GPU_ENOTREADY, "%d inlet records (401, 403) read the gas, and the run has none (a coupled "
+                "run with ice_gpu_set_gas for every block)", c->ngas_inlet);
   return 0;
 }
 

@@ -1233,6 +1233,18 @@ int orc_step(orc_ctx* c, int nsteps, ice_gpu_step_out* out) {
     int rc = 0;
     if (c->nchim > 0 && !c->have_chim)
         return seterr(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (set_chimera)", c->nchim);
+    /* the sources of a coupled run and the 401 and 403 inlets read the gas of their block: a block
+     * without one is refused before any step (the reference refuses an inlet 401 or 403 without a
+     * gas at set-up) */
+    for (int b = 0; b < c->nb; ++b)
+        if (c->P.coupled && !c->blk[b].gprim)
+            return seterr(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas of every block (block %d has none)", b + 1);
+    for (int n = 0; n < c->nrec; ++n) {
+        const orec* r = &c->bc[n];
+        if ((r->type == 401 || r->type == 403) && !c->blk[r->b - 1].gprim)
+            return seterr(c, ICE_GPU_ENOTREADY, "inlet %d of block %d reads the gas, and the run has no gas there "
+                          "(a coupled run with set_gas)", r->type, r->b);
+    }
     c->res_end = 0;
     for (int s = 0; s < nsteps && !rc && !c->res_end; ++s) rc = explicit_step(c, out);
     if (out) {

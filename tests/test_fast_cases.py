@@ -10,7 +10,7 @@ import pytest
 
 from ice_b200 import abi, configs
 from ice_b200.case import SetupError
-from ice_b200.solver import Solver
+from ice_b200.solver import SolveError, Solver
 
 THR, ITERS = 1e-5, 20000
 
@@ -185,6 +185,27 @@ def test_populations_oracle(orc):
     _populations(orc)
 
 
+def _gas_refusals(lib):
+    """refusals (test/fast/refusals: inlet 401 and 403 without a gas): an inlet that reads the gas in a run
+    without one, and a coupled run whose gas is missing in a block, are refused before any step, with
+    the reason; nothing is launched."""
+    case = configs.inlet_duct("angles")
+    case.gas = []
+    case.numerics.coupled = False
+    s = Solver(case, lib)
+    with pytest.raises(SolveError, match="read.* the gas"):
+        s.step(1)
+    case = configs.multiblock_tree(nblocks=3, seed=2, lo=4, hi=6, steps=2)
+    case.gas = case.gas[:1]
+    s = Solver(case, lib)
+    with pytest.raises(SolveError, match="gas of every block"):
+        s.step(1)
+
+
+def test_gas_refusals_oracle(orc):
+    _gas_refusals(orc)
+
+
 def test_thread_count_equivalence_oracle(orc):
     """equiv3d's threads leg (and openmp-equiv): a 12-block, three-family case steps to the same bits on
     1, 2, 3, 4 and 8 threads. The oracle computes each face flux once and sums a cell's boundary
@@ -251,3 +272,8 @@ def test_populations_gpu():
 @pytest.mark.gpu
 def test_restart_gpu():
     _restart_checks(_gpu())
+
+
+@pytest.mark.gpu
+def test_gas_refusals_gpu():
+    _gas_refusals(_gpu())
