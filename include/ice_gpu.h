@@ -251,7 +251,10 @@ int ice_gpu_get_res_reference(ice_gpu_ctx* ctx, double* ref);
  * step ended on a state the reference stops on (out->status says which). A steady run with
  * res_threshold > 0 takes the residual norm after every step (out->residual) and the call ends at
  * the step whose density residual is at most res_threshold times the run's first non-zero one
- * (out->todo = 3), as the driver's loop ends on TODO = 3. */
+ * (out->todo = 3), as the driver's loop ends on TODO = 3. Returns ICE_GPU_ENOTREADY, before any
+ * launch, when the set-up is incomplete: a block without metrics, no boundary table, chimera records
+ * without donors, or gas missing where it is read (a coupled run, or a 401 or 403 inlet, with a block
+ * that ice_gpu_set_gas has not filled). */
 int ice_gpu_step(ice_gpu_ctx* ctx, int32_t nsteps, ice_gpu_step_out* out);
 
 /* nsteps time steps for a driver that keeps the state on the host. prim_in[(b-1)*nfam + (p-1)]
