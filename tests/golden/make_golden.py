@@ -41,7 +41,7 @@ ICE_RES_REFERENCE (the first non-zero density residual of the run: the unit of r
 tecplot_sample.npz: the text of the reference's solution files (test/Doisneau/{MK,IG,AG}/reference/
 part-field.tec, written by its Tecplot writer): per case the two header lines, the data set auxiliary
 data lines of the restart counters, and a sample of the value lines (every 97th, and the first 200
-negative ones), as strings.
+negative ones), as strings, with their positions among the value lines.
 
 The reference is read here, in this container; the fixtures travel, the reference does not.
 """
@@ -262,10 +262,11 @@ def tecplot_sample(ref):
         lines = (ref / "test" / "Doisneau" / case / "reference" / "part-field.tec").read_text().split("\n")
         head, body = lines[:2], [l for l in lines[2:] if l and not l.startswith("DATASETAUXDATA")]
         aux = [l for l in lines if l.startswith("DATASETAUXDATA")]
-        sample = body[::97] + [l for l in body if l.startswith("-")][:200]
+        idx = list(range(0, len(body), 97)) + [n for n, l in enumerate(body) if l.startswith("-")][:200]
         out[f"{case}_head"] = np.array(head)
         out[f"{case}_aux"] = np.array(aux)
-        out[f"{case}_values"] = np.array(sample)
+        out[f"{case}_values"] = np.array([body[n] for n in idx])
+        out[f"{case}_index"] = np.array(idx)
     np.savez_compressed(HERE / "tecplot_sample.npz", **out)
     print("tecplot_sample", {k: len(v) for k, v in out.items()})
 

@@ -41,6 +41,33 @@ def test_header_and_counters_match_reference_files(closure):
     assert output.aux_lines(int(values["CYCLE"]), values) == aux
 
 
+@pytest.mark.parametrize("closure", ["MK", "IG", "AG"])
+def test_layout_matches_reference_files(closure):
+    """The reference's own crossing-jets fields (tests/golden/crossing_jets_<closure>.npz), written with the
+    case's mesh and the stored counters, give the stored file's lines at the sampled positions: every
+    cell line to the character (the order of variables and cells), every node line to 1e-15 of the unit
+    domain. The reference's mesh file carries y = 0.060000000000000102 at j = 56, where the case's evenly
+    spaced mesh has the double nearest 0.06, so those node lines differ in their last digits."""
+    from ice_b200.case import empty_state
+    case = configs.crossing_jets(closure, steps=1)
+    field = np.load(Path(__file__).resolve().parent / "golden" / f"crossing_jets_{closure}.npz")["field"]
+    st = empty_state(case.dims[0], case.families[0].nc)
+    for v in range(field.shape[0]):
+        st[2, 2:-2, 2:-2, v] = field[v]
+    aux = list(GOLD[f"{closure}_aux"])
+    values = {l.split()[1]: float(l.split('"')[1]) for l in aux}
+    text = output.solution_text(case, [[st]], -5000.0, int(values["CYCLE"]), values).split("\n")
+    assert text[:2] == list(GOLD[f"{closure}_head"])
+    body = text[2:]
+    nn = 3 * int(np.prod([d + 1 for d in case.dims[0]]))
+    for n, line in zip(GOLD[f"{closure}_index"], GOLD[f"{closure}_values"]):
+        if n < nn:
+            assert abs(float(body[n]) - float(line)) <= 1e-15, (n, body[n], line)
+        else:
+            assert body[n] == line, (n, body[n], line)
+    assert text[-7:-1] == aux
+
+
 def _restart_through_file(lib, tmp_path, make, n, total):
     a = Solver(make(), lib)
     oa = a.step(total)
