@@ -119,7 +119,6 @@ struct ice_gpu_ctx {
   bool have_gas = false;
   std::vector<bool> have_block;
   std::vector<bool> gas_set;     // per block: ice_gpu_set_gas was called
-  int ngas_inlet = 0;            // 401 and 403 records, whose ghosts read the gas
   bool have_records = false;
   bool exchange = false;  // two-way coupling: the step's weighted source is kept for the gas
   int nchim = 0;          // 102 records of the table
@@ -858,13 +857,11 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
   if (!c) return ICE_GPU_EINVAL;
   if (nrec < 0 || (nrec > 0 && (!ri || !rr))) return fail(c, ICE_GPU_EINVAL, "set_records: bad arguments");
   c->recs.resize(nrec);
-  c->ngas_inlet = 0;
   for (int n = 0; n < nrec; ++n) {
     const int32_t* q = ri + (long long)n * ICE_GPU_REC_INTS;
     const double* x = rr + (long long)n * ICE_GPU_REC_REALS;
     HRec& r = c->recs[n];
     r.b = q[0]; r.i = q[1]; r.j = q[2]; r.k = q[3]; r.f = q[4]; r.type = q[5]; r.p = q[6];
-    if (r.type == 401 || r.type == 403) ++c->ngas_inlet;
     r.bs = q[7]; r.is = q[8]; r.js = q[9]; r.ks = q[10]; r.fs = q[11]; r.partner = q[12]; r.owner = q[13]; r.cf = q[14];
     r.massflux = x[0]; r.velocity = x[1]; r.alpha = x[2]; r.beta = x[3]; r.temperature = x[4]; r.radius = x[5];
     r.gfixed = x[6]; r.normal_dir = x[7];
@@ -894,7 +891,10 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
           return fail(c, ICE_GPU_EINVAL, "record %d: the two source cells of its ghosts are not inside block %d", n + 1, r.bs);
       if (r.partner < 1 || r.partner > nrec || r.cf < 1) return fail(c, ICE_GPU_EINVAL, "record %d: connection not paired", n + 1);
     }
-    if ((t >= 401 && t <= 403) && t != 402 && !c->P.coupled)
+    // read_bc (io/IO_BC.f90:264-271): a 401 or 403 inlet that injects (non-zero mass flux) reads the gas
+    // speed; a run without a gas phase refuses it while the table is read. A zero-flux inlet mirrors
+    // (ghost_rule, Lib_Ghost.f90:409) and reads no gas.
+    if ((t == 401 || t == 403) && r.massflux != 0.0 && !c->P.coupled)
       return fail(c, ICE_GPU_EINVAL, "record %d: inlet %d takes its speed from the gas, and the run has no gas", n + 1, t);
   }
   for (int p = 0; p < c->P.nfam; ++p) {
@@ -1125,12 +1125,10 @@ static int check_ready(ice_gpu_ctx* c) {
   if (!c->have_records) return fail(c, ICE_GPU_ENOTREADY, "no boundary table");
   if (!c->have_chimera)
     return fail(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (ice_gpu_set_chimera)", c->nchim);
-  // the sources of a coupled run and the ghosts of 401 and 403 inlets read the gas: refused here, before
-  // any launch, where a block has none (the reference refuses an inlet 401 or 403 without a gas at set-up)
+  // the sources of a coupled run and the ghosts of its 401 and 403 inlets read the gas of their block:
+  // refused here, before any launch, where a block has none (an uncoupled run's injecting 401 or 403
+  // inlets were refused by ice_gpu_set_records)
   if (c->P.coupled && !c->have_gas) return fail(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas of every block");
-  if (c->ngas_inlet > 0 && !c->have_gas)
-    return fail(c, ICE_GPU_ENOTREADY, "%d inlet records (401, 403) read the gas, and the run has none (a coupled "
-                "run with ice_gpu_set_gas for every block)", c->ngas_inlet);
   return 0;
 }
 

@@ -350,6 +350,11 @@ int orc_set_records(orc_ctx* c, int nrec, const int* ri, const double* rr) {
         r->temperature = x[4]; r->radius = x[5]; r->gfixed = x[6]; r->normal_dir = x[7] != 0.0;
         if (r->b < 1 || r->b > c->nb || r->p < 1 || r->p > nf || r->f < 1 || r->f > 6)
             return seterr(c, ICE_GPU_EINVAL, "record %d: bad block, family or face", n + 1);
+        /* read_bc, IO_BC.f90:264-271: an injecting 401 or 403 inlet reads the gas speed, and a run
+         * without a gas phase refuses it while the table is read (a zero-flux inlet mirrors) */
+        if ((r->type == 401 || r->type == 403) && r->massflux != 0.0 && !c->P.coupled)
+            return seterr(c, ICE_GPU_EINVAL, "record %d: inlet %d takes its speed from the gas, and the run has no gas",
+                          n + 1, r->type);
     }
     c->nchim = 0;
     for (int n = 0; n < nrec; ++n) { c->nchim += c->bc[n].type == 102; c->bc[n].d0 = 0; c->bc[n].n1 = c->bc[n].n2 = 0; }
@@ -1233,18 +1238,12 @@ int orc_step(orc_ctx* c, int nsteps, ice_gpu_step_out* out) {
     int rc = 0;
     if (c->nchim > 0 && !c->have_chim)
         return seterr(c, ICE_GPU_ENOTREADY, "%d chimera records have no donors (set_chimera)", c->nchim);
-    /* the sources of a coupled run and the 401 and 403 inlets read the gas of their block: a block
-     * without one is refused before any step (the reference refuses an inlet 401 or 403 without a
-     * gas at set-up) */
+    /* the sources of a coupled run and the ghosts of its 401 and 403 inlets read the gas of their
+     * block: a block without one is refused before any step (an uncoupled run's injecting 401 or 403
+     * inlets were refused by set_records) */
     for (int b = 0; b < c->nb; ++b)
         if (c->P.coupled && !c->blk[b].gprim)
             return seterr(c, ICE_GPU_ENOTREADY, "a coupled run needs the gas of every block (block %d has none)", b + 1);
-    for (int n = 0; n < c->nrec; ++n) {
-        const orec* r = &c->bc[n];
-        if ((r->type == 401 || r->type == 403) && !c->blk[r->b - 1].gprim)
-            return seterr(c, ICE_GPU_ENOTREADY, "inlet %d of block %d reads the gas, and the run has no gas there "
-                          "(a coupled run with set_gas)", r->type, r->b);
-    }
     c->res_end = 0;
     for (int s = 0; s < nsteps && !rc && !c->res_end; ++s) rc = explicit_step(c, out);
     if (out) {
