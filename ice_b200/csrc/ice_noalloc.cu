@@ -29,10 +29,33 @@ constexpr int kMaxDevices = 64;
 // the partial sums of every chunk, then the five totals
 __device__ __align__(256) double g_noalloc_scratch[(kMaxChunks + 1) * 5];
 
-// per device: the address of g_noalloc_scratch in that device's memory (the host-side symbol is only
-// a stand-in and must not be given to a kernel)
-double* g_scratch_of[kMaxDevices] = {nullptr};
+// per CUDA context: the address of g_noalloc_scratch in that context's copy of the module (the
+// host-side symbol is only a stand-in and must not be given to a kernel). The key is the current
+// context, not the device ordinal: a caller whose runtime made its own context (cuCtxCreate) holds the
+// module, and so the array, at another address than the device's primary context.
+struct ScratchOf {
+  void* ctx;
+  double* addr;
+};
+ScratchOf g_scratch_of[kMaxDevices] = {};
+int g_nscratch = 0;
 std::mutex g_scratch_mu;
+
+// cuCtxGetCurrent through the runtime's driver entry point (the library links no libcuda)
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrentFn)f;
+    looked = true;
+  }
+  return fn;
+}
 
 __global__ void k_residual_sq_chunks(const double* __restrict__ pn, const double* __restrict__ po, int nc, int it,
                                      int ni, int nj, long long ncell, double* __restrict__ part) {
@@ -103,19 +126,33 @@ extern "C" int ice_gpu_residual_sq_noalloc(const double* prim_new, const double*
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(err, errlen, ICE_GPU_ECUDA, "residual_sq_noalloc: cudaGetDevice: ", cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return fail(err, errlen, ICE_GPU_EINVAL, "residual_sq_noalloc: device ordinal beyond 63");
+  CtxGetCurrentFn cur = ctx_get_current();
+  void* ctx = nullptr;
+  if (!cur || cur(&ctx) != 0)
+    return fail(err, errlen, ICE_GPU_ECUDA, "residual_sq_noalloc: cuCtxGetCurrent is not available from the driver");
+  if (!ctx) {
+    // no context is current yet on this thread: the runtime's first call on the device makes the
+    // device's primary context current
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(err, errlen, ICE_GPU_ECUDA, "residual_sq_noalloc: cudaGetSymbolAddress: ", cudaGetErrorString(e));
+    if (cur(&ctx) != 0 || !ctx) return fail(err, errlen, ICE_GPU_ECUDA, "residual_sq_noalloc: no current CUDA context");
+  }
   double* scratch = nullptr;
   {
-    // set-up, once per device, with that device current (the first call on a device does it)
+    // set-up, once per context, with its device current (the first call in a context does it)
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_of[dev]) {
+    for (int q = 0; q < g_nscratch; ++q)
+      if (g_scratch_of[q].ctx == ctx) scratch = g_scratch_of[q].addr;
+    if (!scratch) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess)
         return fail(err, errlen, ICE_GPU_ECUDA, "residual_sq_noalloc: cudaGetSymbolAddress: ", cudaGetErrorString(e));
-      g_scratch_of[dev] = (double*)p;
+      scratch = (double*)p;
+      if (g_nscratch < kMaxDevices) g_scratch_of[g_nscratch++] = {ctx, scratch};
     }
-    scratch = g_scratch_of[dev];
   }
   cudaStream_t s = (cudaStream_t)stream;
   double* total = scratch + (size_t)kMaxChunks * 5;

@@ -284,9 +284,11 @@ int ice_gpu_residual_norm(ice_gpu_ctx* ctx, double* total, double* fam);
  * ice_gpu_residual_norm for the same states). stream: a cudaStream_t, or NULL.
  * It allocates nothing: its scratch is a static device array of 4096 x 5 partial sums (plus 5),
  * which every GPU that loads the library holds until exit; a block of more than 8,388,608 cells is
- * refused with ICE_GPU_EINVAL. The first call on a device looks the array up on that device (make
- * it before any stream capture). Every call overwrites all the scratch it reads, so nothing carries
- * over between calls; two calls that overlap on the GPU (other streams) share the array and race.
+ * refused with ICE_GPU_EINVAL. The first call in a CUDA context (the device's primary context, or
+ * one the caller's runtime made) looks the array up in that context (make it before any stream
+ * capture). Each call ends by copying the five sums to the host and synchronising its stream. Every
+ * call overwrites all the scratch it reads, so nothing carries over between calls; two calls that
+ * overlap on the GPU (other streams) share the array and race.
  * Errors: a message in err[errlen]. */
 int ice_gpu_residual_sq_noalloc(const double* prim_new, const double* prim_old, int32_t nc,
                                 int32_t t_slot, const int32_t* dims, double* sums, void* stream,
