@@ -206,6 +206,38 @@ class CpuSample:
         return f"{self.what}: {self.case.ncells} cells, 1 step per sample, {secs:.2f} s"
 
 
+def accuracy_leg(lib, steps=100):
+    """Part of the CPU-baseline leg: the oracle steps the 48-block tree of the same recipe at U[8, 16]
+    cells per axis (seed 9) for 100 steps, as config 4 states them, and both device forms step the
+    same case; the per-field relative L1 and L-infinity error of each form against the oracle (every
+    slot of every family, and the particle mass), with the oracle's time on every host core."""
+    import oracle
+    from ice_b200.accuracy import field_errors, worst
+    orc = oracle.load()
+    cores = orc.set_threads(os.cpu_count() or 1)
+    make = lambda prec: configs.multiblock_tree(nblocks=48, lo=8, hi=16, steps=steps, precision=prec)
+    ref_case = make(abi.PREC_FP64)
+    s = Solver(ref_case, orc)
+    t = time.perf_counter()
+    o = s.step(steps)
+    secs = time.perf_counter() - t
+    ref = s.download_all()
+    s.close()
+    out = {"workload": "48-block tree of the same recipe, U[8, 16] cells per axis (seed 9)",
+           "cells": ref_case.ncells, "steps": steps, "oracle_s": round(secs, 1), "oracle_cores": cores,
+           "oracle_status": int(o.status)}
+    for name, prec in (("plain", abi.PREC_FP64), ("chosen", abi.PREC_FP32FLUX)):
+        case = make(prec)
+        g = Solver(case, lib)
+        og = g.step(steps)
+        err = field_errors(case, g.download_all(), ref)
+        g.close()
+        out[name] = {"status": int(og.status), "time_rel_diff": abs(og.time - o.time) / o.time,
+                     "worst_l1_rho_n_mass": worst(err, ("rho", "n", "mass"), "l1"),
+                     "worst_linf": worst(err, None, "linf"), "fields": err}
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: rank 0 alone times the FP64 CPU restatement; other ranks do nothing."""
     if rank != 0:
@@ -438,6 +470,8 @@ def run_ours(args, rank, world, dist):
                     "form": "every step: ice_gpu_step_host (upload of every block and family, one step, download; "
                             "the copies overlap the other families' stages)"}
     if world == 1:
+        if args.workload == "multiblock48" and not args.no_plain:
+            extra["accuracy_vs_oracle"] = accuracy_leg(lib)
         cs = CpuSample(args.workload, os.cpu_count() or 1)
         cs.step()
         n, secs = 0, 0.0

@@ -57,7 +57,7 @@ class Params(C.Structure):
 class StepOut(C.Structure):
     _fields_ = [("dtglobal", C.c_double), ("time", C.c_double), ("iter", C.c_int32), ("todo", C.c_int32),
                 ("status", C.c_int32), ("have_norm", C.c_int32), ("nfloored", C.c_int64),
-                ("residual", C.c_double * 5), ("device_ms", C.c_double)]
+                ("residual", C.c_double * 5), ("device_ms", C.c_double), ("nrealized", C.c_int64)]
 
 
 class SurrogateOpts(C.Structure):

@@ -922,3 +922,25 @@ def _eval_blobs(centres, xc, width):
                      * np.exp(-((y[None, :, None] - c[1]) ** 2) / (2 * width ** 2))
                      * np.exp(-((z[:, None, None] - c[2]) ** 2) / (2 * width ** 2)))
     return out
+
+
+def near_singular_ag_cloud(n=16, steps=20, corr=1.0 - 1e-9, precision=0):
+    """An AG cloud whose velocity covariance is nearly singular: a Gaussian blob of bulk density
+    (1e-3 kg/m3 at the centre over a floor of 1e-6 of it) moving at (3, 2, 1) m/s, every cell with the
+    covariance rho theta M, theta = 0.01 m2/s2 and M = [[1, c, c], [c, 1, c], [c, c, 1]], c = corr
+    (smallest eigenvalue 1 - c). Single precision rounds c to 1, so fluxes evaluated in it can carry a
+    cell's covariance across the positive-definite bound. One n^3 block of 1 mm cells, extrapolation on
+    every face, no gas; MUSCL van Leer, Rusanov, SSP-RK3, CFL 0.5, 60 um droplets."""
+    h = 1e-3
+    nodes = box_nodes(n, n, n, size=(n * h, n * h, n * h))
+    fam = Family("AG", riemann="Rusanov", **droplet_material())
+    num = Numerics(scheme="RK3", cfl=0.5, dt_max=1.0, limiter="vanleer", itermax=steps, precision=precision)
+    xc = (np.arange(n) + 0.5) * h
+    X, Y, Z = np.meshgrid(xc, xc, xc, indexing="ij")
+    c0 = n * h / 2
+    rho = 1e-3 * (1e-6 + np.exp(-((X - c0) ** 2 + (Y - c0) ** 2 + (Z - c0) ** 2) / (0.2 * n * h) ** 2))
+    th = 0.01
+    mass = particle_mass(60e-6, fam.rho_al)
+    prims = [rho, 3.0, 2.0, 1.0, rho * th, rho * th * corr, rho * th * corr, rho * th, rho * th * corr,
+             rho * th, 300.0, rho / mass]
+    return _single_block("near_singular_ag", nodes, fam, num, {f: 400 for f in range(1, 7)}, prims)

@@ -1198,6 +1198,7 @@ static int finish_step(ice_gpu_ctx* c, ice_gpu_step_out* out, float dms) {
     out->dtglobal = h.dtglobal; out->time = h.time; out->iter = h.iter; out->status = (int)h.flags;
     const bool res_stop = !c->P.time_accurate && c->P.res_threshold > 0.0;
     out->nfloored = (int64_t)h.nfloored; out->have_norm = res_stop ? 1 : 0;
+    out->nrealized = (int64_t)h.nrealized;
     bool endsim = h.iter_from_call >= c->P.itermax || c->res_end || h.time >= c->P.time_threshold;
     bool iosim = c->P.sol_diter > 0 && h.iter % c->P.sol_diter == 0;
     out->todo = endsim ? 3 : iosim ? 2 : 1;

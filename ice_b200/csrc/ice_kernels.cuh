@@ -809,6 +809,9 @@ k_stage(Geo G, FamDev F, const Tile* tiles, int TX, int TY, int KZ, int write_r,
         for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + r[v]) * F.rk; cn[v] = co[v] + rr; }
         if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
         cons2prim<CL>(cn, p, F.mat.cp);
+        if constexpr (sizeof(R) == 4) {
+          if (realize<CL>(p)) atomicAdd(&st->nrealized, 1ULL);
+        }
         if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
 #pragma unroll
         for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];

@@ -60,6 +60,7 @@ struct Status {
   int iter;
   int iter_from_call;
   unsigned long long sur_cells, sur_env, sur_res;   // surrogate: cells, envelope and check fallbacks
+  unsigned long long nrealized;  // cells the chosen form's realizability correction changed
 };
 
 __device__ __forceinline__ long long gidx(const DBlock& B, int i, int j, int k) {

@@ -486,6 +486,9 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
         for (int v = 0; v < nc; ++v) { double rr = (cn[v] - co[v] + rd[v]) * F.rk; cn[v] = co[v] + rr; }
         if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
         cons2prim<CL, sizeof(R) == 4>(cn, p, F.mat.cp);
+        if constexpr (sizeof(R) == 4) {
+          if (realize<CL>(p)) atomicAdd(&st->nrealized, 1ULL);
+        }
         if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
 #pragma unroll
         for (int v = 0; v < nc; ++v) F.Uo[(long long)v * G.NG + g] = p[v];

@@ -39,6 +39,7 @@ module ice_gpu
     integer(c_int64_t) :: nfloored
     real(c_double)     :: residual(5)
     real(c_double)     :: device_ms
+    integer(c_int64_t) :: nrealized
   end type ice_gpu_step_out_t
 
   public :: ice_gpu_create, ice_gpu_set_block, ice_gpu_set_records, ice_gpu_set_chimera, ice_gpu_set_gas, &

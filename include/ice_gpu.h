@@ -140,6 +140,9 @@ typedef struct ice_gpu_step_out {
     double  residual[5];                /* residual norm (rho, rho u, rho v, rho w, T)    */
     double  device_ms;                  /* device time of this call's steps (CUDA events on
                                            the context's stream)                          */
+    int64_t nrealized;                  /* cell updates whose AG covariance the FP32-flux
+                                           form's realizability correction made positive
+                                           definite, so far (0 in the plain form)         */
 } ice_gpu_step_out;
 
 /* Training of the evaporation surrogate (ice_gpu_surrogate_train). */

@@ -1249,6 +1249,7 @@ int orc_step(orc_ctx* c, int nsteps, ice_gpu_step_out* out) {
     if (out) {
         out->dtglobal = c->dtglobal; out->time = c->time; out->iter = c->iter;
         out->status = c->status; out->nfloored = c->nfloored; out->device_ms = 0.0;
+        out->nrealized = 0;
     }
     return rc;
 }

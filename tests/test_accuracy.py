@@ -1,0 +1,166 @@
+"""The per-field L1 and L-infinity error of both forms against the FP64 oracle, for every
+configuration: the 1-D IG Riemann problem (config 1, its full 2,000 cells and 1,000 steps), the 2-D
+jets (config 2, MK and IG together), the 3-D evaporating AG cloud (config 3), the 48-block
+three-family tree (config 4) and the same tree with evaporation everywhere and the surrogate source
+(config 5). Configs 2-5 run at reduced sizes here, with their step counts; ICE_ACCURACY_FULL=1 runs
+config 2 at 1024^2, config 3 at 96^3 and the 48-block tree at U[8, 24] cells per axis.
+
+Fields: every primitive slot of every family and the particle mass rho / n (ice_b200.accuracy). The
+plain form must reproduce the oracle: bit for bit on config 1, within 1e-12 relative L-infinity on
+every field elsewhere. The chosen form (FP32 reconstruction, fluxes and sources; FP64 accumulation)
+must hold bulk density, number density and particle mass within 1e-4 relative L1 (config 1 is stated
+for the plain form; its chosen form is reported too).
+
+Config 2's plain form, like the reference, lets rounding-noise velocities of nearly empty cells
+beside the jets set the global step (2e-7 s against 2e-5 s in the chosen form), so the two forms
+reach different times after the same steps. Its chosen form is therefore compared on the oracle's
+own sequence of steps (dt-max set to the oracle's step before each step); the time the chosen form
+reaches on its own steps is reported beside it.
+
+The table of every run is written as JSON to $ICE_ACCURACY_OUT, or to gpurun_out/accuracy.json when
+that folder exists.
+"""
+import ctypes as C
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from ice_b200 import abi, configs
+from ice_b200.accuracy import field_errors, worst
+from ice_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+FULL = os.environ.get("ICE_ACCURACY_FULL") == "1"
+PLAIN_LINF = 1e-12
+CHOSEN_L1 = 1e-4
+KEY_FIELDS = ("rho", "n", "mass")
+ROOT = Path(__file__).resolve().parents[1]
+TABLE = {}
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from ice_b200 import build
+    build.build()
+    return abi.load_gpu()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def write_table():
+    yield
+    out = os.environ.get("ICE_ACCURACY_OUT")
+    if not out and (ROOT / "gpurun_out").is_dir():
+        out = str(ROOT / "gpurun_out" / "accuracy.json")
+    if out and TABLE:
+        Path(out).write_text(json.dumps(TABLE, indent=1))
+
+
+def _with_precision(case, prec):
+    case.numerics.precision = prec
+    return case
+
+
+def _cases():
+    if FULL:
+        return {
+            "1": lambda prec: _with_precision(configs.riemann_1d(n=2000, steps=1000), prec),
+            "2": lambda prec: configs.jets_2d(n=1024, steps=500, precision=prec),
+            "3": lambda prec: configs.cloud_3d(n=96, steps=200, length=0.0096, precision=prec),
+            "4": lambda prec: configs.multiblock_tree(nblocks=48, lo=8, hi=24, steps=100, precision=prec),
+            "5": lambda prec: configs.multiblock_tree(nblocks=48, lo=8, hi=24, steps=100, precision=prec,
+                                                      evaporation_everywhere=True),
+        }
+    return {
+        "1": lambda prec: _with_precision(configs.riemann_1d(n=2000, steps=1000), prec),
+        "2": lambda prec: configs.jets_2d(n=96, steps=500, length=0.1 * 96 / 1024, precision=prec),
+        "3": lambda prec: configs.cloud_3d(n=24, steps=200, length=0.0024, precision=prec),
+        "4": lambda prec: configs.multiblock_tree(nblocks=48, lo=4, hi=8, steps=100, precision=prec),
+        "5": lambda prec: configs.multiblock_tree(nblocks=48, lo=4, hi=8, steps=100, precision=prec,
+                                                  evaporation_everywhere=True),
+    }
+
+
+def _run(lib, case, steps, dts=None, surrogate=False):
+    s = Solver(case, lib)
+    if surrogate:
+        for p, fam in enumerate(case.families):
+            if fam.evap == "none":
+                continue
+            o = abi.SurrogateOpts(nsamples=1 << 18, epochs=20, batch=8192, lr=2e-3, jitter=0.05, seed=17 + p,
+                                  val_frac=0.02)
+            rep = abi.SurrogateReport()
+            assert lib.surrogate_train(s.ctx, p + 1, C.byref(o), C.byref(rep)) == abi.OK, lib.error(s.ctx)
+    seq = []
+    if dts is None:
+        out = s.step(steps)
+        assert out.status == 0, out.status
+    else:
+        params = case.params()
+        for dt in dts:
+            params.dt_max = dt
+            s.update_params(params)
+            out = s.step(1)
+            assert out.status == 0, out.status
+            seq.append(out.dtglobal)
+    res = s.download_all(), float(out.time), seq
+    s.close()
+    return res
+
+
+def _oracle_steps(orc, case, steps):
+    """The oracle one step per call, keeping each step's dt."""
+    s = Solver(case, orc)
+    dts = []
+    for _ in range(steps):
+        out = s.step(1)
+        assert out.status == 0, out.status
+        dts.append(out.dtglobal)
+    res = s.download_all(), float(out.time), dts
+    s.close()
+    return res
+
+
+@pytest.mark.parametrize("cfg", ["1", "2", "3", "4", "5"])
+def test_fields_against_the_oracle(gpu, orc, cfg):
+    make = _cases()[cfg]
+    ref_case = make(abi.PREC_FP64)
+    steps = ref_case.numerics.itermax
+    before = orc.set_threads(os.cpu_count() or 1)
+    try:
+        ref, t_ref, dts = _oracle_steps(orc, ref_case, steps)
+    finally:
+        orc.set_threads(before)
+    row = {"cells": ref_case.ncells, "steps": steps, "families": [f.closure for f in ref_case.families],
+           "time_oracle": t_ref}
+
+    plain_case = make(abi.PREC_FP64)
+    plain, t_plain, _ = _run(gpu, plain_case, steps)
+    e_plain = field_errors(ref_case, plain, ref)
+    row["plain"] = e_plain
+    row["time_plain"] = t_plain
+    if cfg == "1":
+        for a, b in zip(plain, ref):
+            for pa, pb in zip(a, b):
+                assert np.array_equal(pa[2:-2, 2:-2, 2:-2], pb[2:-2, 2:-2, 2:-2])
+    assert t_plain == t_ref
+    assert worst(e_plain, norm="linf") <= PLAIN_LINF, e_plain
+
+    chosen_case = make(abi.PREC_FP32FLUX)
+    if cfg == "2":
+        own, t_own, _ = _run(gpu, make(abi.PREC_FP32FLUX), steps)
+        row["time_chosen_own_steps"] = t_own
+        chosen, t_chosen, seq = _run(gpu, chosen_case, steps, dts=dts)
+        row["chosen_on_oracle_steps"] = bool(seq == dts)
+        assert seq == dts
+    else:
+        chosen, t_chosen, _ = _run(gpu, chosen_case, steps, surrogate=cfg == "5")
+    row["time_chosen"] = t_chosen
+    e_chosen = field_errors(ref_case, chosen, ref)
+    row["chosen"] = e_chosen
+    TABLE[cfg] = row
+    assert abs(t_chosen - t_ref) <= 1e-3 * t_ref
+    assert worst(e_chosen, KEY_FIELDS, "l1") <= CHOSEN_L1, e_chosen
