@@ -49,7 +49,7 @@ class Params(C.Structure):
                 ("irs", C.c_int32), ("irs_beta", C.c_double),
                 ("coupled", C.c_int32), ("drag", C.c_int32), ("heat", C.c_int32), ("blow", C.c_int32),
                 ("precision", C.c_int32), ("itermax", C.c_int32), ("sol_diter", C.c_int32),
-                ("shell_diter", C.c_int32), ("res_diter", C.c_int32), ("pad0", C.c_int32),
+                ("shell_diter", C.c_int32), ("res_diter", C.c_int32), ("no_realize", C.c_int32),
                 ("time_threshold", C.c_double), ("res_threshold", C.c_double), ("sol_dtime", C.c_double),
                 ("fam", Family * MAX_FAMILIES)]
 

@@ -242,6 +242,7 @@ class Numerics:
     heat: str = "Ranz-Marshall"
     blowing: bool = False
     precision: int = abi.PREC_FP64
+    realize: bool = True              # the FP32-flux form's realizability correction of AG states
     itermax: int = 1_000_000_000
     time_threshold: float = 1e30
     res_threshold: float = 0.0
@@ -401,6 +402,7 @@ class Case:
         P.coupled = int(nm.coupled)
         P.drag, P.heat, P.blow = abi.DRAG[nm.drag], abi.HEAT[nm.heat], int(nm.blowing)
         P.precision = nm.precision
+        P.no_realize = 0 if nm.realize else 1
         P.itermax = nm.itermax
         P.sol_diter, P.shell_diter, P.res_diter = nm.sol_diter, 0, 0
         P.time_threshold, P.res_threshold, P.sol_dtime = nm.time_threshold, nm.res_threshold, 1e30

@@ -82,8 +82,9 @@ struct FamHost {
   bool ghost_split = false;                  // the ghost layers in two launches (upload_recs)
   DevBuf<int> bfirst, blist, own;
   DevBuf<CUtensorMap> maps[3];               // per state buffer, per block: the staged kernel's TMA maps
-  DevBuf<Tile> tiles3;                       // the staged kernel's tiles (the tile shape is the closure's)
+  DevBuf<Tile> tiles3;                       // the staged kernel's tiles
   int ntile3 = 0;
+  std::vector<Tile> shape3;                  // per block: the staged kernel's tile shape (w, h, bx, by)
   // the evaporation surrogate (FP32-flux form): the network's BF16 image, its standardisation and
   // envelope, its FP32 parameters; on = the stage's source comes from the surrogate source kernel
   DevBuf<unsigned char> mlp_img;
@@ -223,6 +224,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   memset(&F, 0, sizeof F);
   F.closure = H.closure; F.riemann = H.riemann; F.nc = H.nc;
   F.limiter = c->P.limiter; F.sd = c->P.shock_detector; F.coupled = c->P.coupled;
+  F.realize = c->P.precision == ICE_PREC_FP32FLUX && !c->P.no_realize;
   F.drag = c->P.drag; F.heat = c->P.heat; F.blow = c->P.blow;
   F.frozen_mask = 0;
   for (int q = 0; q < pf.nfrozen; ++q) F.frozen_mask |= 1u << (pf.frozen[q] - 1);
@@ -424,12 +426,56 @@ static void tile_shape(int ndir, int& TX, int& TY, int& KZ) {
   }
 }
 
-// The chunk height of the staged kernel's tiles for one closure: of a few candidates up to ST_KZ
+// The staged kernel's limits for a closure (Shape<CL> of ice_stage3.cuh).
+static void shape_limits(int closure, int& NT, int& MW, int& MH, int& MB, int& FX, int& FY) {
+  if (closure == ICE_CLOSURE_AG) {
+    NT = Shape<AG>::NT; MW = Shape<AG>::MAXW; MH = Shape<AG>::MAXH; MB = Shape<AG>::MAXBOX;
+    FX = Shape<AG>::FX; FY = Shape<AG>::FY;
+  } else {
+    NT = Shape<MK>::NT; MW = Shape<MK>::MAXW; MH = Shape<MK>::MAXH; MB = Shape<MK>::MAXBOX;
+    FX = Shape<MK>::FX; FY = Shape<MK>::FY;
+  }
+}
+
+// The staged kernel's tile shape of a block of ni x nj columns: of the shapes W x H that fit the
+// closure's limits (W H <= NT threads, the staged box, the face buffers), the one whose tiles, cut
+// evenly from the block (ceil(ni / W) tiles of ceil(ni / nx) columns, likewise rows), take the fewest
+// passes of the CTA per plane over the whole block: the face tasks (x and y faces below the owned
+// cells, the faces above the last column and row) dealt out to the NT threads, then the z face and
+// the update; among equals, the fewest tiles. Returns w, h (the even cut) and the box.
+static Tile tile_shape3(int ni, int nj, int closure) {
+  int NT, MW, MH, MB, FX, FY;
+  shape_limits(closure, NT, MW, MH, MB, FX, FY);
+  (void)MW;
+  Tile best{};
+  long long best_cost = -1, best_tiles = 0;
+  const bool ax = ni >= 2, ay = nj >= 2;
+  const int wmax = ax ? std::min(ni, NT) : 1;
+  for (int W = 1; W <= wmax; ++W) {
+    if (st_box_x(W) > 256) break;                 // a TMA box is at most 256 elements along each axis
+    const int hmax = std::min(std::min(nj, MH), NT / W);
+    for (int H = 1; H <= hmax; ++H) {
+      if (st_box_x(W) * (H + 4) > MB || H * (W + 1) > FX || (H + 1) * W > FY) break;
+      const int nx = (ni + W - 1) / W, ny = (nj + H - 1) / H;
+      const int w = (ni + nx - 1) / nx, h = (nj + ny - 1) / ny;
+      const int tasks = (ax ? w * h + h : 0) + (ay ? w * h + w : 0);
+      const long long tiles = (long long)nx * ny;
+      const long long cost = tiles * ((tasks + NT - 1) / NT + 2);
+      if (best_cost < 0 || cost < best_cost || (cost == best_cost && tiles < best_tiles)) {
+        best_cost = cost; best_tiles = tiles;
+        best = Tile{0, 0, 0, 0, 0, (short)w, (short)h, (short)st_box_x(w), (short)(h + 4)};
+      }
+    }
+  }
+  return best;
+}
+
+// The chunk height of the staged kernel's tiles for one family: of a few candidates up to ST_KZ
 // planes, the one whose tiles, handed longest first to the least-loaded of the GPU's resident CTA
 // slots (as the block scheduler hands them out), finish soonest; a tile costs its planes plus the
 // three its prologue loads. Small grids get shorter chunks and more tiles, so that the last wave is
 // not left half empty; large ones keep ST_KZ (a change must gain more than 1 %).
-static int choose_kz(const ice_gpu_ctx* c, int closure, int slots) {
+static int choose_kz(const ice_gpu_ctx* c, const FamHost& H, int slots) {
   static const int cand[] = {ST_KZ, 28, 24, 20, 16, 12, 8};
   int best = ST_KZ;
   double best_t = 0.0;
@@ -437,8 +483,8 @@ static int choose_kz(const ice_gpu_ctx* c, int closure, int slots) {
     std::vector<int> cost;
     for (int b = 0; b < c->nb; ++b) {
       int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
-      int sx = ni >= 2 ? ST_TX - 1 : 1, sy = nj >= 2 ? st_ty(closure) - 1 : 1;
-      long long ncol = (long long)((ni + sx - 1) / sx) * ((nj + sy - 1) / sy);
+      const Tile& sp = H.shape3[b];
+      long long ncol = (long long)((ni + sp.w - 1) / sp.w) * ((nj + sp.h - 1) / sp.h);
       int nch = (nk + kz - 1) / kz, base = nk / nch, extra = nk % nch;
       for (int ch = 0; ch < nch; ++ch)
         for (long long q = 0; q < ncol; ++q) cost.push_back(base + (ch < extra ? 1 : 0) + 3);
@@ -472,8 +518,8 @@ static int build_tiles(ice_gpu_ctx* c) {
     CK(c->tiles.alloc(t.size()));
     CK(cudaMemcpy(c->tiles.p, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
   } else {
-    // the staged kernel: column tiles of (ST_TX - 1) x (TY - 1) cells (TY of the family's closure),
-    // each block's height cut into equal chunks of at most kz planes (choose_kz); the longest first
+    // the staged kernel: column tiles of each block's shape (tile_shape3), each block's height cut
+    // into equal chunks of at most kz planes (choose_kz); the longest first
     c->staged = true;
     int nsm = 148;
     {
@@ -485,16 +531,20 @@ static int build_tiles(ice_gpu_ctx* c) {
     for (int p = 0; p < c->P.nfam; ++p) {
       FamHost& H = c->fam[p];
       t.clear();
-      const int kz = choose_kz(c, H.closure, slots);
+      H.shape3.resize(c->nb);
+      for (int b = 0; b < c->nb; ++b) H.shape3[b] = tile_shape3(c->dims[3 * b], c->dims[3 * b + 1], H.closure);
+      const int kz = choose_kz(c, H, slots);
       for (int b = 0; b < c->nb; ++b) {
         int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
-        int sx = ni >= 2 ? ST_TX - 1 : 1, sy = nj >= 2 ? st_ty(H.closure) - 1 : 1;
+        const Tile& sp = H.shape3[b];
         int nch = (nk + kz - 1) / kz, base = nk / nch, extra = nk % nch;
         for (int ch = 0, k = 0; ch < nch; ++ch) {
-          int h = base + (ch < extra ? 1 : 0);
-          for (int j = 0; j < nj; j += sy)
-            for (int i = 0; i < ni; i += sx) t.push_back(Tile{b, i, j, k, h});
-          k += h;
+          int hz = base + (ch < extra ? 1 : 0);
+          for (int j = 0; j < nj; j += sp.h)
+            for (int i = 0; i < ni; i += sp.w)
+              t.push_back(Tile{b, i, j, k, hz, (short)std::min((int)sp.w, ni - i), (short)std::min((int)sp.h, nj - j),
+                               sp.bx, sp.by});
+          k += hz;
         }
       }
       std::stable_sort(t.begin(), t.end(), [](const Tile& x, const Tile& y) { return x.nkz > y.nkz; });
@@ -522,7 +572,7 @@ static int build_tiles(ice_gpu_ctx* c) {
 
 // The staged stage kernel's TMA maps: per family, state buffer and block, a 4-D view (x, y, z,
 // variable) of the block's ghost-cell pool, strides row px, plane pxy and variable NG (all multiples
-// of 16 bytes by the padding of the layout), box ST_BX x ST_BY x 1 x nc.
+// of 16 bytes by the padding of the layout), box bx x by x 1 x nc of the block's tile shape.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -551,7 +601,7 @@ static int build_maps(ice_gpu_ctx* c) {
         const DBlock& B = c->hblk[b];
         cuuint64_t dims[4] = {(cuuint64_t)B.px, (cuuint64_t)(B.nj + 4), (cuuint64_t)(B.nk + 4), (cuuint64_t)H.nc};
         cuuint64_t strides[3] = {(cuuint64_t)B.px * 8, (cuuint64_t)B.pxy * 8, (cuuint64_t)c->NG * 8};
-        cuuint32_t box[4] = {(cuuint32_t)ST_BX, (cuuint32_t)(st_ty(H.closure) + 3), 1, (cuuint32_t)H.nc};
+        cuuint32_t box[4] = {(cuuint32_t)H.shape3[b].bx, (cuuint32_t)H.shape3[b].by, 1, (cuuint32_t)H.nc};
         cuuint32_t es[4] = {1, 1, 1, 1};
         CUresult r = enc(&h[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)(H.S[buf].p + B.goff), dims, strides, box,
                          es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

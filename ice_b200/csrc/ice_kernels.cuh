@@ -810,7 +810,7 @@ k_stage(Geo G, FamDev F, const Tile* tiles, int TX, int TY, int KZ, int write_r,
         if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
         cons2prim<CL>(cn, p, F.mat.cp);
         if constexpr (sizeof(R) == 4) {
-          if (realize<CL>(p)) atomicAdd(&st->nrealized, 1ULL);
+          if (F.realize && realize<CL>(p)) atomicAdd(&st->nrealized, 1ULL);
         }
         if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
 #pragma unroll

@@ -110,6 +110,7 @@ struct FamDev {              // what the kernels of one family read
   double rk;
   int write_tau;
   int src_ready;             // S holds this stage's source already (its own kernel or the surrogate's ran)
+  int realize;               // the FP32-flux form's realizability correction is on
 };
 
 // bound_empty_dt's reductions over one family's cells, as the bits of non-negative doubles (which
@@ -120,8 +121,10 @@ struct EmptyScan {
   unsigned int filled, pad;
 };
 
-struct Tile { int b, i0, j0, k0, nkz; };
-struct MlpNorm;   // a column tile of a block and its chunk of nkz planes
+// A column tile of a block and its chunk of nkz planes. The staged stage kernel's tiles also carry
+// their owned columns and rows (w, h) and the staged box of their block (bx, by: the TMA box's x and y).
+struct Tile { int b, i0, j0, k0, nkz; short w, h, bx, by; };
+struct MlpNorm;
 struct NormChunk { int b; long long q0, q1; };
 
 // Everything one family's stage needs, for the launcher of its closure's translation unit.

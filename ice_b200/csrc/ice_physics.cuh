@@ -186,21 +186,29 @@ template <int CL, bool FAST = false> __device__ __forceinline__ void cons2prim(c
   }
 }
 
-// The chosen form's realizability correction of an AG state (FP64, after cons -> prim and its
-// floors, which keep the density and the diagonal of the covariance positive). The covariance P must
-// stay positive definite, and single-precision fluxes can carry a nearly singular P across that
-// bound. With D the diagonal of P, the correlation C = D^-1/2 P D^-1/2 = I + O has a unit diagonal,
-// and scaling every off-diagonal of P by s scales O by s: the eigenvalues of C become 1 + s mu_i. When
-// the smallest eigenvalue mu of O (the trace-free 3 x 3 case of the closed-form symmetric
-// eigenvalues, 2 q cos(theta + 2 pi / 3)) is below -(1 - kRealizeMargin), the off-diagonals scale by
+// The chosen form's realizability correction of an occupied AG cell (FP64, after cons -> prim and
+// its floors, which keep the density and the diagonal of the covariance positive). The covariance P
+// of a cell whose density is above rho_empty must stay positive definite, and single-precision fluxes
+// can carry a nearly singular P across that bound. Sylvester's test (P11 > 0 by the floors, then the
+// 2 x 2 leading minor and the determinant) passes for a positive definite P at the cost of a few
+// products. Otherwise, with D the diagonal of P, the correlation C = D^-1/2 P D^-1/2 = I + O has a unit
+// diagonal, and scaling every off-diagonal of P by s scales O by s: the eigenvalues of C become
+// 1 + s mu_i. With mu the smallest eigenvalue of O (the trace-free 3 x 3 case of the closed-form
+// symmetric eigenvalues, 2 q cos(theta + 2 pi / 3)), the off-diagonals scale by
 // s = (1 - kRealizeMargin) / -mu, so that the smallest eigenvalue of C is kRealizeMargin. The diagonal,
-// hence the trace and the energy, is kept. Returns true when it changed the state. The plain form
-// never calls it: the reference applies its floors only (Lib_Model_AG.f90:81-90).
+// hence the trace and the energy, is kept. Cells at or below rho_empty keep the reference's caps
+// (their dispersion bounded by theta_cap in cons2prim) and are left alone. Returns true when it
+// changed the state. The plain form never calls it: the reference applies its floors only
+// (Lib_Model_AG.f90:81-90).
 constexpr double kRealizeMargin = 1e-6;
 template <int CL> __device__ __forceinline__ bool realize(double* p) {
   if constexpr (CL != AG) {
     return false;
   } else {
+    if (!(p[0] > kRhoEmpty)) return false;
+    const double m2 = p[4]*p[7] - p[5]*p[5];
+    const double det = p[4]*(p[7]*p[9] - p[8]*p[8]) - p[5]*(p[5]*p[9] - p[8]*p[6]) + p[6]*(p[5]*p[8] - p[7]*p[6]);
+    if (m2 > 0.0 && det > 0.0) return false;
     const double c12 = p[5] / sqrt(p[4]*p[7]), c13 = p[6] / sqrt(p[4]*p[9]), c23 = p[8] / sqrt(p[7]*p[9]);
     const double q2 = (c12*c12 + c13*c13 + c23*c23) / 3.0;
     if (!(q2 > 0.0)) return false;

@@ -3,17 +3,20 @@
 // gathered per cell in the reference's order, the cell source, R = (R/vol + S) dt and the RK stage
 // fused in one launch per family and stage.
 //
-// One CTA of ST_TX x ST_TY threads owns a tile of (ST_TX - 1) x (ST_TY - 1) cells of one block and
-// marches up a chunk of planes. Each plane of the family's state U_{k-1} (every variable, two halo
-// cells below and one above the tile in x and y) arrives by one 4-D TMA load (x, y, z, variable) into
-// an FP64 staging buffer, issued one plane ahead; the CTA converts it into a ring of three planes of
-// the reconstruction type R (float in the FP32-flux form, double in the plain form). On each plane:
+// One CTA of NT threads owns a tile of w x h cells of one block (w h <= NT; the host picks each
+// block's tile shape so that its tiles cut the block evenly, see tile_shape3 in ice_gpu.cu) and
+// marches up a chunk of planes. Thread t < w h owns the cell (t % w, t / w) of the tile. Each plane of
+// the family's state U_{k-1} (every variable, two halo cells on either side in x and y) arrives by one
+// 4-D TMA load (x, y, z, variable) into an FP64 staging buffer, issued one plane ahead; the CTA
+// converts it into a ring of three planes of the reconstruction type R (float in the FP32-flux form,
+// double in the plain form). On each plane:
 //  - z: the limited slope of the cell above (the slope the reference's state_reconstruction computes
 //    for both faces of a cell, Lib_Reconstruction.f90:17-78) from planes k, k+1, k+2, kept in
 //    registers, and the z face above the cell from the two cells' slopes: the same operations on the
 //    same operands as the reference's per-face reconstruction, so the plain form keeps its bits;
-//  - x and y: the face below the thread's cell, reconstructed from the staged plane (face_flux,
-//    Mod_Fluxes.f90:599-685);
+//  - x and y: each thread the face below its own cell, then the w + h faces above the tile's last
+//    column and last row as a short list of extra tasks (face_flux, Mod_Fluxes.f90:599-685), every
+//    interior face of the tile once;
 //  - each owned cell adds its boundary-record fluxes, then its two faces per direction in the
 //    odd-then-even order of tile_sweep (Mod_Fluxes.f90:470-506), evaluates its source
 //    (Mod_Sources.f90:465-622), forms R = (R/vol + S) dt (Lib_Residual.f90:147-156) and applies the
@@ -24,31 +27,32 @@
 
 namespace ice {
 
-// The tile of a closure: ST_TX x TY threads, (ST_TX - 1) x (TY - 1) owned cells. AG's twelve
-// variables take 12 rows, so that two CTAs fit an SM with 168 registers per thread; MK and IG take 15.
-constexpr int ST_TX = 16;
-constexpr int ST_BX = ST_TX + 4;                // staged columns: 2 below, 1 above, 1 for the even x start
 constexpr int ST_KZ = 32;                       // planes per tile chunk at most
-__host__ __device__ constexpr int st_ty(int closure) { return closure == ICE_CLOSURE_AG ? 12 : 15; }
 
+// The tile limits of a closure: NT threads, so w h <= NT owned cells; at most MAXW owned columns and
+// MAXH owned rows; a staged plane of at most MAXBOX positions per variable (bx by, bx = w + 5 rounded
+// up to even: two halo columns on either side and one for the even x start of the TMA box; by = h + 4).
+// AG's twelve variables take 192 threads, so that two CTAs fit an SM; MK and IG take 256.
 template <int CL> struct Shape {
-  static constexpr int TY = st_ty(CL);
-  static constexpr int NT = ST_TX * TY;         // threads
-  static constexpr int BY = TY + 3;             // staged rows: 2 below, 1 above
-  static constexpr int P = ST_BX * BY;          // positions of one variable of one staged plane
+  static constexpr int NT = CL == AG ? 192 : 256;
+  static constexpr int MAXW = CL == AG ? 32 : 64;
+  static constexpr int MAXH = CL == AG ? 24 : 64;
+  static constexpr int MAXBOX = CL == AG ? 360 : 560;
+  static constexpr int FX = NT + MAXH;          // x-face slots: h (w + 1)
+  static constexpr int FY = NT + MAXW;          // y-face slots: (h + 1) w
 };
+__host__ __device__ constexpr int st_box_x(int w) { return (w + 6) & ~1; }
 
 __host__ __device__ constexpr size_t st_align(size_t n) { return (n + 127) & ~(size_t)127; }
 
 template <int CL, typename R> struct StageSmem {
-  static constexpr int nc = NC<CL>::v, P = Shape<CL>::P, NT = Shape<CL>::NT;
-  static constexpr size_t stg = 0;                                          // double [nc][P]
+  static constexpr int nc = NC<CL>::v, P = Shape<CL>::MAXBOX;
+  static constexpr size_t stg = 0;                                          // double [nc][bx by]
   static constexpr size_t ring = st_align(stg + sizeof(double) * nc * P);  // R [3][nc][P]
-  static constexpr size_t fx = st_align(ring + sizeof(R) * 3 * nc * P);    // R [nc][NT]
-  static constexpr size_t fy = st_align(fx + sizeof(R) * nc * NT);         // R [nc][NT]
-  static constexpr int NB = (ST_TX + 1) * (Shape<CL>::TY + 1);              // sensor positions of a plane
-  static constexpr size_t bt = st_align(fy + sizeof(R) * nc * NT);         // R [2][NB]: beta of planes k, k+1
-  static constexpr size_t bar = st_align(bt + sizeof(R) * 2 * NB);         // mbarrier
+  static constexpr size_t fx = st_align(ring + sizeof(R) * 3 * nc * P);    // R [nc][FX]
+  static constexpr size_t fy = st_align(fx + sizeof(R) * nc * Shape<CL>::FX);   // R [nc][FY]
+  static constexpr size_t bt = st_align(fy + sizeof(R) * nc * Shape<CL>::FY);   // R [2][P]: beta of planes k, k+1
+  static constexpr size_t bar = st_align(bt + sizeof(R) * 2 * P);          // mbarrier
   static constexpr size_t bytes = bar + 16 + 128;   // + the alignment of the base to 128 bytes
 };
 
@@ -109,14 +113,14 @@ __device__ __forceinline__ bool states_from_slopes(const QL& ql, const R* sl, R 
   return false;
 }
 
-template <typename S, int NP> struct SmemStencil {     // q(s, v): stencil cell s of a staged plane
-  const S* P; int base, st;
-  __device__ __forceinline__ S operator()(int s, int v) const { return P[v * NP + base + s * st]; }
+template <typename S> struct SmemStencil {     // q(s, v): stencil cell s of a staged plane, np positions a variable
+  const S* P; int base, st, np;
+  __device__ __forceinline__ S operator()(int s, int v) const { return P[v * np + base + s * st]; }
 };
 
-template <typename S, int NP> struct SmemCell {        // c[v]: one cell of a staged plane
-  const S* P; int pos;
-  __device__ __forceinline__ S operator[](int v) const { return P[v * NP + pos]; }
+template <typename S> struct SmemCell {        // c[v]: one cell of a staged plane
+  const S* P; int pos, np;
+  __device__ __forceinline__ S operator[](int v) const { return P[v * np + pos]; }
 };
 
 // One interior face along d (0: x, 1: y) between the 0-based cells (i,j,k) and its upper neighbour,
@@ -124,7 +128,8 @@ template <typename S, int NP> struct SmemCell {        // c[v]: one cell of a st
 // two cells' Jameson weights: face_flux + compute_flux_ (Mod_Fluxes.f90:599-685).
 template <int CL, int RS, int LIM, typename R>
 __device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, const DBlock& B, int d,
-                                                 int i, int j, int k, const R* P, int base, int st, R bf, R* flux) {
+                                                 int i, int j, int k, const R* P, int np, int base, int st, R bf,
+                                                 R* flux) {
   constexpr int nc = NC<CL>::v;
   const int c = d == 0 ? i : j;
   const int n = d == 0 ? B.ni : B.nj;
@@ -147,7 +152,7 @@ __device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, 
   R dl0 = (R)0.5*(l0 + l1), dl1 = (R)0.5*(l1 + l2), dl2 = (R)0.5*(l2 + l3);
   R dll = (R)0.5*l1, dlr = (R)0.5*l2;
   R pl[nc], pr[nc], fl[nc];
-  SmemStencil<R, Shape<CL>::P> q{P, base, st};
+  SmemStencil<R> q{P, base, st, np};
   const bool bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bf);
   const long long fi = fidx(B, d, i, j, k, c + 1);
   R nrm[3], area;
@@ -164,7 +169,8 @@ __global__ void __launch_bounds__(Shape<CL>::NT, (sizeof(R) == 4) ? 2 : 1)
 k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __restrict__ tiles, int write_r,
          Status* st) {
   constexpr int nc = NC<CL>::v;
-  constexpr int ST_TY = Shape<CL>::TY, ST_NT = Shape<CL>::NT, ST_P = Shape<CL>::P;
+  constexpr int NT = Shape<CL>::NT, RSLOT = nc * Shape<CL>::MAXBOX;
+  constexpr int FX = Shape<CL>::FX, FY = Shape<CL>::FY;
   using L = StageSmem<CL, R>;
   extern __shared__ __align__(128) unsigned char smdyn[];
   // the TMA destination must sit on a 128-byte boundary: align the base explicitly
@@ -180,15 +186,17 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   const DBlock B = G.blk[t.b];
   const CUtensorMap* map = maps + t.b;
   const int tid = threadIdx.x;
-  const int tx = tid % ST_TX, ty = tid / ST_TX;
-  const int i = t.i0 + tx, j = t.j0 + ty;
+  const int w = t.w, h = t.h, bx = t.bx, np = t.bx * t.by;   // owned columns and rows; staged row and plane
   const bool ax = B.ni >= 2, ay = B.nj >= 2, az = B.nk >= 2;
-  const bool col = i < B.ni && j < B.nj;
-  const bool owner = col && (ax ? tx < ST_TX - 1 : tx == 0) && (ay ? ty < ST_TY - 1 : ty == 0);
+  const bool own = tid < w * h;
+  const int tx = own ? tid % w : 0, ty = own ? tid / w : 0;
+  const int i = t.i0 + tx, j = t.j0 + ty;
   const int xa = t.i0 & ~1;                      // staged box start (ghost-inclusive x of cell i0 - 2, made even)
-  const int pos = (ty + 2) * ST_BX + (tx + 2 + (t.i0 - xa));
+  const int sh = t.i0 - xa;
+  auto spos = [&](int cx, int cy) { return (cy + 2) * bx + cx + 2 + sh; };   // tile cell (cx, cy) in a plane
+  const int pos = spos(tx, ty);
   const int k0 = t.k0, k1 = t.k0 + t.nkz;
-  constexpr uint32_t kBoxBytes = (uint32_t)(sizeof(double) * nc * ST_P);
+  const uint32_t box_bytes = (uint32_t)(sizeof(double) * nc * np);
 
   if (tid == 0) {
     mbar_init(bar, 1);
@@ -200,7 +208,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   auto issue = [&](int kp) {                    // plane kp (cell index) into the staging buffer
     if (tid == 0) {
       fence_proxy_async_smem();
-      mbar_arrive_expect_tx(bar, kBoxBytes);
+      mbar_arrive_expect_tx(bar, box_bytes);
       tma_load_4d(stg, map, bar, xa, t.j0, kp + 2, 0);
     }
   };
@@ -214,20 +222,19 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       return false;
     }
     parity ^= 1u;
-    R* dst = ring + slot * nc * ST_P;
-    for (int q = tid; q < nc * ST_P; q += ST_NT) dst[q] = (R)stg[q];
+    R* dst = ring + slot * RSLOT;
+    for (int q = tid; q < nc * np; q += NT) dst[q] = (R)stg[q];
     __syncthreads();
     return true;
   };
   auto stall = [&]() { if (tid == 0) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_TIMEOUT); };
-  auto plane = [&](int slot) { return (const R*)(ring + slot * nc * ST_P); };
+  auto plane = [&](int slot) { return (const R*)(ring + slot * RSLOT); };
 
   // The Jameson sensor from the staged densities (compute_beta, Mod_Fluxes.f90:366-389): the weight of
-  // the cell at column cx, row cy of the tile (0-based from the tile's first cell) on the plane of ring
-  // slot s0, with the planes below and above in slots sm and sp; in 2-D runs (no z march) the planes
-  // below and above are the ghost planes, read from global memory.
-  const int sh = t.i0 - xa;
-  auto rho_at = [&](int slot, int cx, int cy) { return plane(slot)[(cy + 2) * ST_BX + cx + 2 + sh]; };
+  // the tile cell (cx, cy) on the plane of ring slot s0, with the planes below and above in slots sm
+  // and sp; in 2-D runs (no z march) the planes below and above are the ghost planes, read from
+  // global memory.
+  auto rho_at = [&](int slot, int cx, int cy) { return plane(slot)[spos(cx, cy)]; };
   auto beta_at = [&](int sm, int s0, int sp, int cx, int cy, int kc) -> R {
     R zm, zp;
     if (az) { zm = rho_at(sm, cx, cy); zp = rho_at(sp, cx, cy); }
@@ -238,13 +245,15 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     return sd_rho<R>(rho_at(s0, cx, cy), rho_at(s0, cx - 1, cy), rho_at(s0, cx + 1, cy),
                      rho_at(s0, cx, cy - 1), rho_at(s0, cx, cy + 1), zm, zp);
   };
-  // the weights of a whole plane's face cells (columns -1..ST_TX-1, rows -1..ST_TY-1) into BT[b]
-  constexpr int NBX = ST_TX + 1;
+  // the weights of a whole plane's face cells (columns -1..w, rows -1..h) into BT[b]
+  const int nbx = w + 2, nb = (w + 2) * (h + 2);
   auto beta_plane = [&](int b, int sm, int s0, int sp, int kc) {
     if (!F.sd) return;
-    for (int e = tid; e < L::NB; e += ST_NT) BT[b * L::NB + e] = beta_at(sm, s0, sp, e % NBX - 1, e / NBX - 1, kc);
+    for (int e = tid; e < nb; e += NT) BT[b * Shape<CL>::MAXBOX + e] = beta_at(sm, s0, sp, e % nbx - 1, e / nbx - 1, kc);
   };
-  auto beta_of = [&](int b, int cx, int cy) { return F.sd ? BT[b * L::NB + (cy + 1) * NBX + cx + 1] : (R)1; };
+  auto beta_of = [&](int b, int cx, int cy) {
+    return F.sd ? BT[b * Shape<CL>::MAXBOX + (cy + 1) * nbx + cx + 1] : (R)1;
+  };
   int bcur = 0;
 
   // z: slope of the thread's cell at plane c from three ring slots (c-1, c, c+1)
@@ -267,13 +276,13 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     if (c == 0 && F.inj[g - B.pxy]) lm = (R)0;
     if (c == B.nk - 1 && F.inj[g + B.pxy]) lp = (R)0;
     const R* Pm = plane(sm); const R* P0 = plane(s0); const R* Pp = plane(sp);
-    auto q = [&](int s, int v) { return (s == 0 ? Pm : s == 1 ? P0 : Pp)[v * ST_P + pos]; };
+    auto q = [&](int s, int v) { return (s == 0 ? Pm : s == 1 ? P0 : Pp)[v * np + pos]; };
     cell_slope<CL, LIM, R>(F.limiter, q, lm, l0, lp, s, dlc, first);
   };
   // z face between c and c + 1 from the ring slots of the two cells and their slopes
   auto zface = [&](int sl, int sr, int c, const R* sa, R da, bool fa, const R* sb, R db, bool fb, R bf, R* out) {
     R pl[nc], pr[nc];
-    const SmemCell<R, ST_P> ql{plane(sl), pos}, qr{plane(sr), pos};
+    const SmemCell<R> ql{plane(sl), pos, np}, qr{plane(sr), pos, np};
     bad |= states_from_slopes<CL, R>(ql, sa, da, fa, qr, sb, db, fb, bf, pl, pr);
     const long long fi = fidx(B, 2, i, j, c, c + 1);
     R nrm[3], area;
@@ -302,7 +311,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     if (!land(2)) { stall(); return; }
     R sm1[nc]; R dm1 = (R)0; bool fm1 = true;
     R bm1 = (R)1;
-    if (owner) {
+    if (own) {
       zslope(0, 1, 2, k0 - 1, sm1, dm1, fm1);
       if (F.sd) bm1 = beta_at(0, 1, 2, tx, ty, k0 - 1);
     }
@@ -310,7 +319,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     __syncthreads();                            // slot 0 (plane k0-2) is read by every thread before reuse
     if (!land(0)) { stall(); return; }
     beta_plane(bcur, 1, 2, 0, k0);
-    if (owner) {
+    if (own) {
       zslope(1, 2, 0, k0, sz, dlz, fz);
       const R b0 = F.sd ? beta_at(1, 2, 0, tx, ty, k0) : (R)1;
       zface(1, 2, k0 - 1, sm1, dm1, fm1, sz, dlz, fz, mn(bm1, b0), flo);
@@ -326,7 +335,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     if (!land(1)) { stall(); return; }
     issue(1);
     if (!land(2)) { stall(); return; }
-    if (owner) zslope(0, 1, 2, 0, sz, dlz, fz);
+    if (own) zslope(0, 1, 2, 0, sz, dlz, fz);
     beta_plane(bcur, 0, 1, 2, 0);
     issue(2);
     __syncthreads();
@@ -334,29 +343,47 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     cur = 1; nx1 = 2; nx2 = 0;
   }
 
+  // the extra face tasks of a plane: the x faces above the last column (rows 0..h-1), then the y faces
+  // above the last row (columns 0..w-1), where they are interior faces of the block
+  const int nhx = (ax && t.i0 + w < B.ni) ? h : 0;
+  const int nhy = (ay && t.j0 + h < B.nj) ? w : 0;
+  // the face tasks: x and y faces below the owned cells (none along a direction with one cell), extras
+  const int nxo = ax ? w * h : 0, nyo = ay ? w * h : 0;
+  const int nfx = nxo + nyo + nhx + nhy;
+
   for (int k = k0; k < k1; ++k) {
     const bool more = k + 1 < k1;
     if (more) issue(k + 3);                     // lands at the end of this plane, into the slot of k
     const R* P = plane(cur);
-    // a face is computed by the thread of the cell above it when an owned cell reads it: the x faces
-    // of the last row and the y faces of the last column belong to the neighbouring tiles
-    if (ax && col && i >= 1 && (!ay || ty < ST_TY - 1)) {   // x face below (i,j,k)
+    // the x and y faces of this plane, each once, as one list of tasks dealt out to the threads in turn:
+    // the x face below every owned cell, the y face below every owned cell, then the x faces above the
+    // last column and the y faces above the last row (a face on the block's boundary is its records')
+    for (int e = tid; e < nfx; e += NT) {
+      int d, cx, cy;
+      if (e < nxo + nyo) {
+        d = e >= nxo;
+        const int c = e - (d ? nxo : 0);
+        cx = c % w; cy = c / w;
+        if (d == 0 ? t.i0 + cx == 0 : t.j0 + cy == 0) continue;
+      } else if (e < nxo + nyo + nhx) {
+        d = 0; cx = w; cy = e - nxo - nyo;
+      } else {
+        d = 1; cx = e - nxo - nyo - nhx; cy = h;
+      }
+      // the face below tile cell (cx, cy) along d: its lower cell, stencil and the two cells' weights
+      const int lx = cx - (d == 0), ly = cy - (d == 1);
+      const int sst = d == 0 ? 1 : bx;
       R fl[nc];
-      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 0, i - 1, j, k, P, pos - 2, 1,
-                                              mn(beta_of(bcur, tx - 1, ty), beta_of(bcur, tx, ty)), fl);
+      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, d, t.i0 + lx, t.j0 + ly, k, P, np, spos(cx, cy) - 2 * sst, sst,
+                                              mn(beta_of(bcur, lx, ly), beta_of(bcur, cx, cy)), fl);
+      R* dst = d == 0 ? Fx + cy * (w + 1) + cx : Fy + cy * w + cx;
+      const int vs = d == 0 ? FX : FY;
 #pragma unroll
-      for (int v = 0; v < nc; ++v) Fx[v * ST_NT + tid] = fl[v];
-    }
-    if (ay && col && j >= 1 && (!ax || tx < ST_TX - 1)) {   // y face below (i,j,k)
-      R fl[nc];
-      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, 1, i, j - 1, k, P, pos - 2 * ST_BX, ST_BX,
-                                              mn(beta_of(bcur, tx, ty - 1), beta_of(bcur, tx, ty)), fl);
-#pragma unroll
-      for (int v = 0; v < nc; ++v) Fy[v * ST_NT + tid] = fl[v];
+      for (int v = 0; v < nc; ++v) dst[v * vs] = fl[v];
     }
     // z: the face above the cell, from the slopes at k (carried) and k + 1
     R szn[nc]; R dlzn = (R)0; bool fzn = true;
-    if (az && owner && k <= B.nk - 2) {
+    if (az && own && k <= B.nk - 2) {
       zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
       const R b1 = F.sd ? beta_at(cur, nx1, nx2, tx, ty, k + 1) : (R)1;
       zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), b1), fhi);
@@ -364,7 +391,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     // the next plane's weights (its planes below and above are in the ring now), read after a barrier
     if (az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
     __syncthreads();
-    if (owner) {
+    if (own) {
       const long long q = iidx(B, i, j, k);
       const int bc = F.bmap[q];
       // the cell's residual, summed in the reference's order: in FP64 in the plain form, in FP32
@@ -375,41 +402,43 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       for (int v = 0; v < nc; ++v) r[v] = bc >= 0 ? (A)F.Rb[(long long)bc * nc + v] : (A)0;
       if (ax) {
         const int ci = i + 1, n = B.ni;
+        const int lo = ty * (w + 1) + tx;
         if (ci % 2 == 1) {
           if (ci < n) {
 #pragma unroll
-            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fx[v * ST_NT + tid + 1];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fx[v * FX + lo + 1];
           }
           if (ci > 1) {
 #pragma unroll
-            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fx[v * ST_NT + tid];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fx[v * FX + lo];
           }
         } else {
 #pragma unroll
-          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fx[v * ST_NT + tid];
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fx[v * FX + lo];
           if (ci < n) {
 #pragma unroll
-            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fx[v * ST_NT + tid + 1];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fx[v * FX + lo + 1];
           }
         }
       }
       if (ay) {
         const int cj = j + 1, n = B.nj;
+        const int lo = ty * w + tx;
         if (cj % 2 == 1) {
           if (cj < n) {
 #pragma unroll
-            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fy[v * ST_NT + tid + ST_TX];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fy[v * FY + lo + w];
           }
           if (cj > 1) {
 #pragma unroll
-            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fy[v * ST_NT + tid];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fy[v * FY + lo];
           }
         } else {
 #pragma unroll
-          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fy[v * ST_NT + tid];
+          for (int v = 0; v < nc; ++v) r[v] = r[v] + (A)Fy[v * FY + lo];
           if (cj < n) {
 #pragma unroll
-            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fy[v * ST_NT + tid + ST_TX];
+            for (int v = 0; v < nc; ++v) r[v] = r[v] - (A)Fy[v * FY + lo + w];
           }
         }
       }
@@ -487,7 +516,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
         if (cn[0] < 0.0) atomicAdd(&st->nfloored, 1ULL);
         cons2prim<CL, sizeof(R) == 4>(cn, p, F.mat.cp);
         if constexpr (sizeof(R) == 4) {
-          if (realize<CL>(p)) atomicAdd(&st->nrealized, 1ULL);
+          if (F.realize && realize<CL>(p)) atomicAdd(&st->nrealized, 1ULL);
         }
         if (!check_prim<CL, double>(p)) atomicOr(&st->flags, (unsigned)ICE_GPU_ST_NAN_STATE);
 #pragma unroll
@@ -502,8 +531,8 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     {
       const bool ok = mbar_wait(bar, parity);
       if (ok) {
-        R* dst = ring + cur * nc * ST_P;
-        for (int e = tid; e < nc * ST_P; e += ST_NT) dst[e] = (R)stg[e];
+        R* dst = ring + cur * RSLOT;
+        for (int e = tid; e < nc * np; e += NT) dst[e] = (R)stg[e];
       }
       if (__syncthreads_or(!ok)) {
         if (!ok) mbar_wait(bar, parity);

@@ -28,7 +28,7 @@ module ice_gpu
     real(c_double)     :: cfl, dt_max, tau_factor
     integer(c_int32_t) :: cfl_ramp_iter, limiter, shock_detector, irs
     real(c_double)     :: irs_beta
-    integer(c_int32_t) :: coupled, drag, heat, blow, precision, itermax, sol_diter, shell_diter, res_diter, pad0
+    integer(c_int32_t) :: coupled, drag, heat, blow, precision, itermax, sol_diter, shell_diter, res_diter, no_realize
     real(c_double)     :: time_threshold, res_threshold, sol_dtime
     type(ice_gpu_family_t) :: fam(ICE_GPU_MAX_FAMILIES)
   end type ice_gpu_params_t

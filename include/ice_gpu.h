@@ -121,7 +121,9 @@ typedef struct ice_gpu_params {
     int32_t sol_diter;
     int32_t shell_diter;
     int32_t res_diter;
-    int32_t pad0;
+    int32_t no_realize;                 /* 1: the FP32-flux form skips its realizability
+                                           correction of AG states (ice_gpu_step_out::
+                                           nrealized); 0, the default, applies it         */
     double  time_threshold;
     double  res_threshold;
     double  sol_dtime;

@@ -208,10 +208,14 @@ def test_multiblock_imports(gpu, orc, steady):
 @pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP32FLUX], ids=["fp64", "fp32flux"])
 def test_exchange_rates(gpu, orc, prec):
     # two-way coupling: the rates the gas receives from every family over a step (3 RK stages). The
-    # plain form against the oracle to 1e-12 of each component's largest value; the chosen form to 1e-4
+    # plain form against the oracle to 1e-12 of each component's largest value; the chosen form to 1e-4,
+    # its single-precision fluxes and sources alone: its realizability correction off, since it moves
+    # the AG cells that the scheme itself leaves with a covariance that is not positive definite in the
+    # first steps of this case (tests/test_realizability.py)
     make = lambda: configs.multiblock_tree(nblocks=5, seed=4, lo=5, hi=10, steps=4, precision=prec)
     cg, co = make(), make()
     cg.numerics.precision = prec
+    cg.numerics.realize = False
     co.numerics.precision = abi.PREC_FP64
     sg, so = Solver(cg, gpu), Solver(co, orc)
     assert gpu.set_exchange(sg.ctx, 1) == 0 and orc.set_exchange(so.ctx, 1) == 0
