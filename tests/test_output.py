@@ -68,15 +68,84 @@ def test_layout_matches_reference_files(closure):
     assert text[-7:-1] == aux
 
 
-def _restart_through_file(lib, tmp_path, make, n, total):
+def _reference_vtk_time(vtm):
+    """The TIME of a VTK solution as the reference's restart test reads it (test/fast/restart/run.py,
+    vtk_time): the first block file the .vtm lists, raw appended data, a 4-byte size, then the value."""
+    import re
+    import struct
+    block = re.search(r'file="([^"]+\.vts)"', vtm.read_text()).group(1)
+    data = (vtm.parent / block).read_bytes()
+    head = data.find(b'<AppendedData')
+    m = re.search(rb'Name="TIME"[^>]*offset="(\d+)"', data[:head])
+    start = data.find(b'_', head) + 1 + int(m.group(1))
+    return struct.unpack('<d', data[start + 4:start + 12])[0]
+
+
+def _reference_read_vts(path):
+    """({name: bytes} of the CellData arrays, (ni, nj, nk)) as the reference's equiv3d test reads a
+    raw-appended .vts (test/fast/equiv3d/run.py, read_vts), without decoding."""
+    import re
+    import struct
+    data = Path(path).read_bytes()
+    head_end = data.find(b'<AppendedData')
+    header = data[:head_end].decode('ascii', 'replace')
+    m = re.search(r'header_type="(\w+)"', header)
+    hsize = 8 if (m and m.group(1) == 'UInt64') else 4
+    hfmt = '<Q' if hsize == 8 else '<I'
+    m = re.search(r'WholeExtent="([+-]?\d+) ([+-]?\d+) ([+-]?\d+) ([+-]?\d+) ([+-]?\d+) ([+-]?\d+)"', header)
+    e = [int(x) for x in m.groups()]
+    dims = (e[1] - e[0], e[3] - e[2], e[5] - e[4])
+    start = data.find(b'_', head_end) + 1
+    arrays = {}
+    cell = header[header.find('<CellData'):header.find('</CellData>')]
+    for name, off in re.findall(r'<DataArray[^>]*Name="+([^"]+)"+[^>]*offset="(\d+)"', cell):
+        off = start + int(off)
+        n = struct.unpack(hfmt, data[off:off + hsize])[0]
+        arrays[name] = data[off + hsize:off + hsize + n]
+    return arrays, dims
+
+
+def test_vtk_layout_as_the_reference_reads_it(orc, tmp_path):
+    """A VTK solution of the three-family multi-block case, as the reference's own test readers parse it:
+    the TIME of the first block file is the solution time; every block file has one CellData array per
+    variable of every family, named as the Tecplot file's VARIABLES, each 8 bytes per cell (raw doubles);
+    the arrays hold the state (i fastest), and the whole solution reads back to the same bits and
+    counters as the Tecplot file of the same state."""
+    case = configs.multiblock_tree(nblocks=3, seed=2, lo=4, hi=6, steps=3)
+    s = Solver(case, orc)
+    out = s.step(3)
+    vtm = Path(output.write_solution(tmp_path / "part-field.vtm", s, out, 2, fmt="vtk"))
+    tec = Path(output.write_solution(tmp_path / "part-field.tec", s, out, 2))
+    assert _reference_vtk_time(vtm) == out.time
+    states = s.download_all()
+    files = sorted((tmp_path / "vtk").glob("*.vts"))
+    assert len(files) == len(case.nodes)
+    for b, f in enumerate(sorted(files, key=lambda x: int(x.stem.split("_")[-1]))):
+        arrays, dims = _reference_read_vts(f)
+        assert dims == tuple(case.dims[b])
+        assert list(arrays) == output.variable_names(case)
+        v0 = 0
+        for p, fam in enumerate(case.families):
+            for v in range(fam.nc):
+                buf = arrays[output.variable_names(case)[v0 + v]]
+                assert len(buf) == 8 * int(np.prod(dims))
+                assert np.array_equal(np.frombuffer(buf, dtype="<f8"), states[b][p][2:-2, 2:-2, 2:-2, v].ravel())
+            v0 += fam.nc
+    a, t = output.read_vtk(vtm), output.read_solution(tec)
+    assert a["time"] == t["time"] and a["aux"] == t["aux"]
+    for (da, na, ca), (dt, nt, ct) in zip(a["blocks"], t["blocks"]):
+        assert da == dt and np.array_equal(na, nt) and np.array_equal(ca, ct)
+
+
+def _restart_through_file(lib, tmp_path, make, n, total, fmt="tecplot"):
     a = Solver(make(), lib)
     oa = a.step(total)
     b = Solver(make(), lib)
     ob = b.step(n)
-    path = tmp_path / "part-field.tec"
-    output.write_solution(path, b, ob)
+    path = tmp_path / ("part-field.vtm" if fmt == "vtk" else "part-field.tec")
+    output.write_solution(path, b, ob, fmt=fmt)
     c = Solver(make(), lib, upload=False)
-    output.restart(c, output.read_solution(path))
+    output.restart(c, output.read_any(path))
     oc = c.step(total - n)
     assert oa.iter == oc.iter and oa.todo == oc.todo
     for per_a, per_c in zip(a.download_all(), c.download_all()):
@@ -88,12 +157,14 @@ def _restart_through_file(lib, tmp_path, make, n, total):
 def _restart_checks(lib, tmp_path):
     """steady: the stream res-threshold stops at 444, written at 200 and restarted from the file, stops
     at 444 in the same state (the file carries the residual reference). transient: the three-family
-    multi-block case, 10 = 5 + 5 steps, with its time. The file's text is the text of the state."""
-    oa, oc = _restart_through_file(lib, tmp_path, lambda: configs.stream_tube("scaling"), 200, 20000)
-    assert 200 < oa.iter < 20000 and oa.todo == 3
-    oa, oc = _restart_through_file(
-        lib, tmp_path, lambda: configs.multiblock_tree(nblocks=4, seed=5, lo=4, hi=7, steps=10), 5, 10)
-    assert oa.time == oc.time
+    multi-block case, 10 = 5 + 5 steps, with its time. In both formats (restart-exact's steady, transient,
+    steady-vtk and transient-vtk legs)."""
+    for fmt in ("tecplot", "vtk"):
+        oa, oc = _restart_through_file(lib, tmp_path, lambda: configs.stream_tube("scaling"), 200, 20000, fmt)
+        assert 200 < oa.iter < 20000 and oa.todo == 3
+        oa, oc = _restart_through_file(
+            lib, tmp_path, lambda: configs.multiblock_tree(nblocks=4, seed=5, lo=4, hi=7, steps=10), 5, 10, fmt)
+        assert oa.time == oc.time
 
 
 def _async_checks(lib, tmp_path):
