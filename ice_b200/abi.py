@@ -17,7 +17,7 @@ NEP = 8
 REC_INTS = 15
 REC_REALS = 8
 
-OK, EINVAL, ECUDA, ESTATE, ENOMEM, ENOTREADY = 0, 1, 2, 3, 4, 5
+OK, EINVAL, ECUDA, ESTATE, ENOMEM, ENOTREADY, EEXCH = 0, 1, 2, 3, 4, 5, 6
 ST_NAN_STATE, ST_BAD_RECON, ST_TIMEOUT = 1, 2, 4
 
 CLOSURE = {"MK": 1, "IG": 2, "AG": 3}
@@ -107,6 +107,9 @@ _SIGNATURES = [
     ("destroy", C.c_int, [_vp]),
     ("pair_connections", C.c_int, [C.c_int32, _ip, C.c_int32, C.c_int32, _ip, C.c_char_p, C.c_int32]),
     ("index_maps", C.c_int, [_vp, C.c_int32, _ip, _ip, _ip, _ip, _ip, _ip]),
+    ("set_partition", C.c_int, [_vp, _ip]),
+    ("set_halo", C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _ip, C.c_int32, _ip]),
+    ("set_exchange_hook", C.c_int, [_vp, _vp, _vp]),
 ]
 GPU_ONLY = [
     ("step_host", C.c_int, [_vp, C.c_int32, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(StepOut)]),

@@ -37,7 +37,7 @@ def nvcc() -> str:
 
 
 def headers():
-    return sorted(SRC.glob("*.cuh")) + [PKG.parent / "include" / "ice_gpu.h"]
+    return sorted(SRC.glob("*.cuh")) + sorted(SRC.glob("*.h")) + [PKG.parent / "include" / "ice_gpu.h"]
 
 
 def _newer(target: Path, deps) -> bool:

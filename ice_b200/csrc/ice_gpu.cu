@@ -44,6 +44,7 @@
 #include "ice_kernels.cuh"
 #include "ice_stage3.cuh"
 #include "ice_mlp.cuh"
+#include "ice_tune.h"
 #include "../../include/ice_gpu.h"
 
 using namespace ice;
@@ -385,6 +386,9 @@ static void enqueue_step_family(ice_gpu_ctx* c, int p, int phase, cudaStream_t s
   for (int srk = 1; srk <= c->P.nrk; ++srk) launch_family(c, p, srk, phase, s, tick);
 }
 
+// The step: its dt over every family, then the families' RK stages one family after the other. (Run
+// side by side on forked streams, the families' stage kernels shared the SMs with one another's
+// differently sized CTAs and the 48-block step took 4.6 % longer, 139.9 ms against 133.7 ms.)
 static void enqueue_step(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*tick)(void*, int, cudaStream_t)) {
   enqueue_step_dt(c, phase, s, tick);
   for (int p = 0; p < c->P.nfam; ++p) enqueue_step_family(c, p, phase, s, tick);
@@ -442,15 +446,27 @@ static void shape_limits(int closure, int& NT, int& MW, int& MH, int& MB, int& F
 // evenly from the block (ceil(ni / W) tiles of ceil(ni / nx) columns, likewise rows), take the fewest
 // passes of the CTA per plane over the whole block: the face tasks (x and y faces below the owned
 // cells, the faces above the last column and row) dealt out to the NT threads, then the z face and
-// the update; among equals, the fewest tiles. Returns w, h (the even cut) and the box.
+// the update (zpass of the tuned schedule); at most wcap columns; among equals, the fewest tiles.
+// Returns w, h (the even cut) and the box.
+// The schedule of a closure: its row of the tuned table (ice_tune.h), or ICE_GPU_TUNE="kz,zpass,wcap".
+static TuneRow tune_of(int closure) {
+  TuneRow r = kTune[std::min(std::max(closure, 1), 3) - 1];
+  if (const char* e = getenv("ICE_GPU_TUNE")) {
+    int kz, zp, wc;
+    if (sscanf(e, "%d,%d,%d", &kz, &zp, &wc) == 3 && kz >= 1 && kz <= ST_KZ && zp >= 0 && wc >= 1) r = TuneRow{kz, zp, wc};
+  }
+  return r;
+}
+
 static Tile tile_shape3(int ni, int nj, int closure) {
   int NT, MW, MH, MB, FX, FY;
   shape_limits(closure, NT, MW, MH, MB, FX, FY);
   (void)MW;
+  const TuneRow tr = tune_of(closure);
   Tile best{};
   long long best_cost = -1, best_tiles = 0;
   const bool ax = ni >= 2, ay = nj >= 2;
-  const int wmax = ax ? std::min(ni, NT) : 1;
+  const int wmax = ax ? std::min(std::min(ni, NT), tr.wcap) : 1;
   for (int W = 1; W <= wmax; ++W) {
     if (st_box_x(W) > 256) break;                 // a TMA box is at most 256 elements along each axis
     const int hmax = std::min(std::min(nj, MH), NT / W);
@@ -460,7 +476,7 @@ static Tile tile_shape3(int ni, int nj, int closure) {
       const int w = (ni + nx - 1) / nx, h = (nj + ny - 1) / ny;
       const int tasks = (ax ? w * h + h : 0) + (ay ? w * h + w : 0);
       const long long tiles = (long long)nx * ny;
-      const long long cost = tiles * ((tasks + NT - 1) / NT + 2);
+      const long long cost = tiles * ((tasks + NT - 1) / NT + tr.zpass);
       if (best_cost < 0 || cost < best_cost || (cost == best_cost && tiles < best_tiles)) {
         best_cost = cost; best_tiles = tiles;
         best = Tile{0, 0, 0, 0, 0, (short)w, (short)h, (short)st_box_x(w), (short)(h + 4)};
@@ -470,16 +486,18 @@ static Tile tile_shape3(int ni, int nj, int closure) {
   return best;
 }
 
-// The chunk height of the staged kernel's tiles for one family: of a few candidates up to ST_KZ
-// planes, the one whose tiles, handed longest first to the least-loaded of the GPU's resident CTA
+// The chunk height of the staged kernel's tiles for one family: of a few candidates up to the tuned
+// kz planes, the one whose tiles, handed longest first to the least-loaded of the GPU's resident CTA
 // slots (as the block scheduler hands them out), finish soonest; a tile costs its planes plus the
 // three its prologue loads. Small grids get shorter chunks and more tiles, so that the last wave is
-// not left half empty; large ones keep ST_KZ (a change must gain more than 1 %).
+// not left half empty; large ones keep the largest (a change must gain more than 1 %).
 static int choose_kz(const ice_gpu_ctx* c, const FamHost& H, int slots) {
-  static const int cand[] = {ST_KZ, 28, 24, 20, 16, 12, 8};
-  int best = ST_KZ;
+  static const int cand[] = {ST_KZ, 28, 24, 20, 16, 12, 8, 4};
+  const int kzmax = tune_of(H.closure).kz;
+  int best = 0;
   double best_t = 0.0;
   for (int kz : cand) {
+    if (kz > kzmax) continue;
     std::vector<int> cost;
     for (int b = 0; b < c->nb; ++b) {
       int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
@@ -498,7 +516,7 @@ static int choose_kz(const ice_gpu_ctx* c, const FamHost& H, int slots) {
       load.pop(); load.push(l);
       span = std::max(span, l);
     }
-    if (kz == ST_KZ || (double)span < 0.99 * best_t) { best = kz; best_t = (double)span; }
+    if (best == 0 || (double)span < 0.99 * best_t) { best = kz; best_t = (double)span; }
   }
   return best;
 }

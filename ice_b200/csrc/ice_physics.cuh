@@ -187,20 +187,22 @@ template <int CL, bool FAST = false> __device__ __forceinline__ void cons2prim(c
 }
 
 // The chosen form's realizability correction of an occupied AG cell (FP64, after cons -> prim and
-// its floors, which keep the density and the diagonal of the covariance positive). The covariance P
-// of a cell whose density is above rho_empty must stay positive definite, and single-precision fluxes
-// can carry a nearly singular P across that bound. Sylvester's test (P11 > 0 by the floors, then the
-// 2 x 2 leading minor and the determinant) passes for a positive definite P at the cost of a few
-// products. Otherwise, with D the diagonal of P, the correlation C = D^-1/2 P D^-1/2 = I + O has a unit
-// diagonal, and scaling every off-diagonal of P by s scales O by s: the eigenvalues of C become
+// its floors, which keep the density and the diagonal of the covariance positive). Single-precision
+// fluxes can carry the covariance P of a nearly singular cell across the positive-definite bound by a
+// rounding; the correction takes such a cell back inside. Sylvester's test (P11 > 0 by the floors,
+// then the 2 x 2 leading minor and the determinant) passes for a positive definite P at the cost of a
+// few products. Otherwise, with D the diagonal of P, the correlation C = D^-1/2 P D^-1/2 = I + O has
+// a unit diagonal, and scaling every off-diagonal of P by s scales O by s: the eigenvalues of C become
 // 1 + s mu_i. With mu the smallest eigenvalue of O (the trace-free 3 x 3 case of the closed-form
-// symmetric eigenvalues, 2 q cos(theta + 2 pi / 3)), the off-diagonals scale by
-// s = (1 - kRealizeMargin) / -mu, so that the smallest eigenvalue of C is kRealizeMargin. The diagonal,
-// hence the trace and the energy, is kept. Cells at or below rho_empty keep the reference's caps
-// (their dispersion bounded by theta_cap in cons2prim) and are left alone. Returns true when it
-// changed the state. The plain form never calls it: the reference applies its floors only
-// (Lib_Model_AG.f90:81-90).
+// symmetric eigenvalues, 2 q cos(theta + 2 pi / 3)), a cell whose smallest correlation eigenvalue
+// 1 + mu lies in [-kRealizeBand, 0) has its off-diagonals scaled by s = (1 - kRealizeMargin) / -mu,
+// so that it becomes kRealizeMargin; the diagonal, hence the trace and the energy, is kept. A larger
+// violation is the scheme's own (the reference's FP64 path produces them too, for instance in the
+// first steps of a cloud, and keeps them: its floors are all it applies, Lib_Model_AG.f90:81-90), and
+// so are cells at or below rho_empty, which keep the reference's dispersion cap: both are left as the
+// reference leaves them. Returns true when it changed the state. The plain form never calls it.
 constexpr double kRealizeMargin = 1e-6;
+constexpr double kRealizeBand = 1e-4;
 template <int CL> __device__ __forceinline__ bool realize(double* p) {
   if constexpr (CL != AG) {
     return false;
@@ -216,7 +218,7 @@ template <int CL> __device__ __forceinline__ bool realize(double* p) {
     double r = (c12*c13*c23) / (q2*q);
     r = fmin(1.0, fmax(-1.0, r));
     const double mu = 2.0*q*cos(acos(r) / 3.0 + 2.0943951023931957);
-    if (!(mu < -(1.0 - kRealizeMargin))) return false;
+    if (!(1.0 + mu < 0.0 && 1.0 + mu >= -kRealizeBand)) return false;
     const double sc = (1.0 - kRealizeMargin) / -mu;
     p[5] = p[5]*sc; p[6] = p[6]*sc; p[8] = p[8]*sc;
     return true;

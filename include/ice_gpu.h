@@ -43,6 +43,7 @@ extern "C" {
 #define ICE_GPU_ESTATE         3   /* the step stopped on a state the reference stops on */
 #define ICE_GPU_ENOMEM         4
 #define ICE_GPU_ENOTREADY      5   /* a required input has not been given */
+#define ICE_GPU_EEXCH          6   /* the exchange hook of a split run reported a failure */
 
 /* Status bits of ice_gpu_step_out.status (the reference's error stops) */
 #define ICE_GPU_ST_NAN_STATE   1   /* NaN/Inf after an update   (Lib_Newstate.f90:189-193)  */
@@ -347,6 +348,42 @@ int ice_gpu_pair_connections(int32_t nblocks, const int32_t* dims, int32_t ngrou
  * grid%bcells(p) and grid%conn(p)%own for comparison with the reference's. */
 int ice_gpu_index_maps(const ice_gpu_ctx* ctx, int32_t p, int32_t* nbcell, int32_t* first,
                        int32_t* nrecs, int32_t* recs, int32_t* nown, int32_t* own);
+
+/* ---- The block split over ranks (one GPU per rank) --------------------------------------------
+ * replaces: the MPI block decomposition of parallel/Mod_MPI.f90:109-183 (blocks per rank) and the
+ * exchanges of parallel/Mod_GhostExchange.f90:737-893 (remote source cells of the ghost layers,
+ * connection fluxes owner -> partner, partner Jameson weights), with the min-reduction of the step's
+ * dt (Mod_Explicit.f90:67-73) and the sum of the residual norm's partial sums.
+ *
+ * Every rank creates a context of the whole case (every block's geometry, records and gas), then
+ * ice_gpu_set_partition names the blocks it steps; it keeps the other blocks' state only where its
+ * ghost layers read them. ice_gpu_set_halo gives, per family and kind, the entries this rank sends
+ * and receives, in buffer order, per peer one after the other. At each exchange point the step packs
+ * the send buffer, calls the hook, and unpacks the receive buffer the hook filled. Every rank calls
+ * the hook at the same points, in the same order: a hook over MPI or torch.distributed matches them.
+ * ice_gpu_residual_norm is then collective too. Imports, chimera records and IRS are refused. */
+#define ICE_GPU_HALO_CELLS 0   /* entries (b, i, j, k), 1-based; nc doubles each: the cell's state      */
+#define ICE_GPU_HALO_BETA  1   /* entries (b, i, j, k); one double each: the cell's Jameson weight     */
+#define ICE_GPU_HALO_FLUX  2   /* entries (cf, 0, 0, 0): nc doubles each, a connection face's flux       */
+#define ICE_GPU_HALO_DT    3   /* the hook's reduction: the minimum over ranks of 1 double             */
+#define ICE_GPU_HALO_NORM  4   /* the hook's reduction: the sum over ranks of 5 nblocks nfam doubles   */
+
+/* The exchange: kind, 1-based family (0 for DT and NORM), the packed send buffer of nsend doubles
+ * and the receive buffer of nrecv doubles to fill (host memory). For DT and NORM the hook writes the
+ * reduction of every rank's send buffer into recv. Returns 0, or non-zero to stop the step with
+ * ICE_GPU_EEXCH. */
+typedef int32_t (*ice_gpu_exchange_fn)(void* user, int32_t kind, int32_t family, int64_t nsend,
+                                       const double* send, int64_t nrecv, double* recv);
+
+/* owned[nblocks]: 1 for a block this rank steps, 0 otherwise (default: every block). */
+int ice_gpu_set_partition(ice_gpu_ctx* ctx, const int32_t* owned);
+
+/* The lists of one kind (HALO_CELLS, BETA or FLUX) of family p: send[4 nsend], recv[4 nrecv]. */
+int ice_gpu_set_halo(ice_gpu_ctx* ctx, int32_t kind, int32_t p, int32_t nsend, const int32_t* send,
+                     int32_t nrecv, const int32_t* recv);
+
+/* The hook a split step calls at its exchange points (user is passed back). */
+int ice_gpu_set_exchange_hook(ice_gpu_ctx* ctx, ice_gpu_exchange_fn fn, void* user);
 
 /* Measurement: device time [ms] of the kernels of the last ice_gpu_step, by kernel
  * class (0 dt, 1 ghost, 2 beta, 3 bound, 4 stage, 5 irs, 6 norm), and the

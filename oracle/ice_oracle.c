@@ -79,8 +79,20 @@ typedef struct orc_ctx {
     int res_end;          /* the last step ended the run on res-threshold */
     double* fbuf;         /* face flux scratch */
     size_t fbuf_n;
+    /* the block split (set_partition, set_halo, set_exchange_hook): the blocks this rank steps (NULL:
+     * every block), the exchange lists per kind and family, the hook and its buffers */
+    int* owned;
+    int nhs[3][MAXF], nhr[3][MAXF];
+    int *hs[3][MAXF], *hr[3][MAXF];
+    ice_gpu_exchange_fn hook;
+    void* hook_user;
+    double* hbuf;
+    size_t hbuf_n;
     char err[512];
 } orc_ctx;
+
+/* The block split: a block this rank steps (every block without a partition). */
+static inline int OWN(const orc_ctx* c, int b) { return !c->owned || c->owned[b]; }
 
 static const int guide[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
 
@@ -163,7 +175,8 @@ int orc_destroy(orc_ctx* c) {
     }
     free(c->blk); free(c->bc); free(c->grp_first); free(c->grp); free(c->cdon); free(c->cw);
     for (int p = 0; p < MAXF; ++p) { free(c->bfirst[p]); free(c->brec[p]); free(c->connF[p]); free(c->own[p]); }
-    free(c->fbuf);
+    free(c->fbuf); free(c->hbuf); free(c->owned);
+    for (int k = 0; k < 3; ++k) for (int p = 0; p < MAXF; ++p) { free(c->hs[k][p]); free(c->hr[k][p]); }
     free(c);
     return 0;
 }
@@ -665,15 +678,112 @@ static void second_ghost_record(orc_ctx* c, const orec* r) {
 static void compute_ghost(orc_ctx* c, int p) {
     int lo = c->grp_first[p], hi = c->grp_first[p + 1];
     #pragma omp parallel for schedule(dynamic, 64)
-    for (int ii = lo; ii < hi; ++ii) ghost_record(c, &c->bc[c->grp[ii]]);
+    for (int ii = lo; ii < hi; ++ii) {
+        const orec* r = &c->bc[c->grp[ii]];
+        if (OWN(c, r->b - 1)) ghost_record(c, r);
+    }
     #pragma omp parallel for schedule(dynamic, 64)
-    for (int ii = lo; ii < hi; ++ii) second_ghost_record(c, &c->bc[c->grp[ii]]);
+    for (int ii = lo; ii < hi; ++ii) {
+        const orec* r = &c->bc[c->grp[ii]];
+        if (OWN(c, r->b - 1)) second_ghost_record(c, r);
+    }
+}
+
+/* ------------------------------------------------------ the block split */
+/* One exchange of a split step (Mod_GhostExchange.f90:737-800 for the cells): pack the kind's send
+ * entries of family p, let the hook move the buffers, unpack the receive entries. CELLS: the cells'
+ * state into the local copy of the remote block; BETA: the Jameson weights of cells; FLUX: connection
+ * face fluxes (nc each) by face number. */
+static int halo_exchange(orc_ctx* c, int kind, int p) {
+    if (!c->owned) return 0;
+    int nc = nc_of(c, p), w = kind == ICE_GPU_HALO_BETA ? 1 : nc;
+    long ns = (long)c->nhs[kind][p] * w, nr = (long)c->nhr[kind][p] * w;
+    if (c->hbuf_n < (size_t)(ns + nr + 1)) {
+        free(c->hbuf); c->hbuf_n = (size_t)(ns + nr + 1); c->hbuf = (double*)malloc(sizeof(double)*c->hbuf_n);
+    }
+    double* sb = c->hbuf; double* rb = c->hbuf + ns;
+    for (int n = 0; n < c->nhs[kind][p]; ++n) {
+        const int* e = c->hs[kind][p] + 4*n;
+        if (kind == ICE_GPU_HALO_FLUX) { memcpy(sb + (long)n*w, c->connF[p] + (long)(e[0] - 1)*NCM, sizeof(double)*nc); continue; }
+        oblk* B = &c->blk[e[0] - 1];
+        if (kind == ICE_GPU_HALO_CELLS) memcpy(sb + (long)n*w, B->fam[p].prim + (long)nc*CI(B, e[1], e[2], e[3]), sizeof(double)*nc);
+        else sb[n] = B->fam[p].beta[II(B, e[1], e[2], e[3])];
+    }
+    if (!c->hook) return seterr(c, ICE_GPU_ENOTREADY, "a split run needs its exchange hook (set_exchange_hook)");
+    if (c->hook(c->hook_user, kind, p + 1, ns, sb, nr, rb) != 0)
+        return seterr(c, ICE_GPU_EEXCH, "the exchange hook failed (kind %d, family %d)", kind, p + 1);
+    for (int n = 0; n < c->nhr[kind][p]; ++n) {
+        const int* e = c->hr[kind][p] + 4*n;
+        if (kind == ICE_GPU_HALO_FLUX) { memcpy(c->connF[p] + (long)(e[0] - 1)*NCM, rb + (long)n*w, sizeof(double)*nc); continue; }
+        oblk* B = &c->blk[e[0] - 1];
+        if (kind == ICE_GPU_HALO_CELLS) memcpy(B->fam[p].prim + (long)nc*CI(B, e[1], e[2], e[3]), rb + (long)n*w, sizeof(double)*nc);
+        else B->fam[p].beta[II(B, e[1], e[2], e[3])] = rb[n];
+    }
+    return 0;
+}
+
+/* The reductions of a split step: the minimum (DT) or the sum (NORM) over the ranks of n doubles. */
+static int halo_reduce(orc_ctx* c, int kind, double* x, long n) {
+    if (!c->owned) return 0;
+    if (!c->hook) return seterr(c, ICE_GPU_ENOTREADY, "a split run needs its exchange hook (set_exchange_hook)");
+    double* in = (double*)malloc(sizeof(double)*n);
+    memcpy(in, x, sizeof(double)*n);
+    int rc = c->hook(c->hook_user, kind, 0, n, in, n, x);
+    free(in);
+    return rc ? seterr(c, ICE_GPU_EEXCH, "the exchange hook failed (kind %d)", kind) : 0;
+}
+
+int orc_set_partition(orc_ctx* c, const int* owned) {
+    if (!owned) { free(c->owned); c->owned = NULL; return 0; }
+    if (c->P.irs) return seterr(c, ICE_GPU_EINVAL, "set_partition: IRS is not supported in a split run");
+    if (c->nchim > 0) return seterr(c, ICE_GPU_EINVAL, "set_partition: chimera records are not supported in a split run");
+    for (int p = 0; p < c->P.nfam; ++p)
+        if (c->have_imp[p]) return seterr(c, ICE_GPU_EINVAL, "set_partition: imports are not supported in a split run");
+    free(c->owned);
+    c->owned = (int*)malloc(sizeof(int)*c->nb);
+    for (int b = 0; b < c->nb; ++b) c->owned[b] = owned[b] != 0;
+    return 0;
+}
+
+int orc_set_halo(orc_ctx* c, int kind, int p1, int nsend, const int* send, int nrecv, const int* recv) {
+    if (kind < 0 || kind > 2 || p1 < 1 || p1 > c->P.nfam || nsend < 0 || nrecv < 0 ||
+        (nsend > 0 && !send) || (nrecv > 0 && !recv))
+        return seterr(c, ICE_GPU_EINVAL, "set_halo: bad arguments");
+    int p = p1 - 1;
+    for (int side = 0; side < 2; ++side) {
+        int n = side ? nrecv : nsend;
+        const int* e = side ? recv : send;
+        for (int q = 0; q < n; ++q) {
+            const int* x = e + 4*q;
+            if (kind == ICE_GPU_HALO_FLUX) {
+                if (x[0] < 1 || x[0] > c->nconn[p]) return seterr(c, ICE_GPU_EINVAL, "set_halo: connection face %d", x[0]);
+                continue;
+            }
+            if (x[0] < 1 || x[0] > c->nb) return seterr(c, ICE_GPU_EINVAL, "set_halo: block %d", x[0]);
+            const oblk* B = &c->blk[x[0] - 1];
+            if (x[1] < 1 || x[1] > B->ni || x[2] < 1 || x[2] > B->nj || x[3] < 1 || x[3] > B->nk)
+                return seterr(c, ICE_GPU_EINVAL, "set_halo: cell %d %d %d outside block %d", x[1], x[2], x[3], x[0]);
+        }
+    }
+    free(c->hs[kind][p]); free(c->hr[kind][p]);
+    c->hs[kind][p] = (int*)malloc(sizeof(int)*4*(nsend + 1));
+    c->hr[kind][p] = (int*)malloc(sizeof(int)*4*(nrecv + 1));
+    if (nsend) memcpy(c->hs[kind][p], send, sizeof(int)*4*nsend);
+    if (nrecv) memcpy(c->hr[kind][p], recv, sizeof(int)*4*nrecv);
+    c->nhs[kind][p] = nsend; c->nhr[kind][p] = nrecv;
+    return 0;
+}
+
+int orc_set_exchange_hook(orc_ctx* c, ice_gpu_exchange_fn fn, void* user) {
+    c->hook = fn; c->hook_user = user;
+    return 0;
 }
 
 /* ---------------------------------------------------------------- beta */
 static void compute_beta(orc_ctx* c, int p) {
     int nc = nc_of(c, p);
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         #pragma omp parallel for collapse(2) schedule(static)
@@ -743,6 +853,7 @@ static int compute_bound(orc_ctx* c, int p) {
     #pragma omp parallel for schedule(dynamic, 16) reduction(|:bad)
     for (int jj = 0; jj < c->nown[p]; ++jj) {
         const orec* r = &c->bc[c->own[p][jj]];
+        if (!OWN(c, r->b - 1)) continue;
         const orec* q = &c->bc[r->partner - 1];
         double bq = c->blk[q->b - 1].fam[p].beta[II(&c->blk[q->b - 1], q->i, q->j, q->k)];
         double bo = c->blk[r->b - 1].fam[p].beta[II(&c->blk[r->b - 1], r->i, r->j, r->k)];
@@ -751,9 +862,13 @@ static int compute_bound(orc_ctx* c, int p) {
         bad |= record_flux(c, r, fl, &bf);
         for (int v = 0; v < nc; ++v) c->connF[p][(long)(r->cf - 1)*NCM + v] = fl[v];
     }
+    /* a split run: the fluxes of connection faces whose partner another rank steps go to it */
+    if (bad) return bad;
+    if (halo_exchange(c, ICE_GPU_HALO_FLUX, p)) return -1;
     /* boundary cells, records in face order (bound_cell, Mod_BC_Fluxes.f90:105-144) */
     #pragma omp parallel for schedule(dynamic, 16) reduction(|:bad)
     for (int cc = 0; cc < c->bn[p]; ++cc) {
+        if (!OWN(c, c->bc[c->brec[p][c->bfirst[p][cc]]].b - 1)) continue;
         for (int rr = c->bfirst[p][cc]; rr < c->bfirst[p][cc + 1]; ++rr) {
             const orec* r = &c->bc[c->brec[p][rr]];
             oblk* B = &c->blk[r->b - 1];
@@ -803,6 +918,7 @@ static int face_flux(orc_ctx* c, oblk* B, int p, int d, int i, int j, int k, dou
 static int compute_flux(orc_ctx* c, int p) {
     int nc = nc_of(c, p), bad = 0;
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         int dim[3] = {B->ni, B->nj, B->nk};
@@ -842,6 +958,7 @@ static void compute_source(orc_ctx* c, int p) {
     int nc = nc_of(c, p);
     const ice_gpu_family* mat = &c->P.fam[p];
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         #pragma omp parallel for collapse(2) schedule(static)
@@ -862,6 +979,7 @@ static void compute_residual(orc_ctx* c, int p) {
     int nc = nc_of(c, p);
     const ice_gpu_family* mat = &c->P.fam[p];
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         #pragma omp parallel for schedule(static)
@@ -925,6 +1043,7 @@ static int state_update(orc_ctx* c, int p, int srk) {
     double rk = RKC[c->P.nrk - 1][srk - 1];
     long long nfl = 0;
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         #pragma omp parallel for collapse(2) schedule(static) reduction(|:bad) reduction(+:nfl)
@@ -952,6 +1071,7 @@ static void compute_dt(orc_ctx* c, int p) {
     int tau_limit = c->P.coupled && c->P.tau_factor > 0.0;
     double dtmin = DBL_MAX;
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         #pragma omp parallel for collapse(2) schedule(static) reduction(min:dtmin)
@@ -984,6 +1104,7 @@ static void compute_dt(orc_ctx* c, int p) {
  * Mod_Exchange.f90:270-390), (nc, ni, nj, nk); NULL zeroes the block's. The first call allocates the
  * family's arrays (zero in every block). */
 int orc_set_imports(orc_ctx* c, int b1, int p1, const double* imports) {
+    if (c->owned) return seterr(c, ICE_GPU_EINVAL, "set_imports: imports are not supported in a split run");
     if (b1 < 1 || b1 > c->nb || p1 < 1 || p1 > c->P.nfam) return seterr(c, ICE_GPU_EINVAL, "set_imports: bad block/family");
     int p = p1 - 1, nc = nc_of(c, p);
     oblk* Bq = &c->blk[b1 - 1];
@@ -1119,6 +1240,7 @@ static void add_stage_source(orc_ctx* c, int p, int srk) {
     int nc = nc_of(c, p);
     double ck = RKC[c->P.nrk - 1][srk - 1];
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         ofam* F = &B->fam[p];
         for (long q = 0; q < (long)nc*ncells(B); ++q)
@@ -1141,10 +1263,11 @@ int orc_exchange_rate(orc_ctx* c, int b1, int p1, double* x) {
 }
 
 /* --------------------------------------------------------------- norm */
-static void residual_norm(orc_ctx* c) {
+static int residual_norm(orc_ctx* c) {
     int nf = c->P.nfam;
     double* part = (double*)calloc((size_t)5*c->nb*nf, sizeof(double));
     for (int b = 0; b < c->nb; ++b) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         for (int p = 0; p < nf; ++p) {
             int nc = nc_of(c, p), iT = o_nbase(c->P.fam[p].closure) - 2;
@@ -1158,6 +1281,9 @@ static void residual_norm(orc_ctx* c) {
             }
         }
     }
+    /* a split run: every block's partial sums come from the one rank that steps it (the others add
+     * zeros), so the sums below keep the block order of an unsplit run */
+    if (halo_reduce(c, ICE_GPU_HALO_NORM, part, 5L*c->nb*nf)) { free(part); return ICE_GPU_EEXCH; }
     double tot[5] = {0, 0, 0, 0, 0};
     for (int b = 0; b < c->nb; ++b) for (int p = 0; p < nf; ++p) for (int m = 0; m < 5; ++m) tot[m] = tot[m] + part[5*((long)b*nf + p) + m];
     for (int m = 0; m < 5; ++m) c->residuo[m] = sqrt(tot[m]);
@@ -1168,10 +1294,11 @@ static void residual_norm(orc_ctx* c) {
     }
     free(part);
     c->have_norm = 1;
+    return 0;
 }
 
 int orc_residual_norm(orc_ctx* c, double* total, double* fam) {
-    residual_norm(c);
+    if (residual_norm(c)) return ICE_GPU_EEXCH;
     memcpy(total, c->residuo, sizeof(double)*5);
     if (fam) memcpy(fam, c->residuofam, sizeof(double)*5*c->P.nfam);
     return 0;
@@ -1186,14 +1313,17 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
     c->iter += 1; c->iter_from_call += 1;
     c->dtglobal = (double)1e+5f;
     for (int p = 0; p < nf; ++p) { compute_dt(c, p); bound_empty_dt(c, p); bound_removal_dt(c, p); }
+    if (halo_reduce(c, ICE_GPU_HALO_DT, &c->dtglobal, 1)) return ICE_GPU_EEXCH;
     if (c->P.time_accurate) {
         c->time = c->time + c->dtglobal;
         for (int b = 0; b < c->nb; ++b) for (int p = 0; p < nf; ++p) {
+            if (!OWN(c, b)) continue;
             oblk* B = &c->blk[b];
             for (long q = 0; q < ncells(B); ++q) B->fam[p].dt[q] = c->dtglobal;
         }
     }
     for (int b = 0; b < c->nb; ++b) for (int p = 0; p < nf; ++p) {
+        if (!OWN(c, b)) continue;
         oblk* B = &c->blk[b];
         int nc = nc_of(c, p);
         for (int k = 1; k <= B->nk; ++k) for (int j = 1; j <= B->nj; ++j) for (int i = 1; i <= B->ni; ++i)
@@ -1201,12 +1331,16 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
     }
     for (int p = 0; p < nf; ++p) {
         for (int srk = 1; srk <= c->P.nrk; ++srk) {
-            for (int b = 0; b < c->nb; ++b) memset(c->blk[b].fam[p].residual, 0, sizeof(double)*nc_of(c, p)*ncells(&c->blk[b]));
+            for (int b = 0; b < c->nb; ++b) if (OWN(c, b)) memset(c->blk[b].fam[p].residual, 0, sizeof(double)*nc_of(c, p)*ncells(&c->blk[b]));
             if (c->P.coupled) compute_source(c, p);
             if (c->P.coupled && c->exchange) add_stage_source(c, p, srk);
+            if (halo_exchange(c, ICE_GPU_HALO_CELLS, p)) return ICE_GPU_EEXCH;
             compute_ghost(c, p);
             compute_beta(c, p);
-            if (compute_bound(c, p)) { c->status |= ICE_GPU_ST_BAD_RECON; return ICE_GPU_ESTATE; }
+            if (halo_exchange(c, ICE_GPU_HALO_BETA, p)) return ICE_GPU_EEXCH;
+            int rb = compute_bound(c, p);
+            if (rb < 0) return ICE_GPU_EEXCH;
+            if (rb) { c->status |= ICE_GPU_ST_BAD_RECON; return ICE_GPU_ESTATE; }
             if (compute_flux(c, p)) { c->status |= ICE_GPU_ST_BAD_RECON; return ICE_GPU_ESTATE; }
             compute_residual(c, p);
             add_births(c, p);
@@ -1221,7 +1355,7 @@ static int explicit_step(orc_ctx* c, ice_gpu_step_out* out) {
     int need_norm = res_stop || due(c->iter, c->P.res_diter) || due(c->iter, c->P.shell_diter) ||
                     c->iter_from_call >= c->P.itermax || c->time >= c->P.time_threshold;
     c->have_norm = 0;
-    if (need_norm) residual_norm(c);
+    if (need_norm && residual_norm(c)) return ICE_GPU_EEXCH;
     if (res_stop && c->res_reference == 0.0) c->res_reference = c->residuo[0];
     c->res_end = res_stop && c->res_reference > 0.0 && c->residuo[0] <= c->P.res_threshold * c->res_reference;
     int endsim = c->iter_from_call >= c->P.itermax || c->res_end || c->time >= c->P.time_threshold;
