@@ -90,18 +90,21 @@ def algorithmic_bytes(case, precision: int = abi.PREC_FP64) -> float:
     stages: read U_(k-1) and U_0 and write U_k (24 nc, FP64 state); per direction the face normal and
     area (32) and the cell length (8) in FP64, or their single-precision copies (16 and 4) in the
     FP32-flux form; the volume (8); the boundary map (4); in a coupled run the nine
-    frozen-gas values the fused source reads (72) and the relaxation time it writes on the last stage
-    (8 / nrk), or, for an evaporating family of a 2-D or 3-D run, the source its own kernel wrote
-    (8 nc); the local dt (8) in steady mode; in 1-D runs the sensor weight (8) when the shock detector
+    frozen-gas values the fused source reads (72; 36 for their single-precision copy in the FP32-flux
+    form) and the relaxation time it writes on the last stage (8 / nrk), or, for an evaporating family
+    of a 2-D or 3-D run, the source its own kernel wrote (8 nc; 4 nc in single precision in the FP32-flux
+    form); the local dt (8) in steady mode; in 1-D runs the sensor weight (8) when the shock detector
     is on (2-D and 3-D runs evaluate it from the staged density)."""
     ndir = case.ndir
     nrk = case.params().nrk
     per = []
-    geo = 20 if precision == abi.PREC_FP32FLUX else 40
+    f32 = precision == abi.PREC_FP32FLUX
+    geo = 20 if f32 else 40
+    word = 4 if f32 else 8
     for f in case.families:
         b = 24 * f.nc + geo * ndir + 8 + 4
         if case.numerics.coupled:
-            b += 8 * f.nc if (ndir >= 2 and f.evap != "none") else 72 + 8 / nrk
+            b += word * f.nc if (ndir >= 2 and f.evap != "none") else 9 * word + 8 / nrk
         if case.numerics.shock_detector and ndir == 1:
             b += 8
         if not case.numerics.time_accurate:

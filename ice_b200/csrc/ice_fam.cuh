@@ -45,6 +45,7 @@ void launch_family_t(const LaunchArgs& a) {
     launch_source_of<CL>(a);
     tick(KC_SOURCE);
   }
+  if (a.xchg) a.xchg(a, ICE_GPU_HALO_CELLS);   // the remote source cells of the ghost layers
   if (a.nrec > 0) {
     if (a.ghost_split) {
       k_ghost<CL><<<grid(a.nrec, 128), 128, 0, s>>>(a.G, a.F, a.grecs, a.nrec, 1);
@@ -60,7 +61,8 @@ void launch_family_t(const LaunchArgs& a) {
     k_beta<<<grid(a.G.NI, 256), 256, 0, s>>>(a.G, a.F);
     tick(KC_BETA);
   }
-  if (a.nown > 0 || a.nbc > 0) {
+  if (a.xchg) a.xchg(a, ICE_GPU_HALO_BETA);    // the weights of partner cells another rank steps
+  if (a.nown > 0 || a.nbc > 0 || a.xchg) {
     launch_bound_of<CL>(a);
     tick(KC_BOUND);
   }

@@ -117,6 +117,7 @@ struct ice_gpu_ctx {
   DevBuf<double> face[3], vol, dl, M, gas;
   DevBuf<float4> facef[3];  // the FP32-flux form's geometry (Geo::ff, dlf), rounded from the FP64 arrays
   DevBuf<float> dlf;
+  DevBuf<float> gasf;       // the FP32-flux form's copy of the gas (Geo::gasf)
   bool geo32_ok = false;
   bool have_gas = false;
   std::vector<bool> have_block;
@@ -151,6 +152,20 @@ struct ice_gpu_ctx {
   double last_norm[5] = {0, 0, 0, 0, 0};
   bool profiling = false;
   double kms[KC_N] = {0};
+  // the block split (ice_gpu_set_partition, _set_halo, _set_exchange_hook): the blocks this rank steps
+  // (empty: all), on the device too; per kind and family the entries sent and received (0-based int4:
+  // block, i, j, k; or the connection face in x); the hook and its pinned host buffers
+  std::vector<unsigned char> owned;
+  DevBuf<unsigned char> owned_dev;
+  std::vector<int4> hs[3][kMaxF], hr[3][kMaxF];
+  DevBuf<int4> hs_dev[3][kMaxF], hr_dev[3][kMaxF];
+  ice_gpu_exchange_fn hook = nullptr;
+  void* hook_user = nullptr;
+  DevBuf<double> xdev;
+  double* xhost = nullptr;
+  size_t xhost_n = 0;
+  int xerr = 0;                  // the first failure of an exchange of the running call
+  unsigned long long xbits = 0;  // the reduced dt on its way back to the device
   long long nlaunch = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf<double> xfer;    // one block of one family in the caller's layout (upload/download)
@@ -244,6 +259,7 @@ static FamDev make_famdev(ice_gpu_ctx* c, int p, int srk, int phase) {
   F.dtg = &c->st.p->dtglobal;
   F.tau = H.tau.p;
   F.S = H.src.p;
+  F.Sf = c->P.precision == ICE_PREC_FP32FLUX ? (float*)H.src.p : nullptr;
   F.bmap = H.bmap.p;
   F.Rb = H.Rb.p; F.Rbw = H.Rb.p;
   F.connF = H.connF.p;
@@ -267,6 +283,8 @@ static Geo make_geo(ice_gpu_ctx* c) {
   G.vol = c->vol.p; G.dl = c->dl.p; G.M = c->M.p; G.gas = c->gas.p;
   for (int d = 0; d < 3; ++d) G.ff[d] = c->facef[d].p;
   G.dlf = c->dlf.p;
+  G.gasf = c->gasf.p;
+  G.owned = c->owned.empty() ? nullptr : c->owned_dev.p;
   return G;
 }
 
@@ -296,6 +314,11 @@ static int build_geo32(ice_gpu_ctx* c) {
   if (!c->dlf.p) { CK(c->dlf.alloc((size_t)3 * c->NR)); fresh = true; }
   k_dl32<<<grid_of(3 * c->NR), 256, 0, c->stream>>>(c->dl.p, 3 * c->NR, c->dlf.p);
   CK(cudaGetLastError());
+  if (c->P.coupled && c->gas.p) {
+    if (!c->gasf.p) { CK(c->gasf.alloc((size_t)9 * c->NI)); fresh = true; }
+    k_dl32<<<grid_of(9 * c->NI), 256, 0, c->stream>>>(c->gas.p, 9 * c->NI, c->gasf.p);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(c->stream));
   if (fresh) free_graphs(c);          // graphs captured before the buffers existed hold null pointers
   c->geo32_ok = true;
@@ -304,6 +327,108 @@ static int build_geo32(ice_gpu_ctx* c) {
 
 // ---------------------------------------------------------------- kernel dispatch
 #define GRID(n, t) ((unsigned)(((n) + (t) - 1) / (t)))
+
+// ---------------------------------------------------------------- the block split's exchanges
+// Pack and unpack of the exchange lists (0-based int4 entries: block, i, j, k; a connection face in x).
+__global__ void k_pack_cells(Geo G, const double* __restrict__ U, int nc, const int4* __restrict__ e, int n,
+                             double* __restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int4 x = e[q];
+  const long long g = gidx(G.blk[x.x], x.y, x.z, x.w);
+  for (int v = 0; v < nc; ++v) out[(long long)q * nc + v] = U[(long long)v * G.NG + g];
+}
+__global__ void k_unpack_cells(Geo G, double* __restrict__ U, int nc, const int4* __restrict__ e, int n,
+                               const double* __restrict__ in) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int4 x = e[q];
+  const long long g = gidx(G.blk[x.x], x.y, x.z, x.w);
+  for (int v = 0; v < nc; ++v) U[(long long)v * G.NG + g] = in[(long long)q * nc + v];
+}
+__global__ void k_unpack_beta(Geo G, double* __restrict__ beta, const int4* __restrict__ e, int n,
+                              const double* __restrict__ in) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int4 x = e[q];
+  beta[iidx(G.blk[x.x], x.y, x.z, x.w)] = in[q];
+}
+__global__ void k_pack_flux(const double* __restrict__ F, int nc, const int4* __restrict__ e, int n,
+                            double* __restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  for (int v = 0; v < nc; ++v) out[(long long)q * nc + v] = F[(long long)e[q].x * nc + v];
+}
+__global__ void k_unpack_flux(double* __restrict__ F, int nc, const int4* __restrict__ e, int n,
+                              const double* __restrict__ in) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  for (int v = 0; v < nc; ++v) F[(long long)e[q].x * nc + v] = in[(long long)q * nc + v];
+}
+
+static int ensure_xbuf(ice_gpu_ctx* c, size_t n) {
+  if (c->xdev.n < n) CK(c->xdev.alloc(n));
+  if (c->xhost_n < n) {
+    if (c->xhost) cudaFreeHost(c->xhost);
+    c->xhost = nullptr; c->xhost_n = 0;
+    CK(cudaMallocHost((void**)&c->xhost, n * sizeof(double)));
+    c->xhost_n = n;
+  }
+  return 0;
+}
+
+// One exchange of a split step (Mod_GhostExchange.f90:737-800 for the cells), at its point of the
+// family's stage: pack on the device, copy to the host, the hook, copy back, unpack. The stream is
+// drained before the hook, so the hook sees this stage's data and no kernel waits on another rank.
+// The first failure is kept (xerr) and reported by the step; later exchanges of the call are skipped.
+static void halo_xchg(const LaunchArgs& a, int kind) {
+  ice_gpu_ctx* c = (ice_gpu_ctx*)a.tick_ctx;
+  if (c->xerr) return;
+  const int p = a.fam, nc = c->fam[p].nc, w = kind == ICE_GPU_HALO_BETA ? 1 : nc;
+  const int ns = (int)c->hs[kind][p].size(), nr = (int)c->hr[kind][p].size();
+  const size_t ls = (size_t)ns * w, lr = (size_t)nr * w;
+  if (ensure_xbuf(c, ls + lr + 1)) { c->xerr = ICE_GPU_ECUDA; return; }
+  double* ds = c->xdev.p; double* dr = c->xdev.p + ls;
+  const int4* es = c->hs_dev[kind][p].p; const int4* er = c->hr_dev[kind][p].p;
+  if (ns > 0) {
+    if (kind == ICE_GPU_HALO_CELLS) k_pack_cells<<<GRID(ns, 128), 128, 0, a.s>>>(a.G, a.F.Up, nc, es, ns, ds);
+    else if (kind == ICE_GPU_HALO_FLUX) k_pack_flux<<<GRID(ns, 128), 128, 0, a.s>>>(a.F.connF, nc, es, ns, ds);
+    else {
+      // in the translation unit of the closure's connection kernel, compiled as it is, for its bits
+      const int cl = c->fam[p].closure;
+      const bool f32 = a.precision == ICE_PREC_FP32FLUX;
+      if (cl == ICE_CLOSURE_MK) (f32 ? launch_pack_beta_mk_f32 : launch_pack_beta_mk_f64)(a, es, ns, ds);
+      else if (cl == ICE_CLOSURE_IG) (f32 ? launch_pack_beta_ig_f32 : launch_pack_beta_ig_f64)(a, es, ns, ds);
+      else (f32 ? launch_pack_beta_ag_f32 : launch_pack_beta_ag_f64)(a, es, ns, ds);
+    }
+    cudaMemcpyAsync(c->xhost, ds, ls * sizeof(double), cudaMemcpyDeviceToHost, a.s);
+  }
+  if (cudaStreamSynchronize(a.s) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    c->xerr = ICE_GPU_ECUDA; fail(c, ICE_GPU_ECUDA, "split exchange: a CUDA error before the hook");
+    return;
+  }
+  if (!c->hook) { c->xerr = ICE_GPU_ENOTREADY; fail(c, ICE_GPU_ENOTREADY, "a split run needs its exchange hook"); return; }
+  if (c->hook(c->hook_user, kind, p + 1, (int64_t)ls, c->xhost, (int64_t)lr, c->xhost + ls) != 0) {
+    c->xerr = ICE_GPU_EEXCH; fail(c, ICE_GPU_EEXCH, "the exchange hook failed (kind %d, family %d)", kind, p + 1);
+    return;
+  }
+  if (nr > 0) {
+    cudaMemcpyAsync(dr, c->xhost + ls, lr * sizeof(double), cudaMemcpyHostToDevice, a.s);
+    if (kind == ICE_GPU_HALO_CELLS) k_unpack_cells<<<GRID(nr, 128), 128, 0, a.s>>>(a.G, a.F.Ug, nc, er, nr, dr);
+    else if (kind == ICE_GPU_HALO_FLUX) k_unpack_flux<<<GRID(nr, 128), 128, 0, a.s>>>(a.F.connF, nc, er, nr, dr);
+    else k_unpack_beta<<<GRID(nr, 128), 128, 0, a.s>>>(a.G, a.F.betaw, er, nr, dr);
+  }
+}
+
+// The reductions of a split run: the minimum (DT) or the sum (NORM) over the ranks of n doubles.
+static int halo_reduce(ice_gpu_ctx* c, int kind, double* x, long long n) {
+  if (c->owned.empty()) return 0;
+  if (!c->hook) return fail(c, ICE_GPU_ENOTREADY, "a split run needs its exchange hook (ice_gpu_set_exchange_hook)");
+  std::vector<double> in(x, x + n);
+  if (c->hook(c->hook_user, kind, 0, n, in.data(), n, x) != 0)
+    return fail(c, ICE_GPU_EEXCH, "the exchange hook failed (kind %d)", kind);
+  return 0;
+}
 
 static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_t s,
                           void (*tick)(void*, int, cudaStream_t)) {
@@ -325,6 +450,8 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   a.st = c->st.p;
   a.s = s;
   a.tick = tick; a.tick_ctx = c;
+  a.xchg = c->owned.empty() ? nullptr : halo_xchg;
+  a.fam = p;
   if (H.closure == ICE_CLOSURE_MK) launch_family_mk(a);
   else if (H.closure == ICE_CLOSURE_IG) launch_family_ig(a);
   else launch_family_ag(a);
@@ -377,6 +504,22 @@ static void enqueue_step_dt(ice_gpu_ctx* c, int phase, cudaStream_t s, void (*ti
     k_dt_all<<<GRID(c->NI, 256), 256, 0, s>>>(make_geo(c), a, c->st.p);
   }
   for (int p = 0; p < c->P.nfam; ++p) launch_dt_bounds(c, p, phase, s);
+  if (!c->owned.empty() && !c->xerr) {
+    // a split run: the step's dt is the smallest over every rank (Mod_Explicit.f90:67-73)
+    unsigned long long bits = 0;
+    if (cudaMemcpyAsync(&bits, &c->st.p->dtbits, sizeof bits, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      c->xerr = ICE_GPU_ECUDA; fail(c, ICE_GPU_ECUDA, "split exchange: reading the dt");
+    } else {
+      double d;
+      memcpy(&d, &bits, sizeof d);
+      if (halo_reduce(c, ICE_GPU_HALO_DT, &d, 1)) c->xerr = ICE_GPU_EEXCH;
+      memcpy(&bits, &d, sizeof d);
+      c->xbits = bits;
+      cudaMemcpyAsync(&c->st.p->dtbits, &c->xbits, sizeof bits, cudaMemcpyHostToDevice, s);
+      cudaStreamSynchronize(s);
+    }
+  }
   k_time<<<1, 1, 0, s>>>(c->st.p, c->P.time_accurate);
   if (tick) tick(c, KC_DT, s);
 }
@@ -526,6 +669,7 @@ static int build_tiles(ice_gpu_ctx* c) {
   std::vector<Tile> t;
   if (c->P.ndir == 1) {
     for (int b = 0; b < c->nb; ++b) {
+      if (!c->owned.empty() && !c->owned[b]) continue;       // a split run steps its own blocks
       int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
       int sx = ni >= 2 ? c->TX - 1 : 1, sy = nj >= 2 ? std::max(c->TY - 1, 1) : 1;
       for (int k = 0; k < nk; k += c->KZ)
@@ -553,6 +697,7 @@ static int build_tiles(ice_gpu_ctx* c) {
       for (int b = 0; b < c->nb; ++b) H.shape3[b] = tile_shape3(c->dims[3 * b], c->dims[3 * b + 1], H.closure);
       const int kz = choose_kz(c, H, slots);
       for (int b = 0; b < c->nb; ++b) {
+        if (!c->owned.empty() && !c->owned[b]) continue;     // a split run steps its own blocks
         int ni = c->dims[3 * b], nj = c->dims[3 * b + 1], nk = c->dims[3 * b + 2];
         const Tile& sp = H.shape3[b];
         int nch = (nk + kz - 1) / kz, base = nk / nch, extra = nk % nch;
@@ -728,6 +873,7 @@ int ice_gpu_destroy(ice_gpu_ctx* c) {
   if (c->s_up) { cudaStreamSynchronize(c->s_up); cudaStreamDestroy(c->s_up); }
   if (c->s_down) { cudaStreamSynchronize(c->s_down); cudaStreamDestroy(c->s_down); }
   if (c->ev_up) cudaEventDestroy(c->ev_up);
+  if (c->xhost) cudaFreeHost(c->xhost);
   for (auto& e : c->ev_fam) if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -795,6 +941,7 @@ int ice_gpu_set_gas(ice_gpu_ctx* c, int32_t b1, const double* prim5, const doubl
   for (int comp = 0; comp < 4; ++comp)
     CK(cudaMemcpy(c->gas.p + (long long)(5 + comp) * c->NI + B.ioff, rest[comp], n * sizeof(double), cudaMemcpyHostToDevice));
   c->gas_set[b1 - 1] = true;
+  c->geo32_ok = false;                 // the FP32-flux form's copy of the gas is made again
   c->have_gas = std::all_of(c->gas_set.begin(), c->gas_set.end(), [](bool x) { return x; });
   return 0;
 }
@@ -1226,6 +1373,15 @@ int ice_gpu_step(ice_gpu_ctx* c, int32_t nsteps, ice_gpu_step_out* out) {
       CK(cudaEventRecord(c->ev0, s));
       enqueue_step(c, ph, s, prof_tick);
       c->nlaunch += launches_per_step(c);
+    } else if (!c->owned.empty()) {
+      // a split run: launched as it goes, the stream drained at each exchange for the hook
+      c->xerr = 0;
+      enqueue_step(c, ph, s, nullptr);
+      if (c->xerr) {
+        cudaStreamSynchronize(s);
+        cudaEventDestroy(t0); cudaEventDestroy(t1);
+        return c->xerr;
+      }
     } else {
       if (!c->graph[ph]) {
         cudaGraph_t g;
@@ -1293,6 +1449,7 @@ int ice_gpu_step_host(ice_gpu_ctx* c, int32_t nsteps, const double* const* prim_
   if (int rc = build_geo32(c)) return rc;
   if (nsteps < 1) return fail(c, ICE_GPU_EINVAL, "step_host: nsteps %d", nsteps);
   if (!prim_in || !prim_out) return fail(c, ICE_GPU_EINVAL, "step_host: null array list");
+  if (!c->owned.empty()) return fail(c, ICE_GPU_EINVAL, "step_host: a split run steps through ice_gpu_step");
   const int nf = c->P.nfam;
   for (int q = 0; q < c->nb * nf; ++q)
     if (!prim_in[q] || !prim_out[q]) return fail(c, ICE_GPU_EINVAL, "step_host: null array for block %d family %d",
@@ -1413,10 +1570,14 @@ int ice_gpu_residual_norm(ice_gpu_ctx* c, double* total, double* fam) {
     CK(cudaMemcpyAsync(h.data(), c->npart.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (int q = 0; q < c->nchunk; ++q) {
+      if (!c->owned.empty() && !c->owned[c->chunk_block[q]]) continue;    // another rank's block
       double* a = &part[((size_t)c->chunk_block[q] * nf + p) * 5];
       for (int m = 0; m < 5; ++m) a[m] = a[m] + h[(size_t)q * 5 + m];
     }
   }
+  // a split run: every block's partial sums come from the one rank that steps it (the others add
+  // zeros), so the sums below keep the block order of an unsplit run
+  if (int rc = halo_reduce(c, ICE_GPU_HALO_NORM, part.data(), (long long)part.size())) return rc;
   double tot[5] = {0, 0, 0, 0, 0};
   for (int b = 0; b < c->nb; ++b) for (int p = 0; p < nf; ++p) for (int m = 0; m < 5; ++m) tot[m] = tot[m] + part[((size_t)b * nf + p) * 5 + m];
   for (int m = 0; m < 5; ++m) total[m] = sqrt(tot[m]);
@@ -1427,6 +1588,72 @@ int ice_gpu_residual_norm(ice_gpu_ctx* c, double* total, double* fam) {
       for (int m = 0; m < 5; ++m) fam[p * 5 + m] = sqrt(f[m]);
     }
   }
+  return 0;
+}
+
+// ---------------------------------------------------------------- the block split
+int ice_gpu_set_partition(ice_gpu_ctx* c, const int32_t* owned) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (!owned) {
+    c->owned.clear();
+  } else {
+    if (c->P.irs) return fail(c, ICE_GPU_EINVAL, "set_partition: IRS is not supported in a split run");
+    if (c->nchim > 0) return fail(c, ICE_GPU_EINVAL, "set_partition: chimera records are not supported in a split run");
+    for (int p = 0; p < c->P.nfam; ++p)
+      if (c->fam[p].have_imp) return fail(c, ICE_GPU_EINVAL, "set_partition: imports are not supported in a split run");
+    std::vector<unsigned char> o(c->nb);
+    int n = 0;
+    for (int b = 0; b < c->nb; ++b) { o[b] = owned[b] != 0; n += o[b]; }
+    if (n == 0) return fail(c, ICE_GPU_EINVAL, "set_partition: this rank steps no block");
+    c->owned = o;
+    CK(c->owned_dev.alloc(c->nb));
+    CK(cudaMemcpy(c->owned_dev.p, o.data(), c->nb, cudaMemcpyHostToDevice));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  free_graphs(c);
+  if (build_tiles(c)) return ICE_GPU_ECUDA;
+  return 0;
+}
+
+int ice_gpu_set_halo(ice_gpu_ctx* c, int32_t kind, int32_t p1, int32_t nsend, const int32_t* send, int32_t nrecv,
+                     const int32_t* recv) {
+  if (!c) return ICE_GPU_EINVAL;
+  if (kind < 0 || kind > 2 || p1 < 1 || p1 > c->P.nfam || nsend < 0 || nrecv < 0 || (nsend > 0 && !send) ||
+      (nrecv > 0 && !recv))
+    return fail(c, ICE_GPU_EINVAL, "set_halo: bad arguments");
+  const int p = p1 - 1;
+  std::vector<int4> lists[2];
+  for (int side = 0; side < 2; ++side) {
+    const int n = side ? nrecv : nsend;
+    const int32_t* e = side ? recv : send;
+    for (int q = 0; q < n; ++q) {
+      const int32_t* x = e + 4 * q;
+      if (kind == ICE_GPU_HALO_FLUX) {
+        if (x[0] < 1 || x[0] > c->fam[p].ncf) return fail(c, ICE_GPU_EINVAL, "set_halo: connection face %d", x[0]);
+        lists[side].push_back(make_int4(x[0] - 1, 0, 0, 0));
+        continue;
+      }
+      if (x[0] < 1 || x[0] > c->nb) return fail(c, ICE_GPU_EINVAL, "set_halo: block %d", x[0]);
+      const int* d = &c->dims[3 * (x[0] - 1)];
+      if (x[1] < 1 || x[1] > d[0] || x[2] < 1 || x[2] > d[1] || x[3] < 1 || x[3] > d[2])
+        return fail(c, ICE_GPU_EINVAL, "set_halo: cell %d %d %d outside block %d", x[1], x[2], x[3], x[0]);
+      lists[side].push_back(make_int4(x[0] - 1, x[1] - 1, x[2] - 1, x[3] - 1));
+    }
+  }
+  c->hs[kind][p] = lists[0];
+  c->hr[kind][p] = lists[1];
+  CK(c->hs_dev[kind][p].alloc(lists[0].size()));
+  CK(c->hr_dev[kind][p].alloc(lists[1].size()));
+  if (!lists[0].empty())
+    CK(cudaMemcpy(c->hs_dev[kind][p].p, lists[0].data(), lists[0].size() * sizeof(int4), cudaMemcpyHostToDevice));
+  if (!lists[1].empty())
+    CK(cudaMemcpy(c->hr_dev[kind][p].p, lists[1].data(), lists[1].size() * sizeof(int4), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int ice_gpu_set_exchange_hook(ice_gpu_ctx* c, ice_gpu_exchange_fn fn, void* user) {
+  if (!c) return ICE_GPU_EINVAL;
+  c->hook = fn; c->hook_user = user;
   return 0;
 }
 

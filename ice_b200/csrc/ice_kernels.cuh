@@ -216,8 +216,9 @@ __device__ __forceinline__ double family_dt(const Geo& G, const DtFam& f, const 
 __global__ void __launch_bounds__(256) k_dt_all(Geo G, DtArgs a, Status* st) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double dt = INFINITY;
-  if (q < G.NI) {
-    const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  const int bq = q < G.NI ? find_block(G.blk, G.nb, q) : 0;
+  if (q < G.NI && stepped(G, bq)) {
+    const DBlock& B = G.blk[bq];
     const unsigned l = (unsigned)(q - B.ioff), ni = (unsigned)B.ni, nj = (unsigned)B.nj;
     const unsigned i = l % ni, jk = l / ni, j = jk % nj, k = jk / nj;
     const long long g = gidx(B, (int)i, (int)j, (int)k);
@@ -576,21 +577,35 @@ __global__ void k_ghost(Geo G, FamDev F, const DRec* recs, int nrec, int layers)
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nrec) return;
   const DRec r = recs[n];
+  if (!stepped(G, r.b)) return;
   if (layers & 1) ghost1_rec<CL>(G, F, r);
   if (layers & 2) ghost2_rec<CL>(G, F, r);
 }
 
 // ------------------------------------------------------------------ boundary fluxes
+// A split run's BETA exchange: the Jameson weight of each listed cell (0-based block, i, j, k), as the
+// connection kernel of the same precision and translation unit evaluates it (k_conn).
+template <typename R>
+__global__ void k_pack_beta(Geo G, FamDev F, const int4* __restrict__ e, int n, double* __restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int4 x = e[q];
+  out[q] = F.sd ? (double)beta_cell<R>(F, G.blk[x.x], x.y, x.z, x.w) : 1.0;
+}
+
 template <int CL, int RS, int LIM, typename R>
 __global__ void __launch_bounds__(128, 4) k_conn(Geo G, FamDev F, const DRec* recs, const int* own, int nown, Status* st) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nown) return;
   constexpr int nc = NC<CL>::v;
   const DRec& r = recs[own[n]];
+  if (!stepped(G, r.b)) return;
   R bo = (R)1, bq = (R)1;
   if (F.sd) {
     bo = beta_cell<R>(F, G.blk[r.b], r.i, r.j, r.k);
-    bq = beta_cell<R>(F, G.blk[r.pb], r.pi, r.pj, r.pk);
+    // a partner in a block another rank steps: its weight, which that rank sent (ICE_GPU_HALO_BETA)
+    bq = stepped(G, r.pb) ? beta_cell<R>(F, G.blk[r.pb], r.pi, r.pj, r.pk)
+                          : (R)F.beta[iidx(G.blk[r.pb], r.pi, r.pj, r.pk)];
   }
   const double bf = (double)mn(bo, bq);
   double fl[nc];
@@ -604,6 +619,7 @@ __global__ void __launch_bounds__(128, 4) k_bound(Geo G, FamDev F, const DRec* r
                                                   int nbc, Status* st) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nbc) return;
+  if (!stepped(G, recs[list[first[c]]].b)) return;
   constexpr int nc = NC<CL>::v;
   double acc[nc];
 #pragma unroll
@@ -636,19 +652,28 @@ __global__ void __launch_bounds__(256) k_source(Geo G, FamDev F) {
   constexpr int nc = NC<CL>::v;
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= G.NI) return;
-  const DBlock& B = G.blk[find_block(G.blk, G.nb, q)];
+  const int bq = find_block(G.blk, G.nb, q);
+  if (!stepped(G, bq)) return;
+  const DBlock& B = G.blk[bq];
   const unsigned l = (unsigned)(q - B.ioff), ni = (unsigned)B.ni, nj = (unsigned)B.nj;   // < 2^31 cells a block
   const unsigned i = l % ni, jk = l / ni, j = jk % nj, k = jk / nj;
   const long long g = gidx(B, (int)i, (int)j, (int)k);
   R p[nc], gas[5], s[nc];
 #pragma unroll
   for (int v = 0; v < nc; ++v) p[v] = (R)F.Up[(long long)v * G.NG + g];
+  R gr[9];
 #pragma unroll
-  for (int v = 0; v < 5; ++v) gas[v] = (R)G.gas[(long long)v * G.NI + q];
-  R tau = cell_source<CL, R>(p, gas, (R)G.gas[5 * G.NI + q], (R)G.gas[6 * G.NI + q], (R)G.gas[7 * G.NI + q],
-                             (R)G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, s);
+  for (int v = 0; v < 9; ++v) gr[v] = sizeof(R) == 4 ? (R)G.gasf[(long long)v * G.NI + q] : (R)G.gas[(long long)v * G.NI + q];
 #pragma unroll
-  for (int v = 0; v < nc; ++v) F.S[(long long)v * G.NI + q] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)s[v];
+  for (int v = 0; v < 5; ++v) gas[v] = gr[v];
+  R tau = cell_source<CL, R>(p, gas, gr[5], gr[6], gr[7], gr[8], F.mat, F.drag, F.heat, F.blow, s);
+  if constexpr (sizeof(R) == 4) {
+#pragma unroll
+    for (int v = 0; v < nc; ++v) F.Sf[(long long)v * G.NI + q] = (F.frozen_mask & (1u << v)) ? 0.f : s[v];
+  } else {
+#pragma unroll
+    for (int v = 0; v < nc; ++v) F.S[(long long)v * G.NI + q] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)s[v];
+  }
   if (F.write_tau) F.tau[q] = (double)tau;
 }
 
@@ -784,7 +809,8 @@ k_stage(Geo G, FamDev F, const Tile* tiles, int TX, int TY, int KZ, int write_r,
       for (int v = 0; v < nc; ++v) p[v] = F.Up[(long long)v * G.NG + g];
       double s[nc];
 #pragma unroll
-      for (int v = 0; v < nc; ++v) s[v] = F.coupled ? F.S[(long long)v * G.NI + q] : 0.0;
+      for (int v = 0; v < nc; ++v)
+        s[v] = !F.coupled ? 0.0 : F.Sf ? (double)F.Sf[(long long)v * G.NI + q] : F.S[(long long)v * G.NI + q];
       if (F.xstep) accumulate_source<CL>(F.xstep, G.NI, q, s, F.xfirst, F.rk);
       const double dt = F.dt ? F.dt[q] : *F.dtg;
       const double vol = G.vol[q];

@@ -33,7 +33,12 @@ struct Geo {                 // geometry shared by the families
   // of the cell lengths, rounded once from the FP64 arrays above (null in the plain form)
   const float4* ff[3];
   const float* dlf;
+  const float* gasf;         // the FP32-flux form's copy of the frozen gas (coupled runs), rounded once
+  // a split run (ice_gpu_set_partition): per block, whether this rank steps it; null when it steps all
+  const unsigned char* owned;
 };
+__device__ __forceinline__ bool stepped(const Geo& G, int b) { return !G.owned || G.owned[b]; }
+
 
 struct DRec {                // one boundary record, 0-based cells
   int b, i, j, k, f, type;
@@ -97,6 +102,7 @@ struct FamDev {              // what the kernels of one family read
   const double* dtg;         // &status->dtglobal (time-accurate)
   double* tau;               // NI
   double* S;                 // [v][NI]: the stage's source (coupled runs)
+  float* Sf;                 // the FP32-flux form's source, [v][NI] floats in the same buffer (else null)
   const int* bmap;           // NI: boundary-cell index or -1
   const double* Rb;          // [nbcell][nc]
   double* Rbw;
@@ -148,6 +154,10 @@ struct LaunchArgs {
   cudaStream_t s;
   void (*tick)(void*, int, cudaStream_t);
   void* tick_ctx;
+  // a split run: the exchange of one kind (ICE_GPU_HALO_CELLS, BETA, FLUX) of this family at its point
+  // of the stage, called on every rank whatever its local work (null when every block is stepped here)
+  void (*xchg)(const struct LaunchArgs&, int kind);
+  int fam;                                           // 0-based family
 };
 
 enum { KC_DT = 0, KC_GHOST, KC_BETA, KC_BOUND, KC_STAGE, KC_IRS, KC_NORM, KC_SOURCE, KC_N };
@@ -169,6 +179,12 @@ void launch_bound_ig_f64(const LaunchArgs& a);
 void launch_bound_ig_f32(const LaunchArgs& a);
 void launch_bound_ag_f64(const LaunchArgs& a);
 void launch_bound_ag_f32(const LaunchArgs& a);
+void launch_pack_beta_mk_f64(const LaunchArgs& a, const int4* e, int n, double* out);
+void launch_pack_beta_mk_f32(const LaunchArgs& a, const int4* e, int n, double* out);
+void launch_pack_beta_ig_f64(const LaunchArgs& a, const int4* e, int n, double* out);
+void launch_pack_beta_ig_f32(const LaunchArgs& a, const int4* e, int n, double* out);
+void launch_pack_beta_ag_f64(const LaunchArgs& a, const int4* e, int n, double* out);
+void launch_pack_beta_ag_f32(const LaunchArgs& a, const int4* e, int n, double* out);
 void launch_stage_mk_f64(const LaunchArgs& a, bool write_r);
 void launch_stage_mk_f32(const LaunchArgs& a, bool write_r);
 void launch_stage_ig_f64(const LaunchArgs& a, bool write_r);

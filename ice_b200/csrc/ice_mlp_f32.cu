@@ -255,9 +255,9 @@ k_source_mlp(Geo G, FamDev F, const unsigned char* __restrict__ img, MlpNorm nm,
 #pragma unroll
       for (int v = 0; v < nc; ++v) p[v] = (float)F.Up[(long long)v * G.NG + g];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) gas[v] = (float)G.gas[(long long)v * G.NI + q];
-      gR = (float)G.gas[5 * G.NI + q]; gg = (float)G.gas[6 * G.NI + q];
-      gk = (float)G.gas[7 * G.NI + q]; gm = (float)G.gas[8 * G.NI + q];
+      for (int v = 0; v < 5; ++v) gas[v] = G.gasf[(long long)v * G.NI + q];
+      gR = G.gasf[5 * G.NI + q]; gg = G.gasf[6 * G.NI + q];
+      gk = G.gasf[7 * G.NI + q]; gm = G.gasf[8 * G.NI + q];
       c = cell_phys<CL, float>(p, gas, gR, gg, gk, gm, F.mat, F.drag, F.heat);
       float f[MLP_IN];
       mlp_features<float>(c.Rp, c.T, gas[4], c.du, yinf, gas[0] * gR * gas[4], c.Re, f);
@@ -285,7 +285,7 @@ k_source_mlp(Geo G, FamDev F, const unsigned char* __restrict__ img, MlpNorm nm,
       float s[nc];
       const float tau = cell_source_finish<CL, float>(c, p, gas, F.mat, md, Q, s);
 #pragma unroll
-      for (int v = 0; v < nc; ++v) F.S[(long long)v * G.NI + q] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)s[v];
+      for (int v = 0; v < nc; ++v) F.Sf[(long long)v * G.NI + q] = (F.frozen_mask & (1u << v)) ? 0.f : s[v];
       if (F.write_tau) F.tau[q] = (double)tau;
     }
     // per warp: cells, envelope fallbacks, check fallbacks

@@ -44,6 +44,7 @@ template <int CL, int RS, int LIM, typename R>
 void launch_bound_k(const LaunchArgs& a) {
   auto grid = [](long long n, int t) { return (unsigned)((n + t - 1) / t); };
   if (a.nown > 0) k_conn<CL, RS, LIM, R><<<grid(a.nown, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.own, a.nown, a.st);
+  if (a.xchg) a.xchg(a, ICE_GPU_HALO_FLUX);    // connection fluxes to the partners another rank steps
   if (a.nbc > 0)
     k_bound<CL, RS, LIM, R><<<grid(a.nbc, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.bfirst, a.blist, a.nbc, a.st);
 }
@@ -62,6 +63,11 @@ void launch_bound_t(const LaunchArgs& a) {
   }
   if (a.F.riemann == ICE_RIEMANN_HLLE) launch_bound_l<CL, ICE_RIEMANN_HLLE, R>(a);
   else launch_bound_l<CL, ICE_RIEMANN_RUSANOV, R>(a);
+}
+
+template <typename R>
+void launch_pack_beta_t(const LaunchArgs& a, const int4* e, int n, double* out) {
+  k_pack_beta<R><<<(unsigned)((n + 127) / 128), 128, 0, a.s>>>(a.G, a.F, e, n, out);
 }
 
 template <int CL, typename R>

@@ -471,15 +471,18 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       for (int v = 0; v < nc; ++v) s[v] = 0.0;
       if (F.coupled && F.src_ready) {           // a source kernel ran first (evaporating family or surrogate)
 #pragma unroll
-        for (int v = 0; v < nc; ++v) s[v] = F.S[(long long)v * G.NI + q];
+        for (int v = 0; v < nc; ++v) s[v] = F.Sf ? (double)F.Sf[(long long)v * G.NI + q] : F.S[(long long)v * G.NI + q];
       } else if (F.coupled) {                   // compute_source_ on the stage's state
         R pr_[nc], gas[5], sr[nc];
 #pragma unroll
         for (int v = 0; v < nc; ++v) pr_[v] = (R)p[v];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) gas[v] = (R)G.gas[(long long)v * G.NI + q];
-        R tau = cell_source<CL, R>(pr_, gas, (R)G.gas[5 * G.NI + q], (R)G.gas[6 * G.NI + q], (R)G.gas[7 * G.NI + q],
-                                   (R)G.gas[8 * G.NI + q], F.mat, F.drag, F.heat, F.blow, sr);
+        R gr[9];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) gr[v] = sizeof(R) == 4 ? (R)G.gasf[(long long)v * G.NI + q] : (R)G.gas[(long long)v * G.NI + q];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) gas[v] = gr[v];
+        R tau = cell_source<CL, R>(pr_, gas, gr[5], gr[6], gr[7], gr[8], F.mat, F.drag, F.heat, F.blow, sr);
 #pragma unroll
         for (int v = 0; v < nc; ++v) s[v] = (F.frozen_mask & (1u << v)) ? 0.0 : (double)sr[v];
         if (F.write_tau) F.tau[q] = (double)tau;

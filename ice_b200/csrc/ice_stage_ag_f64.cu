@@ -4,4 +4,7 @@ namespace ice {
 void launch_stage_ag_f64(const LaunchArgs& a, bool write_r) { launch_stage_t<AG, double>(a, write_r); }
 void launch_source_ag_f64(const LaunchArgs& a) { launch_source_t<AG, double>(a); }
 void launch_bound_ag_f64(const LaunchArgs& a) { launch_bound_t<AG, double>(a); }
+void launch_pack_beta_ag_f64(const LaunchArgs& a, const int4* e, int n, double* out) {
+  launch_pack_beta_t<double>(a, e, n, out);
+}
 }  // namespace ice

@@ -13,7 +13,11 @@ module ice_gpu
   integer(c_int32_t), parameter, public :: ICE_GPU_MAX_FAMILIES = 4, ICE_GPU_NCOND_MAX = 12, ICE_GPU_NEP = 8
   integer(c_int32_t), parameter, public :: ICE_GPU_REC_INTS = 15, ICE_GPU_REC_REALS = 8
   integer(c_int),     parameter, public :: ICE_GPU_OK = 0, ICE_GPU_EINVAL = 1, ICE_GPU_ECUDA = 2, &
-                                           ICE_GPU_ESTATE = 3, ICE_GPU_ENOMEM = 4, ICE_GPU_ENOTREADY = 5
+                                           ICE_GPU_ESTATE = 3, ICE_GPU_ENOMEM = 4, ICE_GPU_ENOTREADY = 5, &
+                                           ICE_GPU_EEXCH = 6
+  !> the kinds of a split run's exchanges (ice_gpu_set_halo, the exchange hook)
+  integer(c_int32_t), parameter, public :: ICE_GPU_HALO_CELLS = 0, ICE_GPU_HALO_BETA = 1, ICE_GPU_HALO_FLUX = 2, &
+                                           ICE_GPU_HALO_DT = 3, ICE_GPU_HALO_NORM = 4
 
   type, bind(C), public :: ice_gpu_family_t
     integer(c_int32_t) :: closure, riemann, nfrozen
@@ -47,7 +51,8 @@ module ice_gpu
             ice_gpu_upload_state, &
             ice_gpu_download_state, ice_gpu_set_time, ice_gpu_set_res_reference, ice_gpu_get_res_reference, &
             ice_gpu_step, ice_gpu_residual_norm, ice_gpu_update_params, &
-            ice_gpu_last_error, ice_gpu_destroy, ice_gpu_pair_connections
+            ice_gpu_last_error, ice_gpu_destroy, ice_gpu_pair_connections, &
+            ice_gpu_set_partition, ice_gpu_set_halo, ice_gpu_set_exchange_hook
 
   interface
     integer(c_int) function ice_gpu_create(params, nblocks, dims, ctx) bind(C, name='ice_gpu_create')
@@ -190,6 +195,31 @@ module ice_gpu
       integer(c_int32_t), intent(in)       :: dims(*)
       integer(c_int32_t), intent(inout)    :: rec(*)
       character(kind=c_char), intent(out)  :: err(*)
+    end function
+
+    !> The block split over MPI ranks (one GPU each): the blocks this rank steps, the exchange lists,
+    !> and the hook, a bind(C) function of the driver that moves the buffers with MPI (its interface:
+    !> integer(c_int32_t) function hook(user, kind, family, nsend, send, nrecv, recv) bind(C), with
+    !> user a c_ptr value, kind and family c_int32_t values, nsend and nrecv c_int64_t values, send
+    !> and recv real(c_double) arrays).
+    integer(c_int) function ice_gpu_set_partition(ctx, owned) bind(C, name='ice_gpu_set_partition')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value             :: ctx
+      integer(c_int32_t), intent(in) :: owned(*)
+    end function
+
+    integer(c_int) function ice_gpu_set_halo(ctx, kind, p, nsend, send, nrecv, recv) bind(C, name='ice_gpu_set_halo')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value             :: ctx
+      integer(c_int32_t), value      :: kind, p, nsend, nrecv
+      integer(c_int32_t), intent(in) :: send(*), recv(*)
+    end function
+
+    integer(c_int) function ice_gpu_set_exchange_hook(ctx, fn, user) bind(C, name='ice_gpu_set_exchange_hook')
+      import :: c_int, c_ptr, c_funptr
+      type(c_ptr), value    :: ctx
+      type(c_funptr), value :: fn
+      type(c_ptr), value    :: user
     end function
   end interface
 

@@ -86,3 +86,93 @@ def test_lpt_matches_the_reference_rule():
     owner = parallel.lpt(w, 8)
     loads = [sum(x for x, o in zip(w, owner) if o == r) for r in range(8)]
     assert max(loads) <= sum(w) / 8 + max(w)
+
+
+class _Loopback:
+    """The exchange hook of two ranks that live as two threads of one process, each with its own CUDA
+    context on the one GPU: every call posts this rank's send buffer, meets the other rank at a
+    barrier and takes the other's buffer (the plan sends everything to the one peer), or reduces both
+    for DT (min) and NORM (sum). Each rank's step has drained its stream before it calls the hook, so
+    no kernel of one rank waits on the other's; a rank that fails breaks the barrier, which ends the
+    other's wait within its timeout."""
+
+    def __init__(self):
+        import threading
+        self.barrier = threading.Barrier(2, timeout=120)
+        self.slot = [None, None]
+
+    def hook(self, rank):
+        def call(user, kind, family, nsend, send, nrecv, recv):
+            try:
+                mine = np.ctypeslib.as_array(send, shape=(max(nsend, 1),))[:nsend].copy()
+                self.slot[rank] = mine
+                self.barrier.wait()
+                other = self.slot[1 - rank]
+                out = np.ctypeslib.as_array(recv, shape=(max(nrecv, 1),))[:nrecv]
+                if kind == parallel.DT:
+                    out[:] = np.minimum(mine, other)
+                elif kind == parallel.NORM:
+                    out[:] = mine + other if rank == 0 else other + mine
+                else:
+                    out[:] = other[:nrecv]
+                self.barrier.wait()
+                return 0
+            except Exception:
+                self.barrier.abort()
+                return 1
+        return parallel.EXCHANGE_FN(call)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32flux"])
+def test_two_rank_split_on_the_gpu(precision):
+    """The CUDA library's split step, two ranks as two contexts on one GPU exchanging through the
+    hook: the same bits as one context stepping every block, in both forms."""
+    import threading
+    import torch
+    from ice_b200 import abi
+    from ice_b200.solver import Solver
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    gpu = abi.load_gpu()
+
+    def make():
+        c = _case()
+        c.numerics.precision = precision
+        return c
+    ref = Solver(make(), gpu)
+    out = ref.step(STEPS)
+    tot, fam = ref.residual_norm()
+    loop = _Loopback()
+    owner = parallel.lpt([int(np.prod(d)) for d in ref.case.dims], 2)
+    ranks, hooks, results = [], [], [None, None]
+    for r in range(2):
+        s = Solver(make(), gpu)
+        apply = parallel.halo_plan(s.case, owner, r)
+        parallel.apply_plan(gpu, s.ctx, s.case, owner, r, apply)
+        fn = loop.hook(r)
+        parallel.attach_hook(gpu, s.ctx, fn)
+        ranks.append(s)
+        hooks.append(fn)
+
+    def run(r):
+        try:
+            o = ranks[r].step(STEPS)
+            t, f = ranks[r].residual_norm()
+            results[r] = (o.status, o.dtglobal, o.time, t, f)
+        except Exception as e:                  # reported below
+            results[r] = e
+    th = [threading.Thread(target=run, args=(r,)) for r in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=300)
+    for r in range(2):
+        assert not isinstance(results[r], Exception), results[r]
+        status, dt, time, t, f = results[r]
+        assert status == 0 and dt == out.dtglobal and time == out.time
+        assert np.array_equal(t, tot) and np.array_equal(f, fam)
+    for b in range(len(ref.case.nodes)):
+        for p in range(len(ref.case.families)):
+            got = ranks[owner[b]].download(b, p)[2:-2, 2:-2, 2:-2]
+            assert np.array_equal(got, ref.download(b, p)[2:-2, 2:-2, 2:-2]), (b, p)
