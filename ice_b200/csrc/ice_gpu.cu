@@ -366,7 +366,9 @@ __global__ void k_unpack_flux(double* __restrict__ F, int nc, const int4* __rest
   for (int v = 0; v < nc; ++v) F[(long long)e[q].x * nc + v] = in[(long long)q * nc + v];
 }
 
-static int ensure_xbuf(ice_gpu_ctx* c, size_t n) {
+static int ensure_xbuf(ice_gpu_ctx* c, size_t n, cudaStream_t s) {
+  if (c->xdev.n >= n && c->xhost_n >= n) return 0;
+  CK(cudaStreamSynchronize(s));                    // the last exchange's copy and unpack read the buffers
   if (c->xdev.n < n) CK(c->xdev.alloc(n));
   if (c->xhost_n < n) {
     if (c->xhost) cudaFreeHost(c->xhost);
@@ -387,7 +389,7 @@ static void halo_xchg(const LaunchArgs& a, int kind) {
   const int p = a.fam, nc = c->fam[p].nc, w = kind == ICE_GPU_HALO_BETA ? 1 : nc;
   const int ns = (int)c->hs[kind][p].size(), nr = (int)c->hr[kind][p].size();
   const size_t ls = (size_t)ns * w, lr = (size_t)nr * w;
-  if (ensure_xbuf(c, ls + lr + 1)) { c->xerr = ICE_GPU_ECUDA; return; }
+  if (ensure_xbuf(c, ls + lr + 1, a.s)) { c->xerr = ICE_GPU_ECUDA; return; }
   double* ds = c->xdev.p; double* dr = c->xdev.p + ls;
   const int4* es = c->hs_dev[kind][p].p; const int4* er = c->hr_dev[kind][p].p;
   if (ns > 0) {

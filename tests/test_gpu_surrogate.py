@@ -42,7 +42,7 @@ def test_training_gradient_matches_oracle(gpu):
             assert err <= 1e-4 * scale + 1e-9, (l, a, err, scale)
 
 
-def test_tensor_core_inference_matches_oracle(gpu):
+def test_tensor_core_inference_matches_oracle(gpu, capsys):
     rng = np.random.default_rng(6)
     w = mlp.glorot(3)
     n = 1000          # four CTAs' worth of 256 rows, the last one partial
@@ -52,8 +52,13 @@ def test_tensor_core_inference_matches_oracle(gpu):
     yb = mlp.forward_bf16(w, x)
     y64, _ = mlp.forward(w.astype(np.float64), x)
     scale = np.abs(y64).max()
-    # against the same roundings: only the order of the FP32 sums and BF16 ties differ
-    assert np.abs(y - yb).max() <= 2e-2 * scale, np.abs(y - yb).max() / scale
+    # against the same roundings: only the order of the FP32 sums, the hardware exponential and
+    # reciprocal of SiLU and the BF16 roundings they tip differ
+    with capsys.disabled():
+        print(f"\ninference against the same roundings: max {np.abs(y - yb).max() / scale:.2e}, "
+              f"median {np.median(np.abs(y - yb)) / scale:.2e} of the output scale")
+    assert np.median(np.abs(y - yb)) <= 1e-3 * scale, np.median(np.abs(y - yb)) / scale
+    assert np.abs(y - yb).max() <= 1e-2 * scale, np.abs(y - yb).max() / scale
     # against the exact network: the BF16 error of four layers
     assert np.abs(y - y64).max() <= 5e-2 * scale, np.abs(y - y64).max() / scale
 
@@ -101,5 +106,7 @@ def test_surrogate_source_against_plain_closure(gpu, capsys):
     assert env <= 0.01 * cells, (env, cells)
     assert 0 <= env + res <= cells
     assert rep.mdot_rel_median < 1e-2 and rep.q_rel_median < 1e-2
+    # what the network gains: the cells it serves skip the iterative closure
+    assert cells - env - res >= 0.1 * cells, (cells - env - res, cells)
     for k, v in e_sur.items():
         assert v <= 1e-4, (k, v)
