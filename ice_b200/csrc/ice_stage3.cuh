@@ -163,6 +163,11 @@ __device__ __forceinline__ bool face_flux_staged(const Geo& G, const FamDev& F, 
   return bad;
 }
 
+// A hint to bring the cache line of p (a valid address of global memory) into L1; nothing waits on it.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" :: "l"((unsigned long long)__cvta_generic_to_global(p)));
+}
+
 // The stage kernel (see the head of this file). write_r: store R instead of updating (IRS runs).
 template <int CL, int RS, int LIM, typename R>
 __global__ void __launch_bounds__(Shape<CL>::NT, (sizeof(R) == 4) ? 2 : 1)
@@ -355,6 +360,37 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     const bool more = k + 1 < k1;
     if (more) issue(k + 3);                     // lands at the end of this plane, into the slot of k
     const R* P = plane(cur);
+    if (own) {
+      // the global operands of this plane's update, z face and own x and y faces, into L1 while the
+      // plane's first faces are computed: the kernel waits on global loads more than on anything else
+      const long long gq = gidx(B, i, j, k), qq = iidx(B, i, j, k);
+#pragma unroll
+      for (int v = 0; v < nc; ++v) { prefetch_l1(F.Up + (long long)v * G.NG + gq); prefetch_l1(F.U0 + (long long)v * G.NG + gq); }
+      if (F.coupled && F.src_ready) {
+        if (F.Sf) { for (int v = 0; v < nc; ++v) prefetch_l1(F.Sf + (long long)v * G.NI + qq); }
+      } else if (F.coupled) {
+        if constexpr (sizeof(R) == 4) { for (int v = 0; v < 9; ++v) prefetch_l1(G.gasf + (long long)v * G.NI + qq); }
+      }
+      prefetch_l1(G.vol + qq); prefetch_l1(F.bmap + qq);
+      if constexpr (sizeof(R) == 4) {
+        if (az && k <= B.nk - 2) {
+          const long long r1 = ridx(B, i, j, k + 1), rs = (long long)(B.ni + 2) * (B.nj + 2);
+          prefetch_l1(G.dlf + 2 * G.NR + r1 + rs);
+          prefetch_l1(G.ff[2] + fidx(B, 2, i, j, k, k + 1));
+        }
+        if (ax && i >= 1) {
+          const long long r0 = ridx(B, i - 1, j, k);
+          prefetch_l1(G.dlf + r0 - 1); prefetch_l1(G.dlf + r0 + 2);
+          prefetch_l1(G.ff[0] + fidx(B, 0, i - 1, j, k, i));
+        }
+        if (ay && j >= 1) {
+          const long long r0 = ridx(B, i, j - 1, k), rs = B.ni + 2;
+          const float* d1 = G.dlf + G.NR;
+          prefetch_l1(d1 + r0 - rs); prefetch_l1(d1 + r0); prefetch_l1(d1 + r0 + rs); prefetch_l1(d1 + r0 + 2 * rs);
+          prefetch_l1(G.ff[1] + fidx(B, 1, i, j - 1, k, j));
+        }
+      }
+    }
     // the x and y faces of this plane, each once, as one list of tasks dealt out to the threads in turn:
     // the x face below every owned cell, the y face below every owned cell, then the x faces above the
     // last column and the y faces above the last row (a face on the block's boundary is its records')
