@@ -576,13 +576,13 @@ static void tile_shape(int ndir, int& TX, int& TY, int& KZ) {
 }
 
 // The staged kernel's limits for a closure (Shape<CL> of ice_stage3.cuh).
-static void shape_limits(int closure, int& NT, int& MW, int& MH, int& MB, int& FX, int& FY) {
+static void shape_limits(int closure, int& NT, int& MW, int& MH, int& MB, int& FX, int& FY, int& SXC, int& SYC) {
   if (closure == ICE_CLOSURE_AG) {
     NT = Shape<AG>::NT; MW = Shape<AG>::MAXW; MH = Shape<AG>::MAXH; MB = Shape<AG>::MAXBOX;
-    FX = Shape<AG>::FX; FY = Shape<AG>::FY;
+    FX = Shape<AG>::FX; FY = Shape<AG>::FY; SXC = Shape<AG>::SXC; SYC = Shape<AG>::SYC;
   } else {
     NT = Shape<MK>::NT; MW = Shape<MK>::MAXW; MH = Shape<MK>::MAXH; MB = Shape<MK>::MAXBOX;
-    FX = Shape<MK>::FX; FY = Shape<MK>::FY;
+    FX = Shape<MK>::FX; FY = Shape<MK>::FY; SXC = Shape<MK>::SXC; SYC = Shape<MK>::SYC;
   }
 }
 
@@ -604,8 +604,8 @@ static TuneRow tune_of(int closure) {
 }
 
 static Tile tile_shape3(int ni, int nj, int closure) {
-  int NT, MW, MH, MB, FX, FY;
-  shape_limits(closure, NT, MW, MH, MB, FX, FY);
+  int NT, MW, MH, MB, FX, FY, SXC, SYC;
+  shape_limits(closure, NT, MW, MH, MB, FX, FY, SXC, SYC);
   (void)MW;
   const TuneRow tr = tune_of(closure);
   Tile best{};
@@ -617,6 +617,7 @@ static Tile tile_shape3(int ni, int nj, int closure) {
     const int hmax = std::min(std::min(nj, MH), NT / W);
     for (int H = 1; H <= hmax; ++H) {
       if (st_box_x(W) * (H + 4) > MB || H * (W + 1) > FX || (H + 1) * W > FY) break;
+      if (H * (W + 2) > SXC || (H + 2) * W > SYC) break;   // the FP32-flux form's cell slopes
       const int nx = (ni + W - 1) / W, ny = (nj + H - 1) / H;
       const int w = (ni + nx - 1) / nx, h = (nj + ny - 1) / ny;
       const int tasks = (ax ? w * h + h : 0) + (ay ? w * h + w : 0);

@@ -16,7 +16,11 @@
 //    same operands as the reference's per-face reconstruction, so the plain form keeps its bits;
 //  - x and y: each thread the face below its own cell, then the w + h faces above the tile's last
 //    column and last row as a short list of extra tasks (face_flux, Mod_Fluxes.f90:599-685), every
-//    interior face of the tile once;
+//    interior face of the tile once. The plain form reconstructs each face from its four-cell stencil;
+//    the FP32-flux form first computes every cell's limited x and y slope once (the value the
+//    per-face reconstruction computes twice, for the two faces of the cell) into the staging buffer,
+//    and each face forms its two states from its cells' slopes; that form issues the next plane's
+//    copy only after the faces, when the buffer is free again;
 //  - each owned cell adds its boundary-record fluxes, then its two faces per direction in the
 //    odd-then-even order of tile_sweep (Mod_Fluxes.f90:470-506), evaluates its source
 //    (Mod_Sources.f90:465-622), forms R = (R/vol + S) dt (Lib_Residual.f90:147-156) and applies the
@@ -40,6 +44,8 @@ template <int CL> struct Shape {
   static constexpr int MAXBOX = CL == AG ? 360 : 560;
   static constexpr int FX = NT + MAXH;          // x-face slots: h (w + 1)
   static constexpr int FY = NT + MAXW;          // y-face slots: (h + 1) w
+  static constexpr int SXC = NT + 2 * MAXH;     // x-slope slots: h (w + 2), the FP32-flux form's cell slopes
+  static constexpr int SYC = NT + 2 * MAXW;     // y-slope slots: (h + 2) w
 };
 __host__ __device__ constexpr int st_box_x(int w) { return (w + 6) & ~1; }
 
@@ -54,6 +60,11 @@ template <int CL, typename R> struct StageSmem {
   static constexpr size_t bt = st_align(fy + sizeof(R) * nc * Shape<CL>::FY);   // R [2][P]: beta of planes k, k+1
   static constexpr size_t bar = st_align(bt + sizeof(R) * 2 * P);          // mbarrier
   static constexpr size_t bytes = bar + 16 + 128;   // + the alignment of the base to 128 bytes
+  // the FP32-flux form's cell slopes of a plane live in the staging buffer while no copy is in flight:
+  // R [nc][SXC] x slopes, R [nc][SYC] y slopes, R [SXC + SYC] half lengths, u8 [SXC + SYC] first-order flags
+  static constexpr int SXC = Shape<CL>::SXC, SYC = Shape<CL>::SYC;
+  static constexpr size_t slope_bytes = (sizeof(R) * (nc + 1) + 1) * (size_t)(SXC + SYC);
+  static_assert(sizeof(R) == 8 || slope_bytes <= sizeof(double) * nc * P, "the cell slopes must fit the staging buffer");
 };
 
 // The limited slope of cell c along one direction, before the face's limval: q(s, v) reads the cells
@@ -356,9 +367,27 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   const int nxo = ax ? w * h : 0, nyo = ay ? w * h : 0;
   const int nfx = nxo + nyo + nhx + nhy;
 
+  // The FP32-flux form computes each cell's limited x and y slopes once per plane (the slope that
+  // state_reconstruction computes for the left state of the face above the cell and for the right
+  // state of the face below it: the same operands and operations, so the same values) into the
+  // staging buffer, and the faces form their states from them; the next plane's copy into that buffer
+  // is then issued once the faces are done. The plain form reconstructs each face from its stencil.
+  constexpr bool SL = sizeof(R) == 4;
+  constexpr int SXC = Shape<CL>::SXC, SYC = Shape<CL>::SYC;
+  R* SX = (R*)stg;                              // [nc][SXC]: tile cell (cx, cy), cx in -1..w: cy (w + 2) + cx + 1
+  R* SY = SX + nc * SXC;                        // [nc][SYC]: cy in -1..h: (cy + 1) w + cx
+  R* DX = SY + nc * SYC;                        // the cells' half lengths along x, then along y
+  R* DY = DX + SXC;
+  unsigned char* QX = (unsigned char*)(DY + SYC);   // the first-order flags along x, then along y
+  unsigned char* QY = QX + SXC;
+  const int sxw = w + 2;
+  const int nsx = ax ? sxw * h : 0, nsy = ay ? w * (h + 2) : 0;
+
   for (int k = k0; k < k1; ++k) {
     const bool more = k + 1 < k1;
-    if (more) issue(k + 3);                     // lands at the end of this plane, into the slot of k
+    if constexpr (!SL) {
+      if (more) issue(k + 3);                   // lands at the end of this plane, into the slot of k
+    }
     const R* P = plane(cur);
     if (own) {
       // the global operands of this plane's update, z face and own x and y faces, into L1 while the
@@ -391,6 +420,38 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
         }
       }
     }
+    if constexpr (SL) {
+      // the cell slopes of this plane: along x for the columns -1..w, along y for the rows -1..h, of
+      // the cells inside the block (the others border no interior face of the tile)
+      for (int e = tid; e < nsx + nsy; e += NT) {
+        int d, cx, cy, idx;
+        if (e < nsx) { d = 0; cx = e % sxw - 1; cy = e / sxw; idx = e; }
+        else { d = 1; idx = e - nsx; cx = idx % w; cy = idx / w - 1; }
+        const int ci = d == 0 ? t.i0 + cx : t.j0 + cy, n = d == 0 ? B.ni : B.nj;
+        if (ci < 0 || ci >= n) continue;
+        const int ic = t.i0 + cx, jc = t.j0 + cy;
+        const long long r0 = ridx(B, ic, jc, k);
+        const long long rs = d == 0 ? 1LL : (long long)(B.ni + 2);
+        const float* dl = G.dlf + (long long)d * G.NR;
+        R lm = dl[r0 - rs], l0 = dl[r0], lp = dl[r0 + rs];
+        if (ci == 0 || ci == n - 1) {
+          const long long g = gidx(B, ic, jc, k), gs = gstride(B, d);
+          if (ci == 0 && F.inj[g - gs]) lm = (R)0;
+          if (ci == n - 1 && F.inj[g + gs]) lp = (R)0;
+        }
+        const int st1 = d == 0 ? 1 : bx;
+        const SmemStencil<R> q{P, spos(cx, cy) - st1, st1, np};
+        R s[nc], dlc; bool first;
+        cell_slope<CL, LIM, R>(F.limiter, q, lm, l0, lp, s, dlc, first);
+        R* S = d == 0 ? SX : SY;
+        const int cap = d == 0 ? SXC : SYC;
+#pragma unroll
+        for (int v = 0; v < nc; ++v) S[v * cap + idx] = s[v];
+        (d == 0 ? DX : DY)[idx] = dlc;
+        (d == 0 ? QX : QY)[idx] = first ? 1 : 0;
+      }
+      __syncthreads();
+    }
     // the x and y faces of this plane, each once, as one list of tasks dealt out to the threads in turn:
     // the x face below every owned cell, the y face below every owned cell, then the x faces above the
     // last column and the y faces above the last row (a face on the block's boundary is its records')
@@ -409,9 +470,31 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       // the face below tile cell (cx, cy) along d: its lower cell, stencil and the two cells' weights
       const int lx = cx - (d == 0), ly = cy - (d == 1);
       const int sst = d == 0 ? 1 : bx;
+      const R bf = mn(beta_of(bcur, lx, ly), beta_of(bcur, cx, cy));
       R fl[nc];
-      bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, d, t.i0 + lx, t.j0 + ly, k, P, np, spos(cx, cy) - 2 * sst, sst,
-                                              mn(beta_of(bcur, lx, ly), beta_of(bcur, cx, cy)), fl);
+      if constexpr (SL) {
+        // the states from the two cells' slopes, then the flux
+        const int il = d == 0 ? cy * sxw + cx : cy * w + cx, iu = il + (d == 0 ? 1 : w);
+        const R* S = d == 0 ? SX : SY;
+        const int cap = d == 0 ? SXC : SYC;
+        const R* D = d == 0 ? DX : DY;
+        const unsigned char* Q = d == 0 ? QX : QY;
+        R sl[nc], sr[nc], pl[nc], pr[nc];
+#pragma unroll
+        for (int v = 0; v < nc; ++v) { sl[v] = S[v * cap + il]; sr[v] = S[v * cap + iu]; }
+        const SmemCell<R> ql{P, spos(lx, ly), np}, qr{P, spos(cx, cy), np};
+        bad |= states_from_slopes<CL, R>(ql, sl, D[il], Q[il] != 0, qr, sr, D[iu], Q[iu] != 0, bf, pl, pr);
+        const int c = d == 0 ? t.i0 + lx : t.j0 + ly;
+        const long long fi = fidx(B, d, t.i0 + lx, t.j0 + ly, k, c + 1);
+        R nrm[3], area;
+        face_geometry<R>(G, d, fi, nrm, area);
+        riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
+#pragma unroll
+        for (int v = 0; v < nc; ++v) fl[v] = fl[v] * area;
+      } else {
+        bad |= face_flux_staged<CL, RS, LIM, R>(G, F, B, d, t.i0 + lx, t.j0 + ly, k, P, np, spos(cx, cy) - 2 * sst,
+                                                sst, bf, fl);
+      }
       R* dst = d == 0 ? Fx + cy * (w + 1) + cx : Fy + cy * w + cx;
       const int vs = d == 0 ? FX : FY;
 #pragma unroll
@@ -426,7 +509,11 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     }
     // the next plane's weights (its planes below and above are in the ring now), read after a barrier
     if (az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
+    if constexpr (SL) fence_proxy_async_smem();   // this thread's slope accesses before the copy that overwrites them
     __syncthreads();
+    if constexpr (SL) {
+      if (more) issue(k + 3);                   // lands at the end of this plane, into the slot of k
+    }
     if (own) {
       const long long q = iidx(B, i, j, k);
       const int bc = F.bmap[q];
