@@ -366,6 +366,18 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   // the face tasks: x and y faces below the owned cells (none along a direction with one cell), extras
   const int nxo = ax ? w * h : 0, nyo = ay ? w * h : 0;
   const int nfx = nxo + nyo + nhx + nhy;
+  // face task e: the face below tile cell (cx, cy) along d; false for a face on the block's boundary
+  auto face_task = [&](int e, int& d, int& cx, int& cy) -> bool {
+    if (e < nxo + nyo) {
+      d = e >= nxo;
+      const int c = e - (d ? nxo : 0);
+      cx = c % w; cy = c / w;
+      return d == 0 ? t.i0 + cx != 0 : t.j0 + cy != 0;
+    }
+    if (e < nxo + nyo + nhx) { d = 0; cx = w; cy = e - nxo - nyo; }
+    else { d = 1; cx = e - nxo - nyo - nhx; cy = h; }
+    return true;
+  };
 
   // The FP32-flux form computes each cell's limited x and y slopes once per plane (the slope that
   // state_reconstruction computes for the left state of the face above the cell and for the right
@@ -457,16 +469,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     // last column and the y faces above the last row (a face on the block's boundary is its records')
     for (int e = tid; e < nfx; e += NT) {
       int d, cx, cy;
-      if (e < nxo + nyo) {
-        d = e >= nxo;
-        const int c = e - (d ? nxo : 0);
-        cx = c % w; cy = c / w;
-        if (d == 0 ? t.i0 + cx == 0 : t.j0 + cy == 0) continue;
-      } else if (e < nxo + nyo + nhx) {
-        d = 0; cx = w; cy = e - nxo - nyo;
-      } else {
-        d = 1; cx = e - nxo - nyo - nhx; cy = h;
-      }
+      if (!face_task(e, d, cx, cy)) continue;
       // the face below tile cell (cx, cy) along d: its lower cell, stencil and the two cells' weights
       const int lx = cx - (d == 0), ly = cy - (d == 1);
       const int sst = d == 0 ? 1 : bx;
@@ -500,20 +503,19 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
 #pragma unroll
       for (int v = 0; v < nc; ++v) dst[v * vs] = fl[v];
     }
-    // z: the face above the cell, from the slopes at k (carried) and k + 1
+    // z: the slope of the cell above (planes k, k+1, k+2 are in the ring), and the weights of the next
+    // plane; after the barrier, the face above the cell from the slopes at k (carried) and k + 1 and the
+    // two cells' weights
     R szn[nc]; R dlzn = (R)0; bool fzn = true;
-    if (az && own && k <= B.nk - 2) {
-      zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
-      const R b1 = F.sd ? beta_at(cur, nx1, nx2, tx, ty, k + 1) : (R)1;
-      zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), b1), fhi);
-    }
-    // the next plane's weights (its planes below and above are in the ring now), read after a barrier
-    if (az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
+    const bool zup = az && k <= B.nk - 2;
+    if (zup && own) zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
+    if (zup) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
     if constexpr (SL) fence_proxy_async_smem();   // this thread's slope accesses before the copy that overwrites them
     __syncthreads();
     if constexpr (SL) {
       if (more) issue(k + 3);                   // lands at the end of this plane, into the slot of k
     }
+    if (zup && own) zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), beta_of(bcur ^ 1, tx, ty)), fhi);
     if (own) {
       const long long q = iidx(B, i, j, k);
       const int bc = F.bmap[q];
