@@ -503,19 +503,20 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
 #pragma unroll
       for (int v = 0; v < nc; ++v) dst[v * vs] = fl[v];
     }
-    // z: the slope of the cell above (planes k, k+1, k+2 are in the ring), and the weights of the next
-    // plane; after the barrier, the face above the cell from the slopes at k (carried) and k + 1 and the
-    // two cells' weights
+    // z: the face above the cell, from the slopes at k (carried) and k + 1
     R szn[nc]; R dlzn = (R)0; bool fzn = true;
-    const bool zup = az && k <= B.nk - 2;
-    if (zup && own) zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
-    if (zup) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
+    if (az && own && k <= B.nk - 2) {
+      zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
+      const R b1 = F.sd ? beta_at(cur, nx1, nx2, tx, ty, k + 1) : (R)1;
+      zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), b1), fhi);
+    }
+    // the next plane's weights (its planes below and above are in the ring now), read after a barrier
+    if (az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
     if constexpr (SL) fence_proxy_async_smem();   // this thread's slope accesses before the copy that overwrites them
     __syncthreads();
     if constexpr (SL) {
       if (more) issue(k + 3);                   // lands at the end of this plane, into the slot of k
     }
-    if (zup && own) zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), beta_of(bcur ^ 1, tx, ty)), fhi);
     if (own) {
       const long long q = iidx(B, i, j, k);
       const int bc = F.bmap[q];
