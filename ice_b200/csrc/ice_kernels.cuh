@@ -572,12 +572,54 @@ __device__ __forceinline__ void ghost2_rec(const Geo& G, const FamDev& F, const 
 // direction the cell is interior, no other record writes it, and one thread does both layers in turn
 // (layers = 3). Where it is one cell deep the cell is the opposite face's layer-1 ghost, which another
 // record writes: then the host launches layer 1 of every record first and layer 2 after it.
+//
+// Both layers of the copying records at once (layers = 3: 0 and 400 extrapolate, 101 and 201 copy
+// from the partner block): every load first, then every store, the values and operations of
+// ghost1_rec followed by ghost2_rec (layer 2 of a 400 record, 3 g1 - 3 m + p, with g1 the layer-1
+// value just copied from m).
+template <int CL>
+__device__ __forceinline__ void ghost12_copy(const Geo& G, const FamDev& F, const DRec& r) {
+  constexpr int nc = NC<CL>::v;
+  const DBlock& B = G.blk[r.b];
+  const int g0 = (r.f == 1) - (r.f == 2), g1 = (r.f == 3) - (r.f == 4), g2 = (r.f == 5) - (r.f == 6);
+  const long long gg1 = gidx(B, r.i - g0, r.j - g1, r.k - g2);
+  const long long gg2 = gidx(B, r.i - 2 * g0, r.j - 2 * g1, r.k - 2 * g2);
+  double* P = F.Ug;
+  const long long NG = G.NG;
+  double a[nc], b[nc];
+  if (r.type == 101 || r.type == 201) {
+    const DBlock& S = G.blk[r.bs];
+    const int s0 = (r.fs == 1) - (r.fs == 2), s1 = (r.fs == 3) - (r.fs == 4), s2 = (r.fs == 5) - (r.fs == 6);
+    const long long gs1 = gidx(S, r.is, r.js, r.ks), gs2 = gidx(S, r.is + s0, r.js + s1, r.ks + s2);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) { a[v] = P[v * NG + gs1]; b[v] = P[v * NG + gs2]; }
+  } else {
+    const long long gm = gidx(B, r.i, r.j, r.k), gp = gidx(B, r.i + g0, r.j + g1, r.k + g2);
+#pragma unroll
+    for (int v = 0; v < nc; ++v) a[v] = P[v * NG + gm];
+    if (r.type == 400) {
+#pragma unroll
+      for (int v = 0; v < nc; ++v) b[v] = 3.0*a[v] - 3.0*a[v] + P[v * NG + gp];
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < nc; ++v) P[v * NG + gg1] = a[v];
+  if (r.type != 0) {
+#pragma unroll
+    for (int v = 0; v < nc; ++v) P[v * NG + gg2] = b[v];
+  }
+}
+
 template <int CL>
 __global__ void k_ghost(Geo G, FamDev F, const DRec* recs, int nrec, int layers) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nrec) return;
   const DRec r = recs[n];
   if (!stepped(G, r.b)) return;
+  if (layers == 3 && (r.type == 0 || r.type == 400 || r.type == 101 || r.type == 201)) {
+    ghost12_copy<CL>(G, F, r);
+    return;
+  }
   if (layers & 1) ghost1_rec<CL>(G, F, r);
   if (layers & 2) ghost2_rec<CL>(G, F, r);
 }
@@ -648,7 +690,7 @@ __global__ void __launch_bounds__(128, 4) k_bound(Geo G, FamDev F, const DRec* r
 // the stage kernel adds to the residual. Its own kernel, so that the iterative closures do not
 // share the stencil kernel's registers.
 template <int CL, typename R>
-__global__ void __launch_bounds__(256) k_source(Geo G, FamDev F) {
+__global__ void __launch_bounds__(256, 4) k_source(Geo G, FamDev F) {
   constexpr int nc = NC<CL>::v;
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= G.NI) return;

@@ -212,6 +212,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   auto spos = [&](int cx, int cy) { return (cy + 2) * bx + cx + 2 + sh; };   // tile cell (cx, cy) in a plane
   const int pos = spos(tx, ty);
   const int k0 = t.k0, k1 = t.k0 + t.nkz;
+  const bool u0p = F.U0 == F.Up;                // the first RK stage: U_0 is the stencil state itself
   const uint32_t box_bytes = (uint32_t)(sizeof(double) * nc * np);
 
   if (tid == 0) {
@@ -406,7 +407,10 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       // plane's first faces are computed: the kernel waits on global loads more than on anything else
       const long long gq = gidx(B, i, j, k), qq = iidx(B, i, j, k);
 #pragma unroll
-      for (int v = 0; v < nc; ++v) { prefetch_l1(F.Up + (long long)v * G.NG + gq); prefetch_l1(F.U0 + (long long)v * G.NG + gq); }
+      for (int v = 0; v < nc; ++v) {
+        prefetch_l1(F.Up + (long long)v * G.NG + gq);
+        if (!u0p) prefetch_l1(F.U0 + (long long)v * G.NG + gq);
+      }
       if (F.coupled && F.src_ready) {
         if (F.Sf) { for (int v = 0; v < nc; ++v) prefetch_l1(F.Sf + (long long)v * G.NI + qq); }
       } else if (F.coupled) {
@@ -637,7 +641,7 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
       } else {
         double po[nc], co[nc], cn[nc];
 #pragma unroll
-        for (int v = 0; v < nc; ++v) po[v] = F.U0[(long long)v * G.NG + g];
+        for (int v = 0; v < nc; ++v) po[v] = u0p ? p[v] : F.U0[(long long)v * G.NG + g];
         prim2cons<CL, double>(po, co, F.mat.cp);
         prim2cons<CL, double>(p, cn, F.mat.cp);
 #pragma unroll
