@@ -82,6 +82,7 @@ struct FamHost {
   DevBuf<DRec> grecs;                        // the same records ordered for the ghost kernel (upload_recs)
   bool ghost_split = false;                  // the ghost layers in two launches (upload_recs)
   DevBuf<int> bfirst, blist, own;
+  DevBuf<int> bperm;                         // the boundary cells in the boundary kernel's thread order
   DevBuf<CUtensorMap> maps[3];               // per state buffer, per block: the staged kernel's TMA maps
   DevBuf<Tile> tiles3;                       // the staged kernel's tiles
   int ntile3 = 0;
@@ -440,7 +441,7 @@ static void launch_family(ice_gpu_ctx* c, int p, int srk, int phase, cudaStream_
   a.F = make_famdev(c, p, srk, phase);
   a.recs = H.recs.p; a.nrec = H.nrec; a.grecs = H.grecs.p; a.ghost_split = H.ghost_split;
   a.own = H.own.p; a.nown = H.nown;
-  a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc;
+  a.bfirst = H.bfirst.p; a.blist = H.blist.p; a.nbc = H.nbc; a.bperm = H.bperm.p;
   a.tiles = c->tiles.p; a.ntile = c->ntile; a.TX = c->TX; a.TY = c->TY; a.KZ = c->KZ;
   a.tiles3 = H.tiles3.p; a.ntile3 = H.ntile3;
   a.maps = H.maps[stencil_buffer(c, srk, phase)].p;
@@ -1183,6 +1184,21 @@ int ice_gpu_set_records(ice_gpu_ctx* c, int32_t nrec, const int32_t* ri, const d
     if (!dlist.empty()) CK(cudaMemcpy(H.blist.p, dlist.data(), dlist.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(H.bmap.p, bmap.data(), c->NI * sizeof(int), cudaMemcpyHostToDevice));
     CK(H.Rb.alloc((size_t)std::max(H.nbc, 1) * H.nc));
+    // the boundary kernel's thread order: the cells grouped by block, by the face of their first record
+    // and by whether it is a connection, in cell order within a group, so that the threads of a warp take
+    // the same branches (each cell's sum and its slot of Rb are the same in any order)
+    {
+      std::vector<int> perm(H.nbc);
+      for (int q = 0; q < H.nbc; ++q) perm[q] = q;
+      auto key = [&](int q) {
+        const HRec& r = c->recs[H.h_list[H.h_first[q]]];
+        const int conn = (r.type == 101 || r.type == 201) ? 1 : 0;
+        return ((long long)r.b * 8 + r.f) * 2 + conn;
+      };
+      std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return key(x) < key(y); });
+      CK(H.bperm.alloc(std::max<size_t>(perm.size(), 1)));
+      if (!perm.empty()) CK(cudaMemcpy(H.bperm.p, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // connection owners, table order
     H.h_own.clear();
     for (int n : grp) {

@@ -213,7 +213,7 @@ __device__ __forceinline__ double family_dt(const Geo& G, const DtFam& f, const 
   return dt;
 }
 
-__global__ void __launch_bounds__(256) k_dt_all(Geo G, DtArgs a, Status* st) {
+__global__ void __launch_bounds__(256, 6) k_dt_all(Geo G, DtArgs a, Status* st) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double dt = INFINITY;
   const int bq = q < G.NI ? find_block(G.blk, G.nb, q) : 0;
@@ -658,9 +658,10 @@ __global__ void __launch_bounds__(128, 4) k_conn(Geo G, FamDev F, const DRec* re
 
 template <int CL, int RS, int LIM, typename R>
 __global__ void __launch_bounds__(128, 4) k_bound(Geo G, FamDev F, const DRec* recs, const int* first, const int* list,
-                                                  int nbc, Status* st) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nbc) return;
+                                                  const int* perm, int nbc, Status* st) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nbc) return;
+  const int c = perm[t];
   if (!stepped(G, recs[list[first[c]]].b)) return;
   constexpr int nc = NC<CL>::v;
   double acc[nc];

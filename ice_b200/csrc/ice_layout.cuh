@@ -142,6 +142,7 @@ struct LaunchArgs {
   int ghost_split;                                   // a record's second layer reads another's first
   const int* own; int nown;
   const int* bfirst; const int* blist; int nbc;
+  const int* bperm;                                  // the boundary cells in the boundary kernel's thread order
   const Tile* tiles; int ntile; int TX, TY, KZ;     // the 1-D stage kernel's tiles
   const Tile* tiles3; int ntile3;                    // the staged stage kernel's tiles (2-D and 3-D runs)
   const CUtensorMap* maps;                           // per block: the TMA map of U_{k-1} (the stencil buffer)

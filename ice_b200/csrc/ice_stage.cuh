@@ -46,7 +46,7 @@ void launch_bound_k(const LaunchArgs& a) {
   if (a.nown > 0) k_conn<CL, RS, LIM, R><<<grid(a.nown, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.own, a.nown, a.st);
   if (a.xchg) a.xchg(a, ICE_GPU_HALO_FLUX);    // connection fluxes to the partners another rank steps
   if (a.nbc > 0)
-    k_bound<CL, RS, LIM, R><<<grid(a.nbc, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.bfirst, a.blist, a.nbc, a.st);
+    k_bound<CL, RS, LIM, R><<<grid(a.nbc, 128), 128, 0, a.s>>>(a.G, a.F, a.recs, a.bfirst, a.blist, a.bperm, a.nbc, a.st);
 }
 
 template <int CL, int RS, typename R>
