@@ -105,6 +105,8 @@ __device__ __forceinline__ R beta_cell(const FamDev& F, const DBlock& B, int i, 
 // record_flux (Mod_BC_Fluxes.f90:180-272): the flux through a record's face into its cell. R is the
 // reconstruction and Riemann type (double in the plain form, float in the FP32-flux form); LIM the
 // limiter the kernel is specialised for (the same formulas as the run-time switch in double).
+// The four stencil cells are read into registers before the reconstruction, so that their loads
+// are in flight together (the reconstruction's branches would otherwise order them).
 template <int CL, int RS, int LIM, typename R>
 __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double* flux, const double* beta_face) {
   constexpr int nc = NC<CL>::v;
@@ -132,7 +134,12 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
     if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = (R)0.5*dl_m; dll = (R)0; }
     if (F.inj[gidx(B, ip, jp, kp)]) dl2 = (R)0.5*dl_m;
     long long a[4] = {gidx(B, ig2, jg2, kg2), gidx(B, ig, jg, kg), gidx(B, i, j, k), gidx(B, ip, jp, kp)};
-    auto q = [&](int s, int v) { return (R)P[(long long)v * G.NG + a[s]]; };
+    R stn[4][nc];
+#pragma unroll
+    for (int s4 = 0; s4 < 4; ++s4)
+#pragma unroll
+      for (int v = 0; v < nc; ++v) stn[s4][v] = (R)P[(long long)v * G.NG + a[s4]];
+    auto q = [&](int s, int v) { return stn[s][v]; };
     bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
     riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
@@ -146,7 +153,12 @@ __device__ bool record_flux(const Geo& G, const FamDev& F, const DRec& r, double
     if (F.inj[gidx(B, ig, jg, kg)]) { dl1 = (R)0.5*dl_m; dlr = (R)0; }
     if (F.inj[gidx(B, ip, jp, kp)]) dl0 = (R)0.5*dl_m;
     long long a[4] = {gidx(B, ip, jp, kp), gidx(B, i, j, k), gidx(B, ig, jg, kg), gidx(B, ig2, jg2, kg2)};
-    auto q = [&](int s, int v) { return (R)P[(long long)v * G.NG + a[s]]; };
+    R stn[4][nc];
+#pragma unroll
+    for (int s4 = 0; s4 < 4; ++s4)
+#pragma unroll
+      for (int v = 0; v < nc; ++v) stn[s4][v] = (R)P[(long long)v * G.NG + a[s4]];
+    auto q = [&](int s, int v) { return stn[s][v]; };
     bad = reconstruct<CL, LIM, R>(F.limiter, q, dl0, dl1, dl2, dll, dlr, pl, pr, bv);
     riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll

@@ -140,6 +140,7 @@ template <typename R> __device__ bool closure_check(R rhog, R Tg, R gamma, R Rg,
       e.Re05 = sqrt(mx(Re, (R)0));
       e.Pr = mug*e.cpg/kg;
       e.Sc = e.Pr*(R)ep[EP_LE];
+      evap_invariants(e);
       if (m.intf == 1) {
         R LKd2 = (R)2*mug*sqrt((R)2*pi*Tp*(R)kRu/(R)ep[EP_MV])/((R)ep[EP_ALPHAE]*e.Sc*e.p)/dp;
         R beta = -md*e.Pr/((R)2*pi*mug*dp);

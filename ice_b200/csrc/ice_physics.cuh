@@ -749,9 +749,19 @@ template <typename R> __device__ __forceinline__ R Fcorr(R B) { return B > (R)1.
 
 template <typename R> struct EvapEnv {
   R rhog, Tg, gamma, Rg, mug, kg, Tp, dp, cpg, p, Mg, Pr, Sc, Re05;
+  R Dv, Sh;          // CEM's vapour diffusivity and Sherwood number: the same for every call of a cell
   int evap;
   const double* ep;
 };
+
+// The parts of the gas-side rate that do not depend on the surface state (every Langmuir-Knudsen
+// iteration of a cell calls gas_side with the same environment): once per cell, the same expressions.
+template <typename R> __device__ __forceinline__ void evap_invariants(EvapEnv<R>& e) {
+  if (e.evap == 2) {
+    e.Dv = e.kg/(e.rhog*e.cpg*(R)e.ep[EP_LE]);
+    e.Sh = (R)2 + (R)0.6*e.Re05*pw(e.Sc, (R)(1.0/3.0));
+  }
+}
 
 // gasSideRate with the five gas-side models (Lib_Evaporation.f90:205-224, 287-521)
 template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, R& md, R& Qd, bool& ovr) {
@@ -766,9 +776,7 @@ template <typename R> __device__ void gas_side(const EvapEnv<R>& e, R Ys, R BM, 
       return;
     }
     case 2: {
-      R Dv = e.kg/(e.rhog*e.cpg*(R)ep[EP_LE]);
-      R Sh = (R)2 + (R)0.6*e.Re05*pw(e.Sc, (R)(1.0/3.0));
-      md = -pi*e.dp*e.rhog*Dv*Sh*lg((R)1 + BM);
+      md = -pi*e.dp*e.rhog*e.Dv*e.Sh*lg((R)1 + BM);
       return;
     }
     case 3: {
@@ -871,6 +879,7 @@ template <typename R> __device__ void evaporation(R rhog, R Tg, R gamma, R Rg, R
   e.Re05 = sqrt(mx(Re, (R)0));
   e.Pr = mug*e.cpg/kg;
   e.Sc = e.Pr*(R)ep[EP_LE];
+  evap_invariants(e);
   gas_side(e, Ys, BM, mdot, Qd, ovr);
   if (m.intf != 1) return;
   const R pi = (R)kPi;
