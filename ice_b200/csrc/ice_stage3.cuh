@@ -299,11 +299,11 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
   // z face between c and c + 1 from the ring slots of the two cells and their slopes
   auto zface = [&](int sl, int sr, int c, const R* sa, R da, bool fa, const R* sb, R db, bool fb, R bf, R* out) {
     R pl[nc], pr[nc];
-    const SmemCell<R> ql{plane(sl), pos, np}, qr{plane(sr), pos, np};
-    bad |= states_from_slopes<CL, R>(ql, sa, da, fa, qr, sb, db, fb, bf, pl, pr);
     const long long fi = fidx(B, 2, i, j, c, c + 1);
     R nrm[3], area;
     face_geometry<R>(G, 2, fi, nrm, area);
+    const SmemCell<R> ql{plane(sl), pos, np}, qr{plane(sr), pos, np};
+    bad |= states_from_slopes<CL, R>(ql, sa, da, fa, qr, sb, db, fb, bf, pl, pr);
     R fl[nc];
     riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
@@ -489,12 +489,12 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
         R sl[nc], sr[nc], pl[nc], pr[nc];
 #pragma unroll
         for (int v = 0; v < nc; ++v) { sl[v] = S[v * cap + il]; sr[v] = S[v * cap + iu]; }
-        const SmemCell<R> ql{P, spos(lx, ly), np}, qr{P, spos(cx, cy), np};
-        bad |= states_from_slopes<CL, R>(ql, sl, D[il], Q[il] != 0, qr, sr, D[iu], Q[iu] != 0, bf, pl, pr);
         const int c = d == 0 ? t.i0 + lx : t.j0 + ly;
         const long long fi = fidx(B, d, t.i0 + lx, t.j0 + ly, k, c + 1);
         R nrm[3], area;
         face_geometry<R>(G, d, fi, nrm, area);
+        const SmemCell<R> ql{P, spos(lx, ly), np}, qr{P, spos(cx, cy), np};
+        bad |= states_from_slopes<CL, R>(ql, sl, D[il], Q[il] != 0, qr, sr, D[iu], Q[iu] != 0, bf, pl, pr);
         riemann<CL, RS, R>(pl, pr, nrm, fl, (R)F.mat.cp);
 #pragma unroll
         for (int v = 0; v < nc; ++v) fl[v] = fl[v] * area;
