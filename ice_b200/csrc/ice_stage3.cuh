@@ -466,6 +466,9 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
         (d == 0 ? DX : DY)[idx] = dlc;
         (d == 0 ? QX : QY)[idx] = first ? 1 : 0;
       }
+      // and the next plane's Jameson weights (planes k, k+1, k+2 are in the ring), which the z face reads
+      // after this barrier
+      if (az && k <= B.nk - 2) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
       __syncthreads();
     }
     // the x and y faces of this plane, each once, as one list of tasks dealt out to the threads in turn:
@@ -511,11 +514,11 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     R szn[nc]; R dlzn = (R)0; bool fzn = true;
     if (az && own && k <= B.nk - 2) {
       zslope(cur, nx1, nx2, k + 1, szn, dlzn, fzn);
-      const R b1 = F.sd ? beta_at(cur, nx1, nx2, tx, ty, k + 1) : (R)1;
+      const R b1 = SL ? beta_of(bcur ^ 1, tx, ty) : (F.sd ? beta_at(cur, nx1, nx2, tx, ty, k + 1) : (R)1);
       zface(cur, nx1, k, sz, dlz, fz, szn, dlzn, fzn, mn(beta_of(bcur, tx, ty), b1), fhi);
     }
     // the next plane's weights (its planes below and above are in the ring now), read after a barrier
-    if (az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
+    if (!SL && az && more) beta_plane(bcur ^ 1, cur, nx1, nx2, k + 1);
     if constexpr (SL) fence_proxy_async_smem();   // this thread's slope accesses before the copy that overwrites them
     __syncthreads();
     if constexpr (SL) {
