@@ -11,9 +11,9 @@
 // tuner's sweep uses it).
 //
 // Measured: the first 8 blocks of the 48-block tree, 5401564 cells, one family at a time, FP32-flux form, 3 profiled steps. Stage-kernel launch in ms, the chosen row first:
-//   MK: (16,1,16) 1.1808, (16,3,64) 1.1812, (16,2,64) 1.1816, (16,4,32) 1.1818, (16,1,32) 1.1818, (16,1,64) 1.1822; slowest (32,4,32) 1.2172
-//   IG: (16,4,16) 1.1982, (16,4,64) 1.1987, (16,1,64) 1.1987, (16,3,64) 1.1992, (16,1,32) 1.1993, (16,2,16) 1.1993; slowest (32,1,32) 1.2460
-//   AG: (32,1,24) 2.0126, (32,3,16) 2.0139, (24,4,24) 2.0145, (24,4,16) 2.0147, (24,3,32) 2.0147, (32,1,16) 2.0158; slowest (8,4,16) 2.1166
+//   MK: (24,4,64) 1.3244, (16,2,32) 1.3248, (16,4,32) 1.3252, (16,3,32) 1.3252, (16,4,64) 1.3254, (24,3,32) 1.3257; slowest (32,3,64) 1.3514
+//   IG: (16,4,32) 1.3802, (16,3,64) 1.3803, (16,2,32) 1.3805, (16,4,16) 1.3807, (16,2,64) 1.3809, (16,4,64) 1.3810; slowest (8,4,64) 1.4076
+//   AG: (32,4,32) 2.3719, (32,2,32) 2.3722, (32,3,16) 2.3727, (24,4,32) 2.3735, (24,3,32) 2.3735, (32,2,16) 2.3735; slowest (8,2,16) 2.4648
 #pragma once
 
 namespace ice {
@@ -22,9 +22,9 @@ struct TuneRow { int kz, zpass, wcap; };
 
 // MK, IG, AG
 constexpr TuneRow kTune[3] = {
-    {16, 1, 16},
-    {16, 4, 16},
-    {32, 1, 24},
+    {24, 4, 64},
+    {16, 4, 32},
+    {32, 4, 32},
 };
 
 }  // namespace ice
