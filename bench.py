@@ -117,7 +117,7 @@ def algorithmic_bytes(case, precision: int = abi.PREC_FP64) -> float:
 # ncu capture of the 4-block case of the 48-block tree in the chosen form (second RK stage of each
 # family, 3,714,802 cells). The 48-block case is the same recipe with the same tile shapes, so its
 # launches move about the same bytes per cell: traffic per launch = these x its cells.
-DRAM_BYTES_PER_CELL = {"MK": 303.1, "IG": 332.4, "AG": 534.2}
+DRAM_BYTES_PER_CELL = {"MK": 302.2, "IG": 333.0, "AG": 537.2}
 
 
 def dram_traffic(case, workload: str, precision: int):
