@@ -17,8 +17,7 @@ reach different times after the same steps. Its chosen form is therefore compare
 own sequence of steps (dt-max set to the oracle's step before each step); the time the chosen form
 reaches on its own steps is reported beside it.
 
-The table of every run is written as JSON to $ICE_ACCURACY_OUT, or to gpurun_out/accuracy.json when
-that folder exists.
+The table of every run is written as JSON to $ICE_ACCURACY_OUT when that variable is set.
 """
 import ctypes as C
 import json
@@ -38,7 +37,6 @@ FULL = os.environ.get("ICE_ACCURACY_FULL") == "1"
 PLAIN_LINF = 1e-12
 CHOSEN_L1 = 1e-4
 KEY_FIELDS = ("rho", "n", "mass")
-ROOT = Path(__file__).resolve().parents[1]
 TABLE = {}
 
 
@@ -53,8 +51,6 @@ def gpu():
 def write_table():
     yield
     out = os.environ.get("ICE_ACCURACY_OUT")
-    if not out and (ROOT / "gpurun_out").is_dir():
-        out = str(ROOT / "gpurun_out" / "accuracy.json")
     if out and TABLE:
         Path(out).write_text(json.dumps(TABLE, indent=1))
 
