@@ -403,8 +403,8 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
     }
     const R* P = plane(cur);
     if (own) {
-      // the global operands of this plane's update, z face and own x and y faces, into L1 while the
-      // plane's first faces are computed: the kernel waits on global loads more than on anything else
+      // the global operands of this plane's update and z face into L1 while the plane's slopes and faces
+      // are computed: the kernel waits on global loads more than on anything else
       const long long gq = gidx(B, i, j, k), qq = iidx(B, i, j, k);
 #pragma unroll
       for (int v = 0; v < nc; ++v) {
@@ -422,17 +422,6 @@ k_stage3(Geo G, FamDev F, const CUtensorMap* __restrict__ maps, const Tile* __re
           const long long r1 = ridx(B, i, j, k + 1), rs = (long long)(B.ni + 2) * (B.nj + 2);
           prefetch_l1(G.dlf + 2 * G.NR + r1 + rs);
           prefetch_l1(G.ff[2] + fidx(B, 2, i, j, k, k + 1));
-        }
-        if (ax && i >= 1) {
-          const long long r0 = ridx(B, i - 1, j, k);
-          prefetch_l1(G.dlf + r0 - 1); prefetch_l1(G.dlf + r0 + 2);
-          prefetch_l1(G.ff[0] + fidx(B, 0, i - 1, j, k, i));
-        }
-        if (ay && j >= 1) {
-          const long long r0 = ridx(B, i, j - 1, k), rs = B.ni + 2;
-          const float* d1 = G.dlf + G.NR;
-          prefetch_l1(d1 + r0 - rs); prefetch_l1(d1 + r0); prefetch_l1(d1 + r0 + rs); prefetch_l1(d1 + r0 + 2 * rs);
-          prefetch_l1(G.ff[1] + fidx(B, 1, i, j - 1, k, j));
         }
       }
     }
